@@ -1,0 +1,281 @@
+/*
+ * btorch_b200.h -- C ABI of the B200-native recurrent spiking step.
+ *
+ * This is the drop-in boundary underneath the btorch module API
+ * (SparseConn, LIF, ALIF, ExponentialPSC, DelayedPSC, HeterSynapsePSC,
+ * RecurrentNN).  Every entry point takes plain pointers and sizes, never a
+ * framework type.  Device pointers are raw CUDA global-memory addresses,
+ * host pointers are ordinary process memory, and `stream` is a cudaStream_t
+ * passed as void*.  No entry point allocates device memory or synchronises
+ * the stream (except bt_layout_build, which is host-only), so every device
+ * entry point can be captured in a CUDA graph.  Each returns a bt_status.
+ *
+ * Sparse layout conventions (shared by all entry points):
+ *   canonical order  -- the reference's COO order: edges sorted by
+ *                       (post, src) where src is the (possibly
+ *                       delay-expanded) presynaptic row  pre*n_bins + bin
+ *                       (btorch/models/linear.py:278-292,
+ *                        btorch/connectome/connection.py:1021-1027).
+ *                       `magnitude` is stored in this order.
+ *   CSC (by post)    -- csc_ptr[n_post+1], csc_src[nnz] = packed
+ *                       (pre | bin << BT_BIN_SHIFT), weights = magnitude.
+ *   CSR (by pre)     -- csr_ptr[n_pre+1], csr_dst[nnz] = packed
+ *                       (post | bin << BT_BIN_SHIFT), csr_perm[nnz] maps a
+ *                       CSR position to its canonical index.
+ *
+ * Numerics: every elementwise update is evaluated op by op with IEEE
+ * round-to-nearest single precision in the reference's operator order (no
+ * contraction to FMA); the ordered gather accumulates each output in
+ * ascending source order with fused multiply-add, which is how the
+ * reference's CPU sparse product (torch.sparse.mm) rounds.
+ */
+#ifndef BTORCH_B200_H
+#define BTORCH_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BT_API __attribute__((visibility("default")))
+#else
+#define BT_API
+#endif
+
+#define BT_ABI_VERSION 1
+#define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
+#define BT_MAX_NEURONS (1 << 25)
+#define BT_MAX_BINS 128
+
+typedef enum bt_status {
+  BT_OK = 0,
+  BT_ERR_INVALID = 1,      /* bad argument: the message names it */
+  BT_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+  BT_ERR_TIMEOUT = 3,      /* a bounded device-side wait gave up */
+  BT_ERR_UNSUPPORTED = 4,  /* configuration the kernels do not implement */
+  BT_ERR_LAYOUT = 5        /* COO indices out of range or not canonical */
+} bt_status;
+
+/* Text of the most recent error on the calling thread ("" if none). */
+BT_API const char* bt_last_error(void);
+BT_API int bt_abi_version(void);
+
+/* ------------------------------------------------------------------ */
+/* Static layout (host only).                                          */
+/* Replaces preprocess_sparse  btorch/models/_sparse_preprocess.py:28-122 */
+/* and BaseSparseConn._rebuild_triton_layout  linear.py:329-349.        */
+/* ------------------------------------------------------------------ */
+
+/* Build CSC and CSR views of a canonical COO matrix in one O(nnz) pass.
+ * post[e], src[e]: canonical COO (sorted by (post, src)); src is the
+ * delay-expanded row index pre*n_bins + bin (n_bins = 1 for a plain
+ * matrix).  Outputs are caller-allocated host arrays of the stated sizes.
+ * Fails with BT_ERR_LAYOUT if an index is out of range or the order is not
+ * canonical, BT_ERR_INVALID if nnz >= 2^31 or sizes exceed the packing. */
+BT_API int bt_layout_build(int64_t nnz, const int64_t* post, const int64_t* src,
+                    int64_t n_post, int64_t n_pre, int32_t n_bins,
+                    int32_t* csc_ptr,   /* [n_post + 1] */
+                    uint32_t* csc_src,  /* [nnz] pre | bin << 25 */
+                    int32_t* csr_ptr,   /* [n_pre + 1] */
+                    uint32_t* csr_dst,  /* [nnz] post | bin << 25 */
+                    int32_t* csr_perm); /* [nnz] CSR position -> canonical */
+
+/* ------------------------------------------------------------------ */
+/* Event-driven sparse product  out = x @ W  for SparseConn.forward.   */
+/* Replaces triton_sparse_mm / _launch_sparse_mm                        */
+/* btorch/models/_sparse_triton.py:272-355,418-444.                     */
+/* x: [batch, n_in] dense (graded values allowed), out: [batch, n_out]. */
+/* ------------------------------------------------------------------ */
+
+/* Pull: each output walks its in-edges in ascending source order and
+ * accumulates x[b, src] * w with fmaf, skipping zero inputs.  Deterministic
+ * and bit-identical to the reference's CPU product.  `bits` is scratch of
+ * batch * ceil(n_in / 32) uint32 words. */
+BT_API int bt_spmv_gather(int64_t batch, int64_t n_in, int64_t n_out,
+                   const int32_t* csc_ptr, const uint32_t* csc_src,
+                   const float* csc_w, const float* x, float* out,
+                   uint32_t* bits, void* stream);
+
+/* Push: nonzero inputs are compacted (warp ballot + prefix sum), then one
+ * warp per active (sample, source) streams that source's out-edges with
+ * 128-bit loads and adds into `out` with fp32 reductions in L2.  Order of
+ * the additions is not fixed; exact whenever the partial sums are (dyadic
+ * weights).  `work` is scratch of batch * n_in + 2 int32 words. */
+BT_API int bt_spmv_scatter(int64_t batch, int64_t n_in, int64_t n_out,
+                    const int32_t* csr_ptr, const uint32_t* csr_dst,
+                    const float* csr_w, const float* x, float* out,
+                    int32_t* work, void* stream);
+
+/* Backward of the product (replaces _TritonSparseMM.backward
+ * btorch/models/_sparse_triton.py:389-415).
+ * grad_x[b, j] = sum over out-edges (j -> i) of w * grad_out[b, i]:
+ * a transpose gather in ascending post order, deterministic. */
+BT_API int bt_spmv_grad_input(int64_t batch, int64_t n_in, int64_t n_out,
+                       const int32_t* csr_ptr, const uint32_t* csr_dst,
+                       const float* csr_w, const float* grad_out,
+                       float* grad_x, void* stream);
+
+/* grad_w[canonical e = (j -> i)] = sum_b x[b, j] * grad_out[b, i], over
+ * stored nonzeros only and only over samples whose input x[b, j] is nonzero
+ * (ascending b, fmaf); entries whose source is silent in every sample are
+ * written as 0.  Written in canonical order (coalesced), deterministic.
+ * `masks` is scratch of n_in * ceil(batch / 32) uint32 words. */
+BT_API int bt_spmv_grad_weight(int64_t batch, int64_t n_in, int64_t n_out,
+                        const int32_t* csc_ptr, const uint32_t* csc_src,
+                        const float* x, const float* grad_out, float* grad_w,
+                        uint32_t* masks, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Neuron and synapse parameter descriptors.                           */
+/* ------------------------------------------------------------------ */
+
+/* A per-neuron parameter: value(i) = ptr[i * stride]; stride 0 = scalar. */
+typedef struct bt_param {
+  const float* ptr;
+  int64_t stride;
+} bt_param;
+
+#define BT_NEURON_LIF 0
+#define BT_NEURON_ALIF 1
+
+/* LIF (btorch/models/neurons/lif.py:29-200) and ALIF
+ * (btorch/models/neurons/alif.py:30-268) through
+ * BaseNode.single_step_forward (btorch/models/base.py:1108-1116). */
+typedef struct bt_neuron_desc {
+  int32_t kind;            /* BT_NEURON_LIF / BT_NEURON_ALIF */
+  int32_t hard_reset;      /* 1: v -= (v - v_reset) * s; 0: v -= (v_th - v_reset) * s */
+  int32_t use_refractory;  /* tau_ref given */
+  int32_t spiking;         /* 1: Heaviside forward; 0: sigmoid(k*alpha*u) (smooth) */
+  float dt;                /* environ dt, as fp32 */
+  float sg_alpha;          /* surrogate alpha * 2 ln(1 + sqrt 2), as fp32 */
+  float sg_damping;        /* surrogate damping factor */
+  float pad_;
+  bt_param v_threshold, v_reset, c_m;
+  bt_param tau;            /* LIF membrane time constant */
+  bt_param tau_ref;
+  bt_param g_leak, E_leak, E_k, dg_k, tau_adapt; /* ALIF */
+  bt_param coef_gk;        /* ALIF: expm1(dt * (-1/tau_adapt)) / (-1/tau_adapt), host-rounded */
+} bt_neuron_desc;
+
+/* One BaseNode.single_step_forward (charge -> adaptation -> fire -> reset),
+ * one launch.  x: input current [batch, n].  State inputs v_in, ref_in
+ * (NULL unless use_refractory), gk_in (ALIF only) and the matching outputs
+ * are [batch, n]; an output may alias its input (in-place update).
+ * spike: [batch, n] output.  Saved for the surrogate backward (each may be
+ * NULL): u_save = (v_charged - v_th) / (v_th - v_reset), mask_save = 1 where
+ * the neuron was not refractory, vch_save = v after charge. */
+BT_API int bt_neuron_step(const bt_neuron_desc* d, int64_t batch, int64_t n,
+                   const float* x, const float* v_in, const float* ref_in,
+                   const float* gk_in, float* v_out, float* ref_out,
+                   float* gk_out, float* spike, float* u_save,
+                   float* mask_save, float* vch_save, void* stream);
+
+/* Surrogate-gradient backward of one neuron step (sigmoid surrogate
+ * btorch/models/surrogate/sigmoid.py:23-29; reset as in
+ * btorch/models/neurons/lif.py:170-187, alif.py:230-249).  Inputs: the
+ * step's input current x, grads of
+ * the step outputs g_spike, g_v_new, g_gk_new (each may be NULL = 0) and the
+ * forward's saved u, spike, mask, v_charged plus v_prev / gk_prev.  Outputs:
+ * g_x (input current), g_v_prev, g_gk_prev (ALIF; may be NULL).  The
+ * refractory counter only feeds a detached comparison, so it carries no
+ * gradient into the spike path. */
+BT_API int bt_neuron_step_backward(const bt_neuron_desc* d, int64_t batch, int64_t n,
+                            const float* x, const float* g_spike, const float* g_v_new,
+                            const float* g_gk_new, const float* u_save,
+                            const float* spike, const float* mask_save,
+                            const float* v_charged, const float* v_prev,
+                            const float* gk_prev, float* g_x,
+                            float* g_v_prev, float* g_gk_prev,
+                            int32_t detach_reset, void* stream);
+
+/* Validate a neuron descriptor without launching anything. */
+BT_API int bt_check_neuron_desc(const bt_neuron_desc* d);
+
+/* Exponential PSC step (btorch/models/synapse.py:99-103,171-178):
+ * out = psc + coef * ((-psc) / tau_syn), then out = out + wz (wz may be
+ * NULL).  out may alias psc.  Because the decay is linear, the same call
+ * with wz = NULL applied to a gradient is the decay's backward. */
+BT_API int bt_psc_step(int64_t batch, int64_t n, bt_param coef, bt_param tau_syn,
+                const float* psc, const float* wz, float* out, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Fused multi-step engine for RecurrentNN                             */
+/* (btorch/models/rnn.py:517-528 driven by rnn.py:200-332).            */
+/* ------------------------------------------------------------------ */
+
+#define BT_MODE_SCATTER 0  /* push: 2 launches per step, L2 fp32 reductions */
+#define BT_MODE_GATHER 1   /* pull: 1 launch per step, ordered, bit-exact   */
+
+typedef struct bt_engine_desc {
+  /* sizes */
+  int64_t n;              /* neurons */
+  int64_t batch;          /* samples */
+  int32_t n_bins;         /* delay bins R: a spike at step s through an edge
+                             with bin d reaches the PSC of step s + d */
+  int32_t mode;           /* BT_MODE_SCATTER / BT_MODE_GATHER */
+  int64_t t0;             /* absolute index of the first step of this call */
+  int64_t n_steps;        /* steps in this call */
+  int32_t first_call;     /* 1: PSC state is psc after step t0-1 (normal) */
+  int32_t hist_len;       /* H: slots of the spike-history bitmap ring (>= n_bins) */
+
+  bt_neuron_desc neuron;
+  bt_param psc_coef, psc_tau;  /* ExponentialPSC decay */
+
+  /* connectivity (n_pre == n) */
+  const int32_t* csr_ptr; const uint32_t* csr_dst; const float* csr_w;
+  const int32_t* csc_ptr; const uint32_t* csc_src; const float* csc_w;
+
+  /* state [batch, n], updated in place */
+  float* v; float* refractory; float* g_k; float* psc;
+  float* ring;            /* [n_bins][batch][n] pending currents (scatter) */
+  uint32_t* hist;         /* [hist_len][batch][words] spike bitmaps, slot = step mod H */
+
+  /* inputs */
+  const float* x;         /* [n_steps][batch][n] input current (already projected) */
+  const int32_t* sample_len; /* [batch] steps each sample runs (absolute, from step 0); NULL = all */
+
+  /* outputs (any may be NULL) */
+  uint32_t* raster;       /* [n_steps][batch][words] spike bitmaps */
+  float* spikes;          /* [n_steps][batch][n] spikes as fp32 (reference output layout) */
+  float* v_trace;         /* [n_steps][batch][n] v after each step */
+  float* psc_trace;       /* [n_steps][batch][n] psc after each step */
+
+  /* scratch (scatter mode) */
+  int32_t* work;          /* 4 + 2 * n * (1 + mask_words) int32 */
+  int64_t* stats;         /* [n_steps][4]: active union, events, edges, 0; may be NULL */
+} bt_engine_desc;
+
+/* Run n_steps recurrent steps.  Per step: I = psc + x; neuron update;
+ * psc = psc + coef*((-psc)/tau) + W z (z through the delay ring). */
+BT_API int bt_engine_run(const bt_engine_desc* d, void* stream);
+
+/* Reload the pending-current ring from the spike-history bitmaps so that a
+ * run can resume after the state was reset or replaced: for every spike
+ * z_s in history (s in [t0 - n_bins + 1, t0 - 1]) and edge bin d with
+ * s + d >= t0, add w into ring slot (s + d) mod n_bins.  The ring must be
+ * zero on entry. */
+BT_API int bt_engine_ring_from_history(const bt_engine_desc* d, void* stream);
+
+/* Input projection for DenseConn as neuron_inp_module (nn.Linear,
+ * btorch/models/linear.py:163-228): out[r, i] = bias[i] + sum over nonzero
+ * xin[r, c] (ascending c) of xin[r, c] * w_t[c, i].  rows = steps*batch;
+ * w_t: [c_in, n] (transpose of the module weight); bias may be NULL. */
+BT_API int bt_input_project(int64_t rows, int64_t c_in, int64_t n,
+                     const float* xin, const float* w_t, const float* bias,
+                     float* out, int32_t* work, void* stream);
+
+/* Expand spike bitmaps [rows][words] to fp32 [rows][n] (words = ceil(n/32),
+ * bit i%32 of word i/32 is neuron i). */
+BT_API int bt_bits_to_float(int64_t rows, int64_t n, const uint32_t* bits,
+                     float* out, void* stream);
+
+/* Pack fp32 rows [rows][n] into bitmaps (bit set where the value != 0). */
+BT_API int bt_float_to_bits(int64_t rows, int64_t n, const float* in,
+                     uint32_t* bits, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BTORCH_B200_H */

@@ -1,0 +1,268 @@
+"""Generate golden vectors from the reference btorch (run in the build container).
+
+The reference checkout is imported read-only from REF_ROOT (default
+/root/reference).  Each case builds the reference's own modules on seeded
+synthetic inputs, runs them on the CPU (native sparse backend, fp32) and
+saves inputs, parameters and outputs to tests/golden/<case>.npz.  The tests
+replay these cases through the CPU oracle (pinning it to the reference) and
+through the CUDA engine.
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib.metadata as md
+import sys
+from pathlib import Path
+
+import numpy as np
+
+OUT = Path(__file__).resolve().parent
+
+
+def _import_reference(ref_root: str):
+    orig = md.version
+    md.version = lambda name: "0.0.0+ref" if name == "btorch" else orig(name)
+    sys.path.insert(0, ref_root)
+    import torch  # noqa: F401
+
+    import btorch  # noqa: F401
+    return
+
+
+def make_conn(rng, n_pre, n_post, p, dyadic, exc_frac=0.8, scale=0.1, inh_gain=-0.4, dy_exp=-8):
+    """(pre, post) dense weights: lognormal E/I (sign by presyn) or dyadic
+    synapse counts (geometric, mean 4) times 2**dy_exp."""
+    mask = rng.random((n_pre, n_post)) < p
+    exc = np.arange(n_pre) < int(round(exc_frac * n_pre))
+    if dyadic:
+        cnt = rng.geometric(0.25, size=(n_pre, n_post)).astype(np.float32)
+        w = cnt * np.float32(2.0**dy_exp)
+        w = np.where(exc[:, None], w, -w)
+    else:
+        w = rng.lognormal(-1.0, 1.0, size=(n_pre, n_post)).astype(np.float32) * np.float32(scale)
+        w = np.where(exc[:, None], w, np.float32(inh_gain) * w)
+    return (w * mask).astype(np.float32)
+
+
+def canonical(conn):
+    """Reference canonical COO (linear.py:278-292): the transposed matrix in
+    sum_duplicates order.  Accepts a dense (pre, post) array or a scipy matrix."""
+    import scipy.sparse as sp
+
+    c = (sp.coo_array(conn) if isinstance(conn, np.ndarray) else conn.tocoo()).T
+    c.sum_duplicates()
+    return c.row.astype(np.int64), c.col.astype(np.int64), c.data.astype(np.float32)
+
+
+def case_spmm(rng):
+    import scipy.sparse as sp
+    import torch
+    from btorch.models.linear import SparseConn
+
+    n_in, n_out, B = 300, 200, 5
+    W = (rng.random((n_in, n_out)) < 0.1) * rng.standard_normal((n_in, n_out))
+    W = W.astype(np.float32)
+    m = SparseConn(sp.coo_array(W), enforce_dale=False, sparse_backend="native")
+    x = (rng.random((B, n_in)) < 0.3) * rng.standard_normal((B, n_in))
+    x = torch.tensor(x.astype(np.float32), requires_grad=True)
+    out = m(x)
+    g = torch.tensor(rng.standard_normal((B, n_out)).astype(np.float32))
+    (out * g).sum().backward()
+    return dict(
+        post=m.indices[0].numpy(), src=m.indices[1].numpy(), w=m.magnitude.detach().numpy(),
+        n_in=n_in, n_out=n_out, x=x.detach().numpy(), out=out.detach().numpy(), g=g.numpy(),
+        grad_x=x.grad.numpy(), grad_w=m.magnitude.grad.numpy(),
+    )
+
+
+def _coef(tau, dt):
+    """expm1(dt * lin) / lin with lin = -1.0 / tau, as the reference evaluates it."""
+    import torch
+
+    lin = -1.0 / torch.as_tensor(tau)
+    return (torch.expm1(dt * lin) / lin).numpy().astype(np.float32)
+
+
+def _run_rnn(neuron, synapse, inp, x, batch, names):
+    """Run RecurrentNN; also returns the per-step outputs of the input module
+    (recorded with a forward hook, i.e. exactly what the loop added to psc)."""
+    import torch
+    from btorch.models import environ
+    from btorch.models.functional import init_net_state
+    from btorch.models.rnn import RecurrentNN
+
+    brain = RecurrentNN(neuron, synapse, neuron_inp_module=inp, update_state_names=names)
+    init_net_state(brain, batch_size=batch, dtype=torch.float32)
+    projected = []
+    if inp is not None:
+        inp.register_forward_hook(lambda m, a, out: projected.append(out.detach().clone()))
+    with torch.no_grad(), environ.context(dt=1.0):
+        z, states = brain(torch.tensor(x))
+    proj = torch.stack(projected).numpy() if projected else None
+    return brain, z.numpy(), {k: v.numpy() for k, v in states.items()}, proj
+
+
+def case_lif(rng, *, n, p, batch, steps, dyadic, hard, tau_ref, c_in, in_gain, rate, scale=0.1):
+    """LIF + ExponentialPSC(5) + SparseConn (+ DenseConn input if c_in)."""
+    import scipy.sparse as sp
+    import torch
+    from btorch.models.linear import DenseConn, SparseConn
+    from btorch.models.neurons import LIF
+    from btorch.models.synapse import ExponentialPSC
+
+    Wd = make_conn(rng, n, n, p, dyadic, scale=scale)
+    conn = SparseConn(sp.coo_array(Wd), sparse_backend="native")
+    neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=tau_ref, hard_reset=hard)
+    syn = ExponentialPSC(n, tau_syn=5.0, linear=conn)
+    if c_in:
+        W_in = rng.normal(0.0, 0.05, size=(c_in, n)).astype(np.float32) * np.float32(in_gain)
+        if dyadic:
+            W_in = np.round(W_in * 64.0).astype(np.float32) / np.float32(64.0)
+        inp = DenseConn(c_in, n, weight=torch.tensor(W_in))
+        x = rng.poisson(rate, size=(steps, batch, c_in)).astype(np.float32)
+    else:
+        W_in = None
+        inp = None
+        x = (rng.poisson(rate, size=(steps, batch, n)) * in_gain).astype(np.float32)
+        if dyadic:
+            x = (np.round(x * 64.0) / 64.0).astype(np.float32)
+    _, z, st, proj = _run_rnn(neuron, syn, inp, x, batch, ("neuron.v", "synapse.psc", "neuron.refractory"))
+    post, src, w = canonical(Wd)
+    out = dict(
+        kind=0, n=n, batch=batch, hard=int(hard), use_ref=int(tau_ref is not None),
+        tau_ref=np.float32(tau_ref or 0.0), tau=np.float32(20.0), vth=np.float32(1.0), vr=np.float32(0.0),
+        cm=np.float32(1.0), psc_tau=np.float32(5.0), psc_coef=_coef(5.0, 1.0), dt=np.float32(1.0),
+        post=post, src=src, w=w, n_bins=1, uniform_delay=0, x=x,
+        z=np.packbits(z.astype(np.uint8), axis=-1, bitorder="little"), v=st["neuron.v"], psc=st["synapse.psc"],
+    )
+    if W_in is not None:
+        out["W_in"] = W_in  # (c_in, n): DenseConn weight is W_in.T
+        out["x_proj_ref"] = proj  # [steps, batch, n], the reference's own per-step projection
+    return out
+
+
+def case_alif(rng, *, n, p, batch, steps, dyadic):
+    import scipy.sparse as sp
+    from btorch.models.linear import SparseConn
+    from btorch.models.neurons import ALIF
+    from btorch.models.synapse import ExponentialPSC
+
+    Wd = make_conn(rng, n, n, p, dyadic)
+    conn = SparseConn(sp.coo_array(Wd), sparse_backend="native")
+    neuron = ALIF(n, v_threshold=1.0, v_reset=0.0, c_m=1.0, g_leak=0.05, E_leak=0.0, E_k=-1.0,
+                  tau_adapt=200.0, dg_k=0.07, tau_ref=2.0, hard_reset=True)
+    syn = ExponentialPSC(n, tau_syn=5.0, linear=conn)
+    x = (rng.poisson(0.08, size=(steps, batch, n)) * GAIN["alif"]).astype(np.float32)
+    _, z, st, _ = _run_rnn(neuron, syn, None, x, batch, ("neuron.v", "synapse.psc", "neuron.g_k"))
+    post, src, w = canonical(Wd)
+    return dict(
+        kind=1, n=n, batch=batch, hard=1, use_ref=1, tau_ref=np.float32(2.0), vth=np.float32(1.0),
+        vr=np.float32(0.0), cm=np.float32(1.0), g_leak=np.float32(0.05), E_leak=np.float32(0.0),
+        E_k=np.float32(-1.0), dg_k=np.float32(0.07), tau_adapt=np.float32(200.0), coef_gk=_coef(200.0, 1.0),
+        psc_tau=np.float32(5.0), psc_coef=_coef(5.0, 1.0), dt=np.float32(1.0),
+        post=post, src=src, w=w, n_bins=1, uniform_delay=0, x=x,
+        z=np.packbits(z.astype(np.uint8), axis=-1, bitorder="little"), v=st["neuron.v"],
+        psc=st["synapse.psc"], g_k=st["neuron.g_k"],
+    )
+
+
+def case_delayed(rng, *, n, p, batch, steps, D):
+    """LIF + DelayedPSC(ExponentialPSC, max_delay_steps=D), dyadic weights."""
+    import scipy.sparse as sp
+    from btorch.models.linear import SparseConn
+    from btorch.models.neurons import LIF
+    from btorch.models.synapse import DelayedPSC, ExponentialPSC
+
+    Wd = make_conn(rng, n, n, p, True)
+    conn = SparseConn(sp.coo_array(Wd), sparse_backend="native")
+    neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=2.0, hard_reset=True)
+    syn = DelayedPSC(ExponentialPSC(n, tau_syn=5.0, linear=conn), max_delay_steps=D, use_circular_buffer=True)
+    x = (np.round(rng.poisson(0.1, size=(steps, batch, n)) * GAIN["delay"] * 64) / 64).astype(np.float32)
+    _, z, st, _ = _run_rnn(neuron, syn, None, x, batch, ("neuron.v", "synapse.psc_module.psc"))
+    post, src, w = canonical(Wd)
+    return dict(
+        kind=0, n=n, batch=batch, hard=1, use_ref=1, tau_ref=np.float32(2.0), tau=np.float32(20.0),
+        vth=np.float32(1.0), vr=np.float32(0.0), cm=np.float32(1.0), psc_tau=np.float32(5.0),
+        psc_coef=_coef(5.0, 1.0), dt=np.float32(1.0), post=post, src=src, w=w, n_bins=1, uniform_delay=D,
+        x=x, z=np.packbits(z.astype(np.uint8), axis=-1, bitorder="little"), v=st["neuron.v"],
+        psc=st["synapse.psc_module.psc"],
+    )
+
+
+def case_hetero(rng, *, n, p, batch, steps, D):
+    """LIF + HeterSynapsePSC(n_receptor=1, ExponentialPSC, max_delay_steps=D) on
+    a delay-expanded matrix from expand_conn_for_delays (per-synapse delays)."""
+    import pandas as pd
+    import scipy.sparse as sp
+    from btorch.connectome.connection import expand_conn_for_delays
+    from btorch.models.linear import SparseConn
+    from btorch.models.neurons import LIF
+    from btorch.models.synapse import ExponentialPSC, HeterSynapsePSC
+
+    Wd = make_conn(rng, n, n, p, True)
+    base = sp.coo_array(Wd)
+    delays = rng.integers(1, D + 1, size=base.nnz)  # 1..D steps
+    conn_d = expand_conn_for_delays(base, delays - 1, n_delay_bins=D)
+    conn = SparseConn(conn_d, sparse_backend="native")
+    neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=2.0, hard_reset=True)
+    rti = pd.DataFrame({"receptor_type": ["syn"], "receptor_index": [0]})
+    syn = HeterSynapsePSC(n, n_receptor=1, receptor_type_index=rti, linear=conn, base_psc=ExponentialPSC,
+                          max_delay_steps=D, use_circular_buffer=True, tau_syn=5.0)
+    x = (np.round(rng.poisson(0.1, size=(steps, batch, n)) * GAIN["delay"] * 64) / 64).astype(np.float32)
+    _, z, st, _ = _run_rnn(neuron, syn, None, x, batch, ("neuron.v", "synapse.psc"))
+    post, src, w = canonical(conn_d)
+    return dict(
+        kind=0, n=n, batch=batch, hard=1, use_ref=1, tau_ref=np.float32(2.0), tau=np.float32(20.0),
+        vth=np.float32(1.0), vr=np.float32(0.0), cm=np.float32(1.0), psc_tau=np.float32(5.0),
+        psc_coef=_coef(5.0, 1.0), dt=np.float32(1.0), post=post, src=src, w=w, n_bins=D, uniform_delay=0,
+        x=x, z=np.packbits(z.astype(np.uint8), axis=-1, bitorder="little"), v=st["neuron.v"], psc=st["synapse.psc"],
+    )
+
+
+TRACE_STEPS = 40
+GAIN = {"c1": 1.0, "soft": 0.6, "inp": 4.0, "alif": 0.6, "delay": 0.5}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    _import_reference(args.ref)
+    import torch
+
+    torch.set_num_threads(4)
+    cases = {
+        "spmm_graded": lambda r: case_spmm(r),
+        "lif_c1_small": lambda r: case_lif(r, n=512, p=0.02 * 8, batch=1, steps=150, dyadic=False, hard=True,
+                                           tau_ref=2.0, c_in=128, in_gain=GAIN["c1"], rate=0.05,
+                                           scale=0.01),
+        "lif_dyadic_soft": lambda r: case_lif(r, n=256, p=0.05, batch=4, steps=120, dyadic=True, hard=False,
+                                              tau_ref=None, c_in=0, in_gain=GAIN["soft"], rate=0.05),
+        "lif_dyadic_input": lambda r: case_lif(r, n=256, p=0.05, batch=3, steps=120, dyadic=True, hard=True,
+                                               tau_ref=2.0, c_in=64, in_gain=GAIN["inp"], rate=0.05),
+        "alif_exppsc": lambda r: case_alif(r, n=320, p=0.05, batch=3, steps=150, dyadic=False),
+        "delayed_psc": lambda r: case_delayed(r, n=256, p=0.05, batch=2, steps=120, D=3),
+        "hetero_delay": lambda r: case_hetero(r, n=256, p=0.05, batch=2, steps=120, D=6),
+    }
+    for i, (name, fn) in enumerate(cases.items()):
+        rng = np.random.default_rng(1000 + i)
+        d = fn(rng)
+        # Full spike rasters (bit-packed) are kept; float traces only for the
+        # first TRACE_STEPS steps, plus the state after the last step.
+        for key in ("v", "psc", "g_k"):
+            if key in d and "z" in d:
+                d[key + "_final"] = d[key][-1]
+                d[key] = d[key][:TRACE_STEPS]
+        np.savez_compressed(OUT / f"{name}.npz", **d)
+        extra = ""
+        if "z" in d:
+            z = np.unpackbits(d["z"], axis=-1, bitorder="little")[..., : d["n"]]
+            extra = f" rate/step={z.mean():.4f}"
+        print(f"{name}: saved{extra}")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,51 @@
+"""Pin the CPU oracle to the reference: replay every golden case (made by
+running the reference's own modules) through oracle.c."""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import cases
+
+
+@pytest.mark.parametrize("name", cases.STEP_CASES)
+def test_oracle_reproduces_reference_rasters(name, cpu_threads):
+    d = cases.load(name)
+    spec = cases.netspec(d)
+    st = O.init_state(spec, int(d["batch"]))
+    out = O.run(spec, st, cases.projected_input(d), threads=cpu_threads, want_v=True, want_psc=True)
+    ref_z = cases.spikes(d)
+    K = d["v"].shape[0]
+    if int(d["kind"]) == 0:
+        # LIF: every op is the reference's op -> bit-identical everywhere
+        np.testing.assert_array_equal(out["spikes"], ref_z)
+        np.testing.assert_array_equal(out["v"][:K], d["v"])
+        np.testing.assert_array_equal(out["psc"][:K], d["psc"])
+        np.testing.assert_array_equal(st.v, d["v_final"])
+        np.testing.assert_array_equal(st.psc, d["psc_final"])
+    else:
+        # ALIF: expm1 of the state-dependent term comes from a different libm
+        # (last-ulp differences): traces within rel 1e-5 until spikes diverge
+        div = np.nonzero((out["spikes"] != ref_z).reshape(len(ref_z), -1).any(1))[0]
+        first = int(div[0]) if div.size else len(ref_z)
+        assert first >= K, f"spike raster diverged at step {first}"
+        np.testing.assert_allclose(out["v"][:K], d["v"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(out["psc"][:K], d["psc"], rtol=1e-5, atol=1e-6)
+
+
+def test_oracle_spmm_matches_reference_bitwise():
+    d = cases.load("spmm_graded")
+    n_out = int(d["n_out"])
+    ptr = np.zeros(n_out + 1, np.int64)
+    np.add.at(ptr, d["post"] + 1, 1)
+    ptr = np.cumsum(ptr)
+    out = O.spmm(ptr, d["src"], d["w"], d["x"], n_out)
+    np.testing.assert_array_equal(out, d["out"])
+
+
+def test_oracle_linear_close_to_reference_mkl():
+    d = cases.load("lif_c1_small")
+    x = d["x"]
+    T, B, c = x.shape
+    ours = O.linear(x.reshape(T * B, c), d["W_in"].T).reshape(T, B, -1)
+    np.testing.assert_allclose(ours, d["x_proj_ref"], rtol=1e-5, atol=1e-6)
