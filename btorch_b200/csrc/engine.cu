@@ -83,6 +83,8 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
         if (KIND == BT_NEURON_ALIF) d.g_k[idx] = gk;
         d.psc[idx] = psc_decay(d.psc_coef, d.psc_tau, i, P);
         if (d.v_trace) d.v_trace[(k * B) * n + idx] = v;
+        if (USE_REF && d.ref_trace) d.ref_trace[(k * B) * n + idx] = ref;
+        if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[(k * B) * n + idx] = gk;
         if (d.psc_trace && k > 0) d.psc_trace[((k - 1) * B) * n + idx] = P;
       } else {
         // Finished sample: its state freezes at its last step.  On the first
@@ -90,6 +92,8 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
         // later arrivals are dropped.
         if (k == len) d.psc[idx] = add(d.psc[idx], pending);
         if (d.v_trace) d.v_trace[(k * B) * n + idx] = d.v[idx];
+        if (USE_REF && d.ref_trace) d.ref_trace[(k * B) * n + idx] = d.refractory[idx];
+        if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[(k * B) * n + idx] = d.g_k[idx];
         if (d.psc_trace && k > 0) d.psc_trace[((k - 1) * B) * n + idx] = d.psc[idx];
       }
       if (d.spikes) d.spikes[(k * B) * n + idx] = s;
@@ -280,6 +284,8 @@ __global__ void __launch_bounds__(1024) k_eng_gather(bt_engine_desc d, int64_t k
         }
         d.psc[idx] = P;
         if (d.v_trace) d.v_trace[(k * B) * n + idx] = d.v[idx];
+        if (USE_REF && d.ref_trace) d.ref_trace[(k * B) * n + idx] = d.refractory[idx];
+        if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[(k * B) * n + idx] = d.g_k[idx];
         if (d.psc_trace && k > 0) d.psc_trace[((k - 1) * B) * n + idx] = P;
         if (d.spikes) d.spikes[(k * B) * n + idx] = s;
         if (s != 0.0f) atomicOr(&sbits[b], 1u << (i & 31));

@@ -1,0 +1,14 @@
+"""Module API of btorch.models for the recurrent spiking step."""
+
+from . import environ, functional
+from .base import BaseNode, MemoryModule, ParamBufferMixin, StepModule
+from .history import SpikeHistory
+from .linear import BaseSparseConn, DenseConn, SparseConn
+from .neurons import ALIF, LIF
+from .rnn import RecurrentNN, RecurrentNNAbstract, make_rnn
+from .surrogate import Sigmoid
+from .synapse import BasePSC, DelayedPSC, ExponentialPSC, HeterSynapsePSC
+
+__all__ = ["environ", "functional", "BaseNode", "MemoryModule", "ParamBufferMixin", "StepModule", "SpikeHistory",
+           "BaseSparseConn", "DenseConn", "SparseConn", "ALIF", "LIF", "RecurrentNN", "RecurrentNNAbstract",
+           "make_rnn", "Sigmoid", "BasePSC", "DelayedPSC", "ExponentialPSC", "HeterSynapsePSC"]

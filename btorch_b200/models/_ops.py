@@ -1,0 +1,323 @@
+"""torch.autograd.Functions over the C ABI: the sparse product, one neuron
+step and one exponential-PSC step.  Each forward and backward is one or two
+launches of the sm_100a kernels in btorch_b200/csrc; nothing here computes
+on the CPU or falls back to torch math."""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from .. import _lib as L
+
+# ----------------------------------------------------------------- layout --
+
+
+@dataclass
+class SparseLayout:
+    """Device views of one canonical COO matrix (see include/btorch_b200.h).
+
+    n_in = n_pre * n_bins presynaptic rows (delay-expanded), n_out = posts.
+    Edge arrays of the CSR view are padded to a multiple of 4 entries (+4) so
+    that 128-bit vector loads never leave the allocation."""
+
+    n_pre: int
+    n_bins: int
+    n_out: int
+    nnz: int
+    csc_ptr: torch.Tensor   # int32 [n_out + 1]
+    csc_src: torch.Tensor   # int32 (uint32 bits) [nnz]: pre | bin << 25
+    csr_ptr: torch.Tensor   # int32 [n_pre + 1]
+    csr_dst: torch.Tensor   # int32 (uint32 bits) [pad4(nnz)]: post | bin << 25
+    csr_perm: torch.Tensor  # int64 [nnz]: CSR position -> canonical index
+
+    @property
+    def n_in(self) -> int:
+        return self.n_pre * self.n_bins
+
+    def to(self, device) -> "SparseLayout":
+        return SparseLayout(self.n_pre, self.n_bins, self.n_out, self.nnz,
+                            *(t.to(device) for t in (self.csc_ptr, self.csc_src, self.csr_ptr,
+                                                     self.csr_dst, self.csr_perm)))
+
+
+def pad4(n: int) -> int:
+    return (n + 3) // 4 * 4 + 4
+
+
+def build_layout(indices: torch.Tensor, n_pre: int, n_out: int, n_bins: int = 1) -> SparseLayout:
+    """indices: canonical (2, nnz) int64 (post, src) with src = pre*n_bins + bin.
+    Runs the host builder of the C ABI (one counting-sort pass)."""
+    idx = indices.detach().to("cpu", torch.int64).contiguous()
+    nnz = int(idx.shape[1])
+    post = idx[0].contiguous().numpy()
+    src = idx[1].contiguous().numpy()
+    csc_ptr = np.zeros(n_out + 1, np.int32)
+    csc_src = np.zeros(max(nnz, 1), np.uint32)
+    csr_ptr = np.zeros(n_pre + 1, np.int32)
+    csr_dst = np.zeros(pad4(nnz), np.uint32)
+    csr_perm = np.zeros(max(nnz, 1), np.int32)
+    st = L.lib().bt_layout_build(nnz, post.ctypes.data, src.ctypes.data, n_out, n_pre, n_bins,
+                                 csc_ptr.ctypes.data, csc_src.ctypes.data, csr_ptr.ctypes.data,
+                                 csr_dst.ctypes.data, csr_perm.ctypes.data)
+    L.check(st, "bt_layout_build")
+    as_t = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a)  # noqa: E731
+    return SparseLayout(n_pre=n_pre, n_bins=n_bins, n_out=n_out, nnz=nnz, csc_ptr=as_t(csc_ptr),
+                        csc_src=as_t(csc_src[:nnz].copy()), csr_ptr=as_t(csr_ptr), csr_dst=as_t(csr_dst),
+                        csr_perm=torch.from_numpy(csr_perm[:nnz].astype(np.int64)))
+
+
+def pack_csr_weights(layout: SparseLayout, w_canonical: torch.Tensor) -> torch.Tensor:
+    """Weights in CSR order, padded like csr_dst (zeros in the padding)."""
+    out = torch.zeros(pad4(layout.nnz), device=w_canonical.device, dtype=torch.float32)
+    if layout.nnz:
+        out[: layout.nnz] = w_canonical.detach().index_select(0, layout.csr_perm)
+    return out
+
+
+# ---------------------------------------------------------- sparse product --
+
+
+def _spmv(direction: str, layout: SparseLayout, x: torch.Tensor, w_canon: torch.Tensor,
+          w_csr: torch.Tensor | None) -> torch.Tensor:
+    B, n_in = x.shape
+    dev = x.device
+    out = torch.empty((B, layout.n_out), device=dev, dtype=torch.float32)
+    s = L.stream_of(dev)
+    if direction == "gather":
+        bits = torch.empty(max(1, B * ((n_in + 31) // 32)), device=dev, dtype=torch.int32)
+        st = L.lib().bt_spmv_gather(B, n_in, layout.n_out, layout.csc_ptr.data_ptr(), layout.csc_src.data_ptr(),
+                                    w_canon.data_ptr(), x.data_ptr(), out.data_ptr(), bits.data_ptr(), s)
+        L.check(st, "bt_spmv_gather")
+    else:
+        if w_csr is None:
+            w_csr = pack_csr_weights(layout, w_canon)
+        work = torch.empty(B * n_in + 2, device=dev, dtype=torch.int32)
+        st = L.lib().bt_spmv_scatter(B, n_in, layout.n_out, layout.csr_ptr.data_ptr(), layout.csr_dst.data_ptr(),
+                                     w_csr.data_ptr(), x.data_ptr(), out.data_ptr(), work.data_ptr(), s)
+        L.check(st, "bt_spmv_scatter")
+    return out
+
+
+class SparseMM(torch.autograd.Function):
+    """out = x @ W for a SparseConn (replaces _TritonSparseMM,
+    btorch/models/_sparse_triton.py:358-415)."""
+
+    @staticmethod
+    def forward(ctx, x, w_canon, layout, direction, w_csr):
+        ctx.layout = layout
+        ctx.save_for_backward(x, w_canon)
+        ctx.w_csr = w_csr
+        return _spmv(direction, layout, x, w_canon, w_csr)
+
+    @staticmethod
+    def backward(ctx, g):
+        x, w_canon = ctx.saved_tensors
+        layout: SparseLayout = ctx.layout
+        g = g.contiguous()
+        B, n_in = x.shape
+        s = L.stream_of(g.device)
+        gx = gw = None
+        if ctx.needs_input_grad[0]:
+            w_csr = ctx.w_csr if ctx.w_csr is not None else pack_csr_weights(layout, w_canon)
+            gx = torch.empty_like(x)
+            L.check(L.lib().bt_spmv_grad_input(B, n_in, layout.n_out, layout.csr_ptr.data_ptr(),
+                                               layout.csr_dst.data_ptr(), w_csr.data_ptr(), g.data_ptr(),
+                                               gx.data_ptr(), s), "bt_spmv_grad_input")
+        if ctx.needs_input_grad[1]:
+            gw = torch.empty(layout.nnz, device=g.device, dtype=torch.float32)
+            masks = torch.empty(max(1, n_in * ((B + 31) // 32)), device=g.device, dtype=torch.int32)
+            L.check(L.lib().bt_spmv_grad_weight(B, n_in, layout.n_out, layout.csc_ptr.data_ptr(),
+                                                layout.csc_src.data_ptr(), x.data_ptr(), g.data_ptr(),
+                                                gw.data_ptr(), masks.data_ptr(), s), "bt_spmv_grad_weight")
+        return gx, gw, None, None, None
+
+
+def sparse_mm(x2d, w_canon, layout, direction, w_csr=None):
+    L.require_cuda(x2d, w_canon, what="SparseConn")
+    if x2d.dtype != torch.float32 or w_canon.dtype != torch.float32:
+        raise TypeError("SparseConn supports float32 only.")
+    x2d = x2d.contiguous()
+    if torch.is_grad_enabled() and (x2d.requires_grad or w_canon.requires_grad):
+        return SparseMM.apply(x2d, w_canon, layout, direction, w_csr)
+    return _spmv(direction, layout, x2d, w_canon.detach(), w_csr)
+
+
+# ----------------------------------------------------------- neuron step --
+
+_coef_cache: dict = {}
+
+
+def exp_euler_coef(tau: torch.Tensor, dt: float) -> torch.Tensor:
+    """expm1(dt * lin) / lin with lin = -1.0 / tau, evaluated by torch on the
+    CPU exactly as the reference's exp_euler_step does (ode.py:50), so the
+    device sees the reference's fp32 value."""
+    key = (tau.data_ptr(), getattr(tau, "_version", 0), float(dt), tuple(tau.shape), tau.device)
+    hit = _coef_cache.get(key)
+    if hit is not None:
+        return hit
+    t_cpu = tau.detach().to("cpu", torch.float32)
+    lin = -1.0 / t_cpu
+    coef = (torch.expm1(dt * lin) / lin).reshape(-1).contiguous().to(tau.device)
+    if len(_coef_cache) > 256:
+        _coef_cache.clear()
+    _coef_cache[key] = coef
+    return coef
+
+
+def _flat(t: torch.Tensor) -> torch.Tensor:
+    t = t.detach()
+    if t.dtype != torch.float32:
+        t = t.float()
+    return t.reshape(-1).contiguous()
+
+
+def neuron_desc(node, dt: float):
+    """bt_neuron_desc for an LIF/ALIF module; returns (desc, keepalive)."""
+    from .neurons.alif import ALIF
+    from .neurons.lif import LIF
+
+    keep = []
+
+    def P(t):
+        f = _flat(torch.as_tensor(t))
+        keep.append(f)
+        return L.param(f)
+
+    d = L.BtNeuronDesc()
+    sg = node.surrogate_function
+    d.hard_reset = int(bool(node.hard_reset))
+    d.use_refractory = int(bool(node._use_refractory))
+    d.spiking = int(bool(getattr(sg, "spiking", True)))
+    d.dt = float(dt)
+    d.sg_alpha = float(getattr(sg, "slope", 2.0 * 1.7627471740390859))
+    d.sg_damping = float(getattr(sg, "damping_factor", 1.0))
+    d.v_threshold = P(node.v_threshold)
+    d.v_reset = P(node.v_reset)
+    d.c_m = P(node.c_m)
+    if node._use_refractory:
+        d.tau_ref = P(node.tau_ref)
+    if isinstance(node, ALIF):
+        d.kind = L.BT_NEURON_ALIF
+        d.g_leak, d.E_leak, d.E_k, d.dg_k = P(node.g_leak), P(node.E_leak), P(node.E_k), P(node.dg_k)
+        d.tau_adapt = P(node.tau_adapt)
+        d.coef_gk = P(exp_euler_coef(node.tau_adapt, dt))
+    elif isinstance(node, LIF):
+        d.kind = L.BT_NEURON_LIF
+        d.tau = P(node.tau)
+    else:
+        raise NotImplementedError(f"{type(node).__name__} has no B200 kernel")
+    return d, keep
+
+
+class NeuronStep(torch.autograd.Function):
+    """One neuron step; backward is the hand-written surrogate gradient."""
+
+    @staticmethod
+    def forward(ctx, x, v, ref, gk, node, dt):
+        d, keep = neuron_desc(node, dt)
+        B, n = x.shape
+        spike = torch.empty_like(x)
+        v_out = torch.empty_like(v)
+        ref_out = torch.empty_like(ref) if ref is not None else None
+        gk_out = torch.empty_like(gk) if gk is not None else None
+        u = torch.empty_like(x)
+        mask = torch.empty_like(x)
+        vch = torch.empty_like(x)
+        st = L.lib().bt_neuron_step(d, B, n, x.data_ptr(), v.data_ptr(), L.ptr(ref), L.ptr(gk), v_out.data_ptr(),
+                                    L.ptr(ref_out), L.ptr(gk_out), spike.data_ptr(), u.data_ptr(), mask.data_ptr(),
+                                    vch.data_ptr(), L.stream_of(x.device))
+        L.check(st, "bt_neuron_step")
+        ctx.node, ctx.dt, ctx.keep = node, dt, keep
+        ctx.save_for_backward(x, v, gk, u, spike, mask, vch)
+        if ref_out is not None:
+            ctx.mark_non_differentiable(ref_out)
+        return spike, v_out, ref_out, gk_out
+
+    @staticmethod
+    def backward(ctx, g_spike, g_v, g_ref, g_gk):
+        x, v, gk, u, spike, mask, vch = ctx.saved_tensors
+        d, keep = neuron_desc(ctx.node, ctx.dt)
+        B, n = x.shape
+        g_x = torch.empty_like(x)
+        g_vp = torch.empty_like(v)
+        g_gkp = torch.empty_like(gk) if gk is not None else None
+        cont = lambda t: None if t is None else t.contiguous()  # noqa: E731
+        g_spike, g_v, g_gk = cont(g_spike), cont(g_v), cont(g_gk)
+        st = L.lib().bt_neuron_step_backward(
+            d, B, n, x.data_ptr(), L.ptr(g_spike), L.ptr(g_v), L.ptr(g_gk), u.data_ptr(), spike.data_ptr(),
+            mask.data_ptr(), vch.data_ptr(), v.data_ptr(), L.ptr(gk), g_x.data_ptr(), g_vp.data_ptr(),
+            L.ptr(g_gkp), int(bool(ctx.node.detach_reset)), L.stream_of(x.device))
+        L.check(st, "bt_neuron_step_backward")
+        return g_x, g_vp, None, g_gkp, None, None
+
+
+def neuron_step(node, x, v, ref, gk, dt):
+    """(spike, v, ref, gk) after one step, as new tensors."""
+    L.require_cuda(x, v, what=type(node).__name__)
+    for t in (x, v, ref, gk):
+        if t is not None and t.dtype != torch.float32:
+            raise TypeError(f"{type(node).__name__}: the B200 kernels support float32 state and input only.")
+    need_grad = torch.is_grad_enabled() and any(t is not None and t.requires_grad for t in (x, v, gk))
+    if need_grad:
+        if any(p.requires_grad for p in node.parameters(recurse=False)):
+            raise NotImplementedError("gradients with respect to neuron parameters are not implemented")
+        return NeuronStep.apply(x.contiguous(), v.contiguous(), None if ref is None else ref.detach().contiguous(),
+                                None if gk is None else gk.contiguous(), node, dt)
+    d, keep = neuron_desc(node, dt)
+    B, n = x.shape
+    x = x.contiguous()
+    # Fresh output tensors every step, like the reference's eager ops: a state
+    # stack collected over steps must hold snapshots, not one aliased buffer.
+    spike = torch.empty_like(x)
+    v_out = torch.empty_like(v)
+    ref_out = torch.empty_like(ref) if ref is not None else None
+    gk_out = torch.empty_like(gk) if gk is not None else None
+    st = L.lib().bt_neuron_step(d, B, n, x.data_ptr(), v.data_ptr(), L.ptr(ref), L.ptr(gk), v_out.data_ptr(),
+                                L.ptr(ref_out), L.ptr(gk_out), spike.data_ptr(), None, None, None,
+                                L.stream_of(x.device))
+    L.check(st, "bt_neuron_step")
+    return spike, v_out, ref_out, gk_out
+
+
+# -------------------------------------------------------------- PSC step --
+
+
+class PscStep(torch.autograd.Function):
+    """psc' = psc + coef*((-psc)/tau) (+ wz).  The map is linear, so its
+    backward is the same kernel applied to the incoming gradient."""
+
+    @staticmethod
+    def forward(ctx, psc, wz, coef, tau):
+        out = torch.empty_like(psc)
+        B = psc.shape[0]
+        n = psc.shape[1]
+        L.check(L.lib().bt_psc_step(B, n, L.param(coef), L.param(tau), psc.data_ptr(), L.ptr(wz), out.data_ptr(),
+                                    L.stream_of(psc.device)), "bt_psc_step")
+        ctx.coef, ctx.tau = coef, tau
+        ctx.has_wz = wz is not None
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous()
+        gp = torch.empty_like(g)
+        L.check(L.lib().bt_psc_step(g.shape[0], g.shape[1], L.param(ctx.coef), L.param(ctx.tau), g.data_ptr(), None,
+                                    gp.data_ptr(), L.stream_of(g.device)), "bt_psc_step")
+        return gp, (g if ctx.has_wz else None), None, None
+
+
+def psc_step(psc, wz, coef, tau):
+    L.require_cuda(psc, what="ExponentialPSC")
+    if psc.dtype != torch.float32 or (wz is not None and wz.dtype != torch.float32):
+        raise TypeError("ExponentialPSC: the B200 kernels support float32 only.")
+    psc = psc.contiguous()
+    wz = None if wz is None else wz.contiguous()
+    if torch.is_grad_enabled() and (psc.requires_grad or (wz is not None and wz.requires_grad)):
+        return PscStep.apply(psc, wz, coef, tau)
+    out = torch.empty_like(psc)
+    L.check(L.lib().bt_psc_step(psc.shape[0], psc.shape[1], L.param(coef), L.param(tau), psc.data_ptr(), L.ptr(wz),
+                                out.data_ptr(), L.stream_of(psc.device)), "bt_psc_step")
+    return out

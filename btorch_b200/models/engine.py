@@ -1,0 +1,333 @@
+"""Fused multi-step engine behind RecurrentNN.multi_step_forward.
+
+A RecurrentNN whose neuron is LIF/ALIF, whose synapse is ExponentialPSC,
+DelayedPSC(ExponentialPSC) or HeterSynapsePSC(n_receptor=1, ExponentialPSC)
+over a SparseConn, and whose input module is absent or a DenseConn/nn.Linear
+runs through ``bt_engine_run``: the whole time loop on the device, one or two
+kernel launches per step (btorch_b200/csrc/engine.cu), with the reference's
+outputs (spike stack and requested state stacks) and final state.
+
+Anything else, and any call that needs gradients, runs the per-module path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import torch
+import torch.nn as nn
+
+from .. import _lib as L
+from . import environ
+from ._ops import exp_euler_coef, neuron_desc, pack_csr_weights
+from .functional import named_hidden_states
+from .history import SpikeHistory
+from .linear import BaseSparseConn
+from .neurons.alif import ALIF
+from .neurons.lif import LIF
+from .synapse import DelayedPSC, ExponentialPSC, HeterSynapsePSC
+
+DEFAULT_CHUNK = 512
+
+
+@dataclass
+class EnginePlan:
+    neuron: LIF
+    psc_mod: ExponentialPSC        # module whose `psc` is the state the engine updates
+    conn: BaseSparseConn
+    inp: nn.Module | None
+    n_bins: int                    # delay ring bins R
+    uniform_delay: int             # DelayedPSC delay (0 otherwise)
+    history: SpikeHistory | None
+    top_syn: nn.Module             # RecurrentNN.synapse
+    hetero: bool
+    paths: dict                    # state key -> trace kind
+
+
+def _module_path(root: nn.Module, target: nn.Module) -> str | None:
+    for name, m in root.named_modules():
+        if m is target:
+            return name
+    return None
+
+
+def match(rnn) -> tuple[EnginePlan | None, str]:
+    """Return an EnginePlan for `rnn`, or (None, reason)."""
+    neuron, syn = rnn.neuron, rnn.synapse
+    if type(neuron) not in (LIF, ALIF):
+        return None, f"neuron {type(neuron).__name__} has no fused kernel"
+    if not getattr(neuron.surrogate_function, "spiking", True):
+        return None, "smooth (non-spiking) surrogate forward"
+    if neuron.pre_spike_v:
+        return None, "pre_spike_v"
+    if rnn.syn_inp_module is not None:
+        return None, "syn_inp_module"
+    hetero = False
+    history = None
+    uniform = 0
+    n_bins = 1
+    if type(syn) is ExponentialPSC:
+        psc_mod = syn
+    elif type(syn) is DelayedPSC and type(syn.psc_module) is ExponentialPSC:
+        psc_mod = syn.psc_module
+        if syn.max_delay_steps > 1:
+            uniform = syn.max_delay_steps
+            n_bins = uniform + 1
+            history = syn.history
+    elif type(syn) is HeterSynapsePSC and type(syn.base_psc) is ExponentialPSC and syn.n_receptor == 1:
+        psc_mod = syn.base_psc
+        hetero = True
+        if syn.max_delay_steps > 1:
+            n_bins = syn.max_delay_steps
+            history = syn.history
+    else:
+        return None, f"synapse {type(syn).__name__} has no fused kernel"
+    conn = psc_mod.linear
+    if not isinstance(conn, BaseSparseConn):
+        return None, "synapse linear is not a SparseConn"
+    if conn.bias is not None:
+        return None, "SparseConn bias"
+    n = neuron.size
+    if conn.out_features != n or conn.in_features != n * (n_bins if hetero else 1):
+        return None, "connectivity shape does not match the neuron count"
+    if n_bins > L.BT_MAX_BINS:
+        return None, "too many delay bins"
+    inp = rnn.neuron_inp_module
+    if inp is not None and not isinstance(inp, nn.Linear):
+        return None, f"neuron_inp_module {type(inp).__name__}"
+    # trace kinds for every requested state key (reference default: all memories)
+    names = named_hidden_states(rnn, rnn.update_state_names, allow_buffer=rnn.allow_buffer)
+    npath = _module_path(rnn, neuron)
+    ppath = _module_path(rnn, psc_mod)
+    spath = _module_path(rnn, syn)
+    hpath = _module_path(rnn, history) if history is not None else None
+    paths = {}
+    for key in names:
+        if key == f"{npath}.v":
+            paths[key] = "v"
+        elif key == f"{npath}.refractory":
+            paths[key] = "ref"
+        elif key == f"{npath}.g_k":
+            paths[key] = "gk"
+        elif key in (f"{ppath}.psc", f"{spath}.psc"):
+            paths[key] = "psc"
+        elif hpath is not None and key == f"{hpath}.history":
+            paths[key] = "history"
+        else:
+            return None, f"state '{key}' is not traced by the fused engine"
+    plan = EnginePlan(neuron=neuron, psc_mod=psc_mod, conn=conn, inp=inp, n_bins=n_bins, uniform_delay=uniform,
+                      history=history, top_syn=syn, hetero=hetero, paths=paths)
+    return plan, ""
+
+
+def _state2d(t: torch.Tensor, n: int) -> torch.Tensor:
+    if t is None:
+        raise RuntimeError("state not initialised; call init_net_state() first.")
+    if t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous():
+        raise TypeError("the fused engine needs contiguous float32 CUDA state")
+    return t.view(-1, n)
+
+
+def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None = None,
+        chunk: int | None = None, spikes_out: str = "dense", stats: bool = False, profile: list | None = None):
+    """Run T = x.shape[0] steps.  Returns (z [T, *batch, n] or bitmaps, states).
+
+    profile: if a list, (kind, start_event, end_event) CUDA-event pairs are
+    appended for every input-projection ("project") and recurrent-step
+    ("step") launch group, recorded on the launching stream."""
+    launches = 0
+
+    def _ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(torch.cuda.current_stream(dev))
+        return e
+
+    neuron, psc_mod, conn = plan.neuron, plan.psc_mod, plan.conn
+    n = neuron.size
+    dev = neuron.v.device
+    L.require_cuda(x, neuron.v, what="RecurrentNN")
+    dt = float(environ.get("dt"))
+    v = _state2d(neuron.v, n)
+    B = v.shape[0]
+    batch_shape = neuron.v.shape[:-1] if neuron.v.ndim > 1 else ()
+    ref = _state2d(neuron.refractory, n) if neuron._use_refractory else None
+    gk = _state2d(neuron.g_k, n) if isinstance(neuron, ALIF) else None
+    psc = _state2d(psc_mod.psc, n)
+    T = int(x.shape[0])
+    words = (n + 31) // 32
+
+    desc = L.BtEngineDesc()
+    keep = []
+    nd, k1 = neuron_desc(neuron, dt)
+    keep.append(k1)
+    desc.neuron = nd
+    coef, tau = psc_mod.coefficients(dt)
+    keep += [coef, tau]
+    desc.psc_coef, desc.psc_tau = L.param(coef), L.param(tau)
+    direction = conn.direction(B)
+    desc.mode = L.BT_MODE_GATHER if direction == "gather" else L.BT_MODE_SCATTER
+    lay = conn.engine_layout(plan.n_bins, plan.uniform_delay, dev)
+    w = conn._get_effective_weight().detach().float().contiguous()
+    keep.append(w)
+    desc.n, desc.batch, desc.n_bins = n, B, plan.n_bins
+    H = plan.n_bins + 2
+    desc.hist_len = H
+    desc.csc_ptr, desc.csc_src, desc.csc_w = lay.csc_ptr.data_ptr(), lay.csc_src.data_ptr(), w.data_ptr()
+    if desc.mode == L.BT_MODE_SCATTER:
+        w_csr = pack_csr_weights(lay, w)
+        keep.append(w_csr)
+        desc.csr_ptr, desc.csr_dst, desc.csr_w = lay.csr_ptr.data_ptr(), lay.csr_dst.data_ptr(), w_csr.data_ptr()
+        ring = torch.zeros((plan.n_bins, B, n), device=dev, dtype=torch.float32)
+        mw = (B + 31) // 32
+        work = torch.empty(4 + 2 * n * (1 + mw), device=dev, dtype=torch.int32)
+        keep += [ring, work]
+        desc.ring, desc.work = ring.data_ptr(), work.data_ptr()
+    desc.v, desc.psc = v.data_ptr(), psc.data_ptr()
+    desc.refractory = L.ptr(ref)
+    desc.g_k = L.ptr(gk)
+    hist = torch.zeros((H, B, words), device=dev, dtype=torch.int32)
+    keep.append(hist)
+    desc.hist = hist.data_ptr()
+    t0 = H
+    s = L.stream_of(dev)
+    hist_depth = plan.history.max_delay if plan.history is not None else 0
+    want_hist_trace = "history" in plan.paths.values()
+    if hist_depth and plan.history.use_circular_buffer:
+        cursor0 = plan.history._cursor.clone()
+    if hist_depth:
+        block = plan.history.recent_block(hist_depth).float().contiguous()  # [Dh, B, n], d steps ago
+        bits = torch.empty((hist_depth, B, words), device=dev, dtype=torch.int32)
+        L.check(L.lib().bt_float_to_bits(hist_depth * B, n, block.data_ptr(), bits.data_ptr(), s), "bt_float_to_bits")
+        for d in range(hist_depth):
+            hist[(t0 - 1 - d) % H] = bits[d]
+    desc.t0 = t0
+    if desc.mode == L.BT_MODE_SCATTER and plan.n_bins > 1:
+        desc.n_steps = 1
+        L.check(L.lib().bt_engine_ring_from_history(C.byref(desc), s), "bt_engine_ring_from_history")
+        launches += 1
+
+    # outputs
+    z = torch.empty((T, B, n), device=dev, dtype=torch.float32) if spikes_out == "dense" else None
+    raster = torch.empty((T, B, words), device=dev, dtype=torch.int32)
+    traces = {kind: torch.empty((T, B, n), device=dev, dtype=torch.float32)
+              for kind in set(plan.paths.values()) if kind != "history"}
+    stat_t = torch.zeros((T, 4), device=dev, dtype=torch.int64) if stats else None
+
+    # input
+    inp = plan.inp
+    if inp is not None:
+        x3 = x.reshape(T, B, -1)
+        w_t = inp.weight.detach().float().t().contiguous()
+        bias = inp.bias.detach().float().contiguous() if inp.bias is not None else None
+        keep += [w_t, bias]
+    else:
+        x3 = x.reshape(T, B, n) if x.numel() == T * B * n else torch.broadcast_to(x.reshape(T, -1, n), (T, B, n))
+        if x3.dtype != torch.float32:
+            raise TypeError("RecurrentNN input must be float32 for the fused engine.")
+        x3 = x3.contiguous()
+    sl = None
+    if sample_len is not None:
+        sl_full = torch.as_tensor(sample_len, device=dev, dtype=torch.int64).reshape(B)
+
+    K = int(chunk or DEFAULT_CHUNK)
+    for k0 in range(0, T, K):
+        kc = min(K, T - k0)
+        if inp is not None:
+            c_in = x3.shape[-1]
+            xc = x3[k0:k0 + kc].reshape(kc * B, c_in).float().contiguous()
+            xp = torch.empty((kc, B, n), device=dev, dtype=torch.float32)
+            pw = torch.empty(kc * B * (c_in + 1), device=dev, dtype=torch.int32)
+            e0 = _ev() if profile is not None else None
+            L.check(L.lib().bt_input_project(kc * B, c_in, n, xc.data_ptr(), w_t.data_ptr(), L.ptr(bias),
+                                             xp.data_ptr(), pw.data_ptr(), s), "bt_input_project")
+            launches += 2
+            if profile is not None:
+                profile.append(("project", e0, _ev()))
+            keep_chunk = (xc, xp, pw)
+        else:
+            xp = x3[k0:k0 + kc]
+            keep_chunk = (xp,)
+        if sample_len is not None:
+            sl = (sl_full - k0).clamp(0, kc).to(torch.int32).contiguous()
+            keep_chunk = keep_chunk + (sl,)
+        desc.x = xp.data_ptr()
+        desc.sample_len = L.ptr(sl)
+        desc.t0 = t0 + k0
+        desc.n_steps = kc
+        desc.raster = raster[k0].data_ptr()
+        desc.spikes = z[k0].data_ptr() if z is not None else None
+        desc.v_trace = traces["v"][k0].data_ptr() if "v" in traces else None
+        desc.psc_trace = traces["psc"][k0].data_ptr() if "psc" in traces else None
+        desc.ref_trace = traces["ref"][k0].data_ptr() if "ref" in traces and ref is not None else None
+        desc.gk_trace = traces["gk"][k0].data_ptr() if "gk" in traces and gk is not None else None
+        desc.stats = stat_t[k0].data_ptr() if stat_t is not None else None
+        e0 = _ev() if profile is not None else None
+        L.check(L.lib().bt_engine_run(C.byref(desc), s), "bt_engine_run")
+        launches += (2 * kc if desc.mode == L.BT_MODE_SCATTER else kc) + 1
+        if profile is not None:
+            profile.append(("step", e0, _ev()))
+        del keep_chunk
+
+    # write the spike history back into the module (last Dh spikes)
+    t_end = t0 + T
+    if hist_depth:
+        sel = torch.stack([hist[(t_end - 1 - d) % H] for d in range(hist_depth)]).contiguous()
+        block = torch.empty((hist_depth, B, n), device=dev, dtype=torch.float32)
+        L.check(L.lib().bt_bits_to_float(hist_depth * B, n, sel.data_ptr(), block.data_ptr(), s), "bt_bits_to_float")
+        init_block = plan.history.recent_block(hist_depth).clone() if want_hist_trace else None
+        plan.history.store_recent_block(block, T)
+    if plan.hetero:
+        plan.top_syn.psc = psc_mod.psc.view(*psc_mod.psc.shape[:-1], *plan.top_syn.n_neuron)
+    if "ref" in traces and ref is None:
+        traces.pop("ref")
+
+    states = {}
+    for key, kind in plan.paths.items():
+        if kind == "history":
+            states[key] = _history_trace(plan.history, z if z is not None else _expand(raster, n), init_block,
+                                         batch_shape, cursor0 if plan.history.use_circular_buffer else None)
+        else:
+            states[key] = traces[kind].view(T, *batch_shape, *_nshape(plan, key))
+    rnn.last_engine_stats = stat_t
+    rnn.last_engine_direction = direction
+    rnn.last_engine_launches = launches
+    if z is not None:
+        z = z.view(T, *batch_shape, *neuron.n_neuron)
+        return z, states
+    return raster, states
+
+
+def _nshape(plan: EnginePlan, key: str):
+    if plan.hetero and key.endswith("base_psc.psc"):
+        return (plan.neuron.size,)
+    return plan.neuron.n_neuron
+
+
+def _expand(raster: torch.Tensor, n: int) -> torch.Tensor:
+    T, B, W = raster.shape
+    out = torch.empty((T, B, n), device=raster.device, dtype=torch.float32)
+    L.check(L.lib().bt_bits_to_float(T * B, n, raster.data_ptr(), out.data_ptr(), L.stream_of(raster.device)),
+            "bt_bits_to_float")
+    return out
+
+
+def _history_trace(hist_mod: SpikeHistory, z: torch.Tensor, init_block: torch.Tensor, batch_shape,
+                   c0: torch.Tensor | None) -> torch.Tensor:
+    """Stack of the history memory after every step, in the module's own
+    layout (circular: slot (c0 + s) mod D holds z_s; cat: index d = d steps ago)."""
+    T, B, n = z.shape[0], z.shape[1], z.shape[-1]
+    D = hist_mod.max_delay
+    z = z.reshape(T, B, n)
+    # full sequence of spikes, oldest first: init (D steps, oldest..newest) then z
+    seq = torch.cat([init_block.flip(0).reshape(D, B, n), z], dim=0)  # index D-1+t = z_t
+    if not hist_mod.use_circular_buffer:
+        idx = torch.arange(T, device=z.device)[:, None] + D - torch.arange(D, device=z.device)[None, :]
+        out = seq[idx]  # [T, D, B, n], d steps ago
+        return out.permute(0, 2, 1, 3).reshape(T, *batch_shape, D, n)
+    t = torch.arange(T, device=z.device)[:, None]
+    j = torch.arange(D, device=z.device)[None, :]
+    # latest step s <= t with (c0 + s) % D == j
+    s = t - ((c0 + t - j) % D)
+    out = seq[s + D]  # [T, D, B, n]
+    return out.permute(0, 2, 1, 3).reshape(T, *batch_shape, D, n)

@@ -1,0 +1,209 @@
+"""Recurrent time loop (API of btorch/models/rnn.py).
+
+RecurrentNN.multi_step_forward runs the whole loop through the fused device
+engine (btorch_b200/models/engine.py) when the model matches it and no
+gradient is needed; otherwise it steps module by module -- each module's
+step is one of the sm_100a kernels with a hand-written backward -- using the
+reference's chunking: unroll blocks, large chunks with optional gradient
+checkpointing per chunk (truncated-BPTT windows recompute their forward in
+backward) and optional CPU offload of per-chunk outputs (rnn.py:200-332).
+"""
+
+from __future__ import annotations
+
+from collections.abc import Sequence
+
+import torch
+import torch.nn as nn
+from torch.utils.checkpoint import checkpoint
+
+from . import base, environ
+from . import engine as _engine
+from .functional import filter_hidden_states, named_hidden_states, prepare_sparse_modules, set_hidden_states
+
+
+class RecurrentNNAbstract(base.MemoryModule):
+    def __init__(self, update_state_names: Sequence[str] | None = None, step_mode="m", unroll: int | bool = 8,
+                 chunk_size: int | None = None, cpu_offload: bool = False, grad_checkpoint: bool = False,
+                 save_grad_history: bool = False, grad_state_names=None, cudagraph: bool = False,
+                 cudagraph_warmup: int = 3, fused: bool = True):
+        super().__init__()
+        self.step_mode = step_mode
+        self.update_state_names = update_state_names
+        self.unroll = unroll
+        self.chunk_size = chunk_size
+        self.cpu_offload = cpu_offload
+        self.grad_checkpoint = grad_checkpoint
+        self.save_grad_history = save_grad_history
+        self.grad_state_names = grad_state_names
+        self._grad_history = {}
+        self.cudagraph = cudagraph
+        self.cudagraph_warmup = cudagraph_warmup
+        self.fused = fused
+        self.last_engine_stats = None
+        self.last_engine_direction = None
+        self.last_path = None
+
+    def single_step_forward(self, *args, **kwargs):
+        raise NotImplementedError
+
+    def _detect_loop_args(self, *args):
+        if len(args) == 1:
+            return args[0].shape[0], (0,)
+        shapes = [a.shape[0] if torch.is_tensor(a) and a.ndim > 0 else None for a in args]
+        T = shapes[0]
+        assert T is not None
+        return T, tuple(i for i, s in enumerate(shapes) if s == T)
+
+    def _chunk_plan(self, *args, loop_args=None):
+        if loop_args is None:
+            T, loop_args = self._detect_loop_args(*args)
+        else:
+            T = args[loop_args[0]].shape[0]
+        unroll = T if self.unroll is False else int(self.unroll)
+        if self.chunk_size is None:
+            large = unroll if self.grad_checkpoint else T
+        else:
+            large = self.chunk_size
+            if self.unroll is not False and large % unroll != 0:
+                raise ValueError(f"chunk_size ({large}) must be a multiple of unroll ({unroll})")
+        return T, loop_args, unroll, large, (T + large - 1) // large
+
+    def _process_chunk(self, *chunk_args, loop_args=(0,), **kwargs):
+        T = chunk_args[loop_args[0]].shape[0]
+        zs, states = [], {}
+        a = list(chunk_args)
+        for t in range(T):
+            for i in loop_args:
+                a[i] = chunk_args[i][t]
+            z, st = self.single_step_forward(*a, **kwargs)
+            zs.append(z)
+            for k, v in st.items():
+                states.setdefault(k, []).append(v)
+        return zs, states
+
+    def _checkpointed_chunk(self, *chunk_args, loop_args=(0,), **kwargs):
+        memories = named_hidden_states(self)
+        env = environ.all()
+
+        def _pure(env, memories, *inner):
+            set_hidden_states(self, memories)
+            with environ.context(**env):
+                zs, st = self._process_chunk(*inner, loop_args=loop_args, **kwargs)
+            return torch.stack(zs), {k: torch.stack(v) for k, v in st.items()}
+
+        return checkpoint(_pure, env, memories, *chunk_args, use_reentrant=False)
+
+    def _modular_forward(self, *args, loop_args=None, **kwargs):
+        T, loop_args, unroll, large, n_chunks = self._chunk_plan(*args, loop_args=loop_args)
+        splits = {i: torch.split(args[i], large, dim=0) for i in loop_args}
+        all_z, all_st = [], {}
+        for c in range(n_chunks):
+            cargs = tuple(splits[i][c] if i in loop_args else args[i] for i in range(len(args)))
+            if self.grad_checkpoint:
+                z, st = self._checkpointed_chunk(*cargs, loop_args=loop_args, **kwargs)
+            else:
+                zs, sts = self._process_chunk(*cargs, loop_args=loop_args, **kwargs)
+                z, st = torch.stack(zs), {k: torch.stack(v) for k, v in sts.items()}
+            if self.cpu_offload:
+                z = z.cpu()
+                st = {k: v.cpu() for k, v in st.items()}
+            all_z.append(z)
+            for k, v in st.items():
+                all_st.setdefault(k, []).append(v)
+        cat = lambda xs: xs[0] if len(xs) == 1 else torch.cat(xs)  # noqa: E731
+        self.last_path = "modular"
+        return cat(all_z), {k: cat(v) for k, v in all_st.items()}
+
+    def multi_step_forward(self, *args, loop_args=None, **kwargs):
+        first = args[0]
+        batch = first[0].numel() // first.shape[-1] if torch.is_tensor(first) and first.ndim >= 2 else None
+        with prepare_sparse_modules(self, batch_size=batch):
+            return self._modular_forward(*args, loop_args=loop_args, **kwargs)
+
+    def get_grad_history(self):
+        return self._grad_history
+
+    def clear_grad_history(self):
+        self._grad_history = {}
+
+
+class RecurrentNN(RecurrentNNAbstract):
+    """z = neuron(synapse.psc + inp(x)); synapse(z) every step (rnn.py:485-528)."""
+
+    def __init__(self, neuron: nn.Module, synapse: nn.Module, syn_inp_module: nn.Module | None = None,
+                 neuron_inp_module: nn.Module | None = None, *, update_state_names=None, unroll: int | bool = 8,
+                 chunk_size: int | None = None, cpu_offload: bool = False, grad_checkpoint: bool = False,
+                 allow_buffer=False, **kwargs):
+        super().__init__(update_state_names=update_state_names, unroll=unroll, chunk_size=chunk_size,
+                         cpu_offload=cpu_offload, grad_checkpoint=grad_checkpoint, **kwargs)
+        self.neuron = neuron
+        self.synapse = synapse
+        self.neuron_inp_module = neuron_inp_module
+        self.syn_inp_module = syn_inp_module
+        self.allow_buffer = allow_buffer
+
+    def single_step_forward(self, x, x_syn=None):
+        if self.neuron_inp_module is not None:
+            x = self.neuron_inp_module(x)
+        if self.syn_inp_module is not None:
+            x_syn = self.syn_inp_module(x_syn)
+        z = self.neuron(self.synapse.psc + x)
+        self.synapse(z if x_syn is None else z + x_syn)
+        return z, filter_hidden_states(self, self.update_state_names, allow_buffer=self.allow_buffer)
+
+    def fused_plan(self):
+        """The engine plan for this model, or (None, reason)."""
+        return _engine.match(self)
+
+    def multi_step_forward(self, *args, loop_args=None, sample_len=None, spikes_out: str = "dense",
+                           engine_chunk: int | None = None, engine_stats: bool = False,
+                           engine_profile: list | None = None, **kwargs):
+        """Run T = args[0].shape[0] steps.  Extensions over the reference:
+        sample_len ([batch] steps per sample; later steps of a sample freeze its
+        state and emit no spikes), spikes_out="bitmask" (return the spike raster
+        as [T, batch, ceil(n/32)] int32 words), engine_stats (record per-step
+        active counts in self.last_engine_stats)."""
+        needs_grad = torch.is_grad_enabled() and (
+            any(p.requires_grad for p in self.parameters())
+            or any(torch.is_tensor(a) and a.requires_grad for a in args))
+        extra = len(args) > 1 and any(a is not None for a in args[1:])
+        plan, reason = (None, "disabled")
+        if self.fused and not needs_grad and not extra and not kwargs and loop_args in (None, (0,)):
+            plan, reason = _engine.match(self)
+        if plan is not None:
+            self.last_path = "fused"
+            return _engine.run(plan, self, args[0], sample_len=sample_len, chunk=engine_chunk,
+                               spikes_out=spikes_out, stats=engine_stats, profile=engine_profile)
+        if sample_len is not None or spikes_out != "dense":
+            raise NotImplementedError(f"sample_len / spikes_out need the fused engine ({reason})")
+        self.last_fused_reason = reason
+        return super().multi_step_forward(*args, loop_args=loop_args, **kwargs)
+
+
+def make_rnn(obj=None, allow_buffer=False, **rnn_kwargs):
+    """Wrap a single-step MemoryModule class/instance into a time loop (rnn.py:433-482)."""
+
+    def _build(cell):
+        class RNNWrapped(RecurrentNNAbstract):
+            def __init__(self, *args, **kwargs):
+                super().__init__(**rnn_kwargs)
+                self.rnn_cell = cell(*args, **kwargs) if isinstance(cell, type) else cell
+
+            def single_step_forward(self, *args, **kwargs):
+                out = self.rnn_cell(*args, **kwargs)
+                return out, filter_hidden_states(self.rnn_cell, self.update_state_names, allow_buffer=allow_buffer)
+
+        RNNWrapped.__name__ = f"RNN_{getattr(cell, '__name__', type(cell).__name__)}"
+        return RNNWrapped
+
+    if isinstance(obj, type):
+        return _build(obj)
+    if isinstance(obj, nn.Module):
+        return _build(obj)()
+    if obj is None:
+        return _build
+    raise TypeError("`make_rnn` expects a module class, a module instance, or None as a decorator.")
+
+
+__all__ = ["RecurrentNNAbstract", "RecurrentNN", "make_rnn"]

@@ -241,6 +241,8 @@ typedef struct bt_engine_desc {
   float* spikes;          /* [n_steps][batch][n] spikes as fp32 (reference output layout) */
   float* v_trace;         /* [n_steps][batch][n] v after each step */
   float* psc_trace;       /* [n_steps][batch][n] psc after each step */
+  float* ref_trace;       /* [n_steps][batch][n] refractory after each step */
+  float* gk_trace;        /* [n_steps][batch][n] g_k after each step (ALIF) */
 
   /* scratch (scatter mode) */
   int32_t* work;          /* 4 + 2 * n * (1 + mask_words) int32 */

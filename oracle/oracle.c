@@ -258,14 +258,18 @@ int orc_spmm(int64_t n_out, int64_t batch, int64_t n_in, const int64_t* ptr, con
  * summation order is not reproducible; this order is the one the CUDA
  * projection uses).  out[r][i] = sum_c x[r][c] * W[i][c] (+ bias[i]). */
 int orc_linear(int64_t rows, int64_t c_in, int64_t n, const float* x, const float* W, const float* bias, float* out) {
-  for (int64_t r = 0; r < rows; ++r)
+  int64_t* nz = (int64_t*)malloc(sizeof(int64_t) * (size_t)(c_in > 0 ? c_in : 1));
+  if (!nz) return 1;
+  for (int64_t r = 0; r < rows; ++r) {
+    int64_t cnt = 0;
+    for (int64_t c = 0; c < c_in; ++c)
+      if (x[r * c_in + c] != 0.0f) nz[cnt++] = c;
     for (int64_t i = 0; i < n; ++i) {
       float acc = 0.0f;
-      for (int64_t c = 0; c < c_in; ++c) {
-        const float xv = x[r * c_in + c];
-        if (xv != 0.0f) acc = fmaf(xv, W[i * c_in + c], acc);
-      }
+      for (int64_t q = 0; q < cnt; ++q) acc = fmaf(x[r * c_in + nz[q]], W[i * c_in + nz[q]], acc);
       out[r * n + i] = bias ? acc + bias[i] : acc;
     }
+  }
+  free(nz);
   return 0;
 }

@@ -63,3 +63,48 @@ def projected_input(d: dict, use_reference_projection: bool = True) -> np.ndarra
         return d["x_proj_ref"]
     T, B, c = x.shape
     return O.linear(x.reshape(T * B, c), d["W_in"].T).reshape(T, B, -1)
+
+
+def build_model(d: dict, device="cuda", direction="gather"):
+    """The golden case's network built from btorch_b200 modules."""
+    import pandas as pd
+    import scipy.sparse as sp
+    import torch
+
+    from btorch_b200.models import ALIF, LIF, DelayedPSC, DenseConn, ExponentialPSC, HeterSynapsePSC, RecurrentNN
+    from btorch_b200.models import SparseConn
+    from btorch_b200.models.functional import init_net_state
+
+    n = int(d["n"])
+    n_bins = int(d["n_bins"])
+    conn_m = sp.coo_array((d["w"], (d["src"], d["post"])), shape=(n * n_bins, n))
+    conn = SparseConn(conn_m, sparse_config={"direction": direction})
+    tau_ref = float(d["tau_ref"]) if int(d["use_ref"]) else None
+    if int(d["kind"]) == 0:
+        neuron = LIF(n, v_threshold=float(d["vth"]), v_reset=float(d["vr"]), c_m=float(d["cm"]),
+                     tau=float(d["tau"]), tau_ref=tau_ref, hard_reset=bool(d["hard"]))
+    else:
+        neuron = ALIF(n, v_threshold=float(d["vth"]), v_reset=float(d["vr"]), c_m=float(d["cm"]),
+                      g_leak=float(d["g_leak"]), E_leak=float(d["E_leak"]), E_k=float(d["E_k"]),
+                      tau_adapt=float(d["tau_adapt"]), dg_k=float(d["dg_k"]), tau_ref=tau_ref,
+                      hard_reset=bool(d["hard"]))
+    tau_syn = float(d["psc_tau"])
+    D = int(d["uniform_delay"])
+    if n_bins > 1:
+        rti = pd.DataFrame({"receptor_type": ["syn"], "receptor_index": [0]})
+        syn = HeterSynapsePSC(n, 1, rti, conn, base_psc=ExponentialPSC, max_delay_steps=n_bins,
+                              use_circular_buffer=True, tau_syn=tau_syn)
+        psc_name = "synapse.psc"
+    elif D:
+        syn = DelayedPSC(ExponentialPSC(n, tau_syn, conn), max_delay_steps=D, use_circular_buffer=True)
+        psc_name = "synapse.psc_module.psc"
+    else:
+        syn = ExponentialPSC(n, tau_syn, conn)
+        psc_name = "synapse.psc"
+    inp = None
+    if "W_in" in d:
+        inp = DenseConn(d["W_in"].shape[0], n, weight=torch.tensor(d["W_in"]))
+    names = ["neuron.v", psc_name] + (["neuron.g_k"] if int(d["kind"]) == 1 else [])
+    rnn = RecurrentNN(neuron, syn, neuron_inp_module=inp, update_state_names=names).to(device)
+    init_net_state(rnn, batch_size=int(d["batch"]), dtype=torch.float32, device=device)
+    return rnn, psc_name

@@ -1,0 +1,148 @@
+"""Host-side logic that needs no GPU: the C-ABI library loads and exports every
+declared symbol, the layout builder, config registry, module state API."""
+
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import torch
+
+from btorch_b200 import _lib as L
+from btorch_b200 import config
+from btorch_b200._sparse_config import SparseConfigRegistry, TritonSparseConfig
+from btorch_b200.connectome import expand_conn_for_delays
+from btorch_b200.models import LIF, ALIF, ExponentialPSC, RecurrentNN, SparseConn
+from btorch_b200.models._ops import build_layout
+from btorch_b200.models.functional import init_net_state, named_hidden_states, prepare_sparse_modules, reset_net
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "btorch_b200.h").read_text()
+    return sorted(set(re.findall(r"BT_API\s+(?:const\s+char\*|int)\s+(bt_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 16
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert set(syms) == set(L.exported_symbols())
+    assert lib.bt_abi_version() == 1
+
+
+def test_layout_matches_numpy_reference():
+    rng = np.random.default_rng(0)
+    n_pre, n_post, D = 37, 29, 4
+    dense = (rng.random((n_pre * D, n_post)) < 0.2) * rng.standard_normal((n_pre * D, n_post))
+    c = sp.coo_array(dense.astype(np.float32)).T
+    c.sum_duplicates()
+    idx = torch.tensor(np.stack([c.row, c.col]), dtype=torch.long)
+    lay = build_layout(idx, n_pre, n_post, D)
+    post, src = c.row, c.col
+    # CSC: canonical order, pre|bin packing
+    assert np.array_equal(lay.csc_ptr.numpy(), np.concatenate([[0], np.cumsum(np.bincount(post, minlength=n_post))]))
+    packed = lay.csc_src.numpy().view(np.uint32)
+    assert np.array_equal(packed & ((1 << 25) - 1), src // D)
+    assert np.array_equal(packed >> 25, src % D)
+    # CSR: grouped by pre, canonical order inside, perm maps back
+    perm = lay.csr_perm.numpy()
+    assert sorted(perm.tolist()) == list(range(c.nnz))
+    pre_of = src[perm] // D
+    assert np.all(np.diff(pre_of) >= 0)
+    for j in range(n_pre):
+        seg = perm[lay.csr_ptr[j]: lay.csr_ptr[j + 1]]
+        assert np.all(np.diff(seg) > 0)
+    dst = lay.csr_dst.numpy().view(np.uint32)[: c.nnz]
+    assert np.array_equal(dst & ((1 << 25) - 1), post[perm])
+    assert np.array_equal(dst >> 25, (src % D)[perm])
+    assert lay.csr_dst.numel() % 4 == 0
+
+
+def test_layout_rejects_non_canonical_order():
+    idx = torch.tensor([[1, 0], [0, 0]], dtype=torch.long)
+    with pytest.raises(ValueError, match="canonical"):
+        build_layout(idx, 2, 2, 1)
+    with pytest.raises(ValueError, match="outside"):
+        build_layout(torch.tensor([[0], [5]]), 2, 2, 1)
+
+
+def test_sparse_config_registry_semantics():
+    reg = SparseConfigRegistry()
+    tpl = reg.backend("triton")
+    assert isinstance(tpl, TritonSparseConfig)
+    r = reg.resolve("triton", {"hash": False, "direction": "scatter"})
+    assert tpl.hash is True and r.hash is False and r.direction == "scatter"
+    with pytest.raises(ValueError):
+        reg.resolve("b200", {"no_such_field": 1})
+    with pytest.raises(ValueError):
+        reg.resolve("triton", {"edge_block": 3})
+    with pytest.raises(ValueError):
+        reg.backend("cusparse")
+    with pytest.raises(ValueError):
+        reg.resolve("b200", {"direction": "sideways"})
+
+
+def test_sparseconn_state_dict_and_prepare_scope():
+    W = sp.coo_array(np.array([[1.0, 0.0], [0.0, 2.0]], np.float32))
+    m = SparseConn(W, enforce_dale=False, sparse_backend="native")
+    assert sorted(m.state_dict()) == ["indices", "magnitude"]
+    W2 = sp.coo_array(np.array([[0.0, 3.0], [4.0, 0.0]], np.float32))
+    t = SparseConn(W2, enforce_dale=False)
+    t.load_state_dict(m.state_dict())
+    assert torch.equal(t.indices, m.indices)
+    lay = t.layout()
+    assert lay.csc_ptr.tolist() == [0, 1, 2]
+    with pytest.raises(RuntimeError):
+        t.finish_sparse()
+    with prepare_sparse_modules(t):
+        assert t._sparse_prepare_depth == 1
+    assert t._sparse_prepare_depth == 0
+
+
+def test_sparseconn_has_no_cpu_path():
+    m = SparseConn(sp.coo_array(np.eye(3, dtype=np.float32)))
+    with pytest.raises(RuntimeError, match="CUDA"):
+        m(torch.ones(3))
+
+
+def test_memory_module_reset_inplace_and_state_names():
+    n = 8
+    rnn = RecurrentNN(LIF(n, tau_ref=2.0), ExponentialPSC(n, 5.0, SparseConn(sp.coo_array(np.eye(n, dtype=np.float32)))))
+    init_net_state(rnn, batch_size=2, dtype=torch.float32)
+    v = rnn.neuron.v
+    v.fill_(3.0)
+    reset_net(rnn, inplace=True)
+    assert rnn.neuron.v is v and float(v.abs().sum()) == 0.0
+    assert sorted(named_hidden_states(rnn)) == ["neuron.refractory", "neuron.v", "synapse.psc"]
+    with pytest.raises(ValueError):
+        reset_net(rnn, batch_size=3, inplace=True)
+    a = ALIF(n, g_k_init=0.5)
+    init_net_state(a, batch_size=(2, 3), dtype=torch.float32)
+    assert a.g_k.shape == (2, 3, n) and float(a.g_k[0, 0, 0]) == 0.5
+
+
+def test_expand_conn_for_delays_rows():
+    conn = sp.coo_array(([1.0, 2.0], ([0, 1], [1, 2])), shape=(3, 3))
+    d = expand_conn_for_delays(conn, np.array([1, 3]), n_delay_bins=5)
+    assert d.shape == (15, 3)
+    dense = d.toarray()
+    assert dense[0 * 5 + 1, 1] == 1.0 and dense[1 * 5 + 3, 2] == 2.0
+    with pytest.raises(ValueError):
+        expand_conn_for_delays(conn, np.array([-1, 0]))
+
+
+def test_engine_plan_matching_on_cpu_modules():
+    n = 16
+    conn = SparseConn(sp.coo_array(np.eye(n, dtype=np.float32)))
+    rnn = RecurrentNN(LIF(n, tau_ref=2.0, hard_reset=True), ExponentialPSC(n, 5.0, conn))
+    plan, why = rnn.fused_plan()
+    assert plan is not None, why
+    assert set(plan.paths.values()) == {"v", "ref", "psc"}
+    rnn2 = RecurrentNN(LIF(n), ExponentialPSC(n, 5.0, torch.nn.Linear(n, n)))
+    plan2, why2 = rnn2.fused_plan()
+    assert plan2 is None and "SparseConn" in why2
