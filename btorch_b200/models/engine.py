@@ -193,8 +193,6 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     s = L.stream_of(dev)
     hist_depth = plan.history.max_delay if plan.history is not None else 0
     want_hist_trace = "history" in plan.paths.values()
-    if hist_depth and plan.history.use_circular_buffer:
-        cursor0 = plan.history._cursor.clone()
     if hist_depth:
         block = plan.history.recent_block(hist_depth).float().contiguous()  # [Dh, B, n], d steps ago
         bits = torch.empty((hist_depth, B, words), device=dev, dtype=torch.int32)
@@ -286,7 +284,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     for key, kind in plan.paths.items():
         if kind == "history":
             states[key] = _history_trace(plan.history, z if z is not None else _expand(raster, n), init_block,
-                                         batch_shape, cursor0 if plan.history.use_circular_buffer else None)
+                                         batch_shape, None)
         else:
             states[key] = traces[kind].view(T, *batch_shape, *_nshape(plan, key))
     rnn.last_engine_stats = stat_t
@@ -314,20 +312,20 @@ def _expand(raster: torch.Tensor, n: int) -> torch.Tensor:
 
 def _history_trace(hist_mod: SpikeHistory, z: torch.Tensor, init_block: torch.Tensor, batch_shape,
                    c0: torch.Tensor | None) -> torch.Tensor:
-    """Stack of the history memory after every step, in the module's own
-    layout (circular: slot (c0 + s) mod D holds z_s; cat: index d = d steps ago)."""
+    """Stack of the history memory after every step, as the reference returns it.
+
+    cat mode (history.py:233-250) rebinds a new tensor every step, so the
+    stack holds true snapshots (index d = d steps ago).  Circular mode
+    (history.py:218-231) writes into the same storage every step, so every
+    entry of the reference's stack aliases that storage and reads as the final
+    buffer; the engine returns the same."""
     T, B, n = z.shape[0], z.shape[1], z.shape[-1]
     D = hist_mod.max_delay
+    if hist_mod.use_circular_buffer:
+        final = hist_mod.history.reshape(*batch_shape, D, n)
+        return final.unsqueeze(0).expand(T, *final.shape).clone()
     z = z.reshape(T, B, n)
-    # full sequence of spikes, oldest first: init (D steps, oldest..newest) then z
-    seq = torch.cat([init_block.flip(0).reshape(D, B, n), z], dim=0)  # index D-1+t = z_t
-    if not hist_mod.use_circular_buffer:
-        idx = torch.arange(T, device=z.device)[:, None] + D - torch.arange(D, device=z.device)[None, :]
-        out = seq[idx]  # [T, D, B, n], d steps ago
-        return out.permute(0, 2, 1, 3).reshape(T, *batch_shape, D, n)
-    t = torch.arange(T, device=z.device)[:, None]
-    j = torch.arange(D, device=z.device)[None, :]
-    # latest step s <= t with (c0 + s) % D == j
-    s = t - ((c0 + t - j) % D)
-    out = seq[s + D]  # [T, D, B, n]
+    seq = torch.cat([init_block.flip(0).reshape(D, B, n), z], dim=0)  # seq[i] = z_{i - D}
+    idx = torch.arange(T, device=z.device)[:, None] + D - torch.arange(D, device=z.device)[None, :]
+    out = seq[idx]  # [T, D, B, n], d steps ago
     return out.permute(0, 2, 1, 3).reshape(T, *batch_shape, D, n)
