@@ -61,6 +61,7 @@ _PROTOS = {
     "bt_layout_build": (C.c_int, [_i64, _vp, _vp, _i64, _i64, _i32, _vp, _vp, _vp, _vp, _vp]),
     "bt_spmv_gather": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_spmv_scatter": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "bt_spmv_gather_noalloc": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_spmv_grad_input": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_spmv_grad_weight": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_check_neuron_desc": (C.c_int, [C.POINTER(BtNeuronDesc)]),

@@ -253,3 +253,72 @@ extern "C" int bt_spmv_grad_weight(int64_t batch, int64_t n_in, int64_t n_out, c
   BT_CHECK_LAUNCH("k_spmv_grad_weight");
   return BT_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of bt_spmv_gather.
+//
+// Some callers cannot allocate device memory at the point where they need the
+// product: code running on a stream that is being captured into a CUDA graph
+// under a fixed memory plan, real-time loops that must never hit the implicit
+// device synchronisation of cudaMalloc/cudaFree, and foreign-language hosts
+// (JNI, cgo, plain C) that bind this library without any device allocator.
+// This entry point needs no caller scratch: its bitmap lives in a file-scope
+// device array that every GPU loading the library holds until process exit.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+__device__ __align__(256) uint32_t g_noalloc_gather_bits[BT_NOALLOC_GATHER_MAX_WORDS];
+
+std::mutex g_noalloc_mu;
+uint32_t* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_gather_bits on the current device.  The array's
+// name in host code is only a host-side stand-in, so the address must come
+// from cudaGetSymbolAddress, looked up once per device with that device current.
+int noalloc_scratch(uint32_t** out) {
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return bt_set_error(BT_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(err));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return bt_set_error(BT_ERR_UNSUPPORTED, "device %d", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    err = cudaGetSymbolAddress(&p, g_noalloc_gather_bits);
+    if (err != cudaSuccess || !p)
+      return bt_set_error(BT_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(err));
+    g_noalloc_addr[dev] = static_cast<uint32_t*>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return BT_OK;
+}
+
+}  // namespace
+
+extern "C" int bt_spmv_gather_noalloc(int64_t batch, int64_t n_in, int64_t n_out, const int32_t* csc_ptr,
+                                      const uint32_t* csc_src, const float* csc_w, const float* x, float* out,
+                                      void* stream) {
+  BT_CHECK_ARG(batch >= 0 && n_in >= 0 && n_out >= 0, "negative size");
+  BT_CHECK_ARG(n_in < BT_MAX_NEURONS && n_out < BT_MAX_NEURONS, "sizes must be below 2^25");
+  const int64_t words = ceil_div(n_in, 32);
+  BT_CHECK_ARG(batch * words <= BT_NOALLOC_GATHER_MAX_WORDS,
+               "batch * ceil(n_in / 32) = %lld exceeds the built-in scratch of %d words; use bt_spmv_gather",
+               (long long)(batch * words), BT_NOALLOC_GATHER_MAX_WORDS);
+  if (batch == 0 || n_out == 0) return BT_OK;
+  BT_CHECK_ARG(csc_ptr && x && out, "null pointer");
+  uint32_t* bits = nullptr;
+  if (int st = noalloc_scratch(&bits)) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // k_nonzero_bits rewrites every word the gather reads, so the contents left
+  // by an earlier call never leak into this one.
+  if (words > 0) {
+    k_nonzero_bits<<<grid_for_warps(batch * words), 256, 0, s>>>(batch, n_in, words, x, bits);
+    BT_CHECK_LAUNCH("k_nonzero_bits");
+  }
+  k_spmv_gather<<<grid_for_warps(n_out), 256, 0, s>>>(batch, n_in, n_out, words, csc_ptr, csc_src, csc_w, x, bits,
+                                                       out);
+  BT_CHECK_LAUNCH("k_spmv_gather");
+  return BT_OK;
+}

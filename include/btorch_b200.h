@@ -108,6 +108,25 @@ BT_API int bt_spmv_scatter(int64_t batch, int64_t n_in, int64_t n_out,
                     const float* csr_w, const float* x, float* out,
                     int32_t* work, void* stream);
 
+/* Allocation-free bt_spmv_gather.  No counterpart in the reference: it exists
+ * for callers that cannot allocate device memory when they need the product
+ * (stream capture under a fixed memory plan, loops that must not take the
+ * device-wide synchronisation of cudaMalloc/cudaFree, foreign-language hosts
+ * with no device allocator).  Same arguments and result as bt_spmv_gather
+ * without `bits`: the scratch is a file-scope device array of
+ * BT_NOALLOC_GATHER_MAX_WORDS uint32 words (1 MiB) that every GPU loading the
+ * library holds until exit.  batch * ceil(n_in / 32) above that limit is
+ * rejected with BT_ERR_INVALID.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress with that device current);
+ * make that first call before any stream capture.  Every call shares the one
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and must be serialised by the caller.  Nothing is allocated or freed. */
+#define BT_NOALLOC_GATHER_MAX_WORDS (1 << 18)
+BT_API int bt_spmv_gather_noalloc(int64_t batch, int64_t n_in, int64_t n_out,
+                                  const int32_t* csc_ptr, const uint32_t* csc_src,
+                                  const float* csc_w, const float* x, float* out,
+                                  void* stream);
+
 /* Backward of the product (replaces _TritonSparseMM.backward
  * btorch/models/_sparse_triton.py:389-415).
  * grad_x[b, j] = sum over out-edges (j -> i) of w * grad_out[b, i]:
