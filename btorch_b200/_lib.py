@@ -17,7 +17,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libbtorch_b200.so"
 
 BT_OK, BT_ERR_INVALID, BT_ERR_CUDA, BT_ERR_TIMEOUT, BT_ERR_UNSUPPORTED, BT_ERR_LAYOUT = range(6)
 BT_NEURON_LIF, BT_NEURON_ALIF = 0, 1
-BT_MODE_SCATTER, BT_MODE_GATHER = 0, 1
+BT_MODE_SCATTER, BT_MODE_GATHER, BT_MODE_PULL = 0, 1, 2
 BT_BIN_SHIFT = 25
 BT_MAX_BINS = 128
 
@@ -51,6 +51,8 @@ class BtEngineDesc(C.Structure):
         ("x", _vp), ("sample_len", _vp),
         ("raster", _vp), ("spikes", _vp), ("v_trace", _vp), ("psc_trace", _vp), ("ref_trace", _vp),
         ("gk_trace", _vp),
+        ("sl_ptr", _vp), ("sl_src", _vp), ("sl_w", _vp), ("masks", _vp), ("outdeg", _vp),
+        ("pull_words_per_warp", _i32), ("pad1_", _i32),
         ("work", _vp), ("stats", _vp),
     ]
 
@@ -59,6 +61,7 @@ _PROTOS = {
     "bt_last_error": (C.c_char_p, []),
     "bt_abi_version": (C.c_int, []),
     "bt_layout_build": (C.c_int, [_i64, _vp, _vp, _i64, _i64, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "bt_layout_slices": (C.c_int, [_i64, _vp, _vp, C.c_uint32, _vp, _vp, _vp, _i64, _vp]),
     "bt_spmv_gather": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_spmv_scatter": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_spmv_gather_noalloc": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -73,6 +76,10 @@ _PROTOS = {
     "bt_input_project": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_bits_to_float": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
     "bt_float_to_bits": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
+    "bt_float_to_masks": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
+    "bt_mask_stride": (C.c_int, [_i64]),
+    "bt_engine_work_words": (C.c_int64, [_i64, _i64]),
+    "bt_masks_to_float": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
 }
 
 _lock = threading.Lock()

@@ -40,6 +40,7 @@ class SparseBackendConfig:
     autotune: bool = True
     gather_max_nnz_per_step: int = 1 << 21
     gather_min_active_fraction: float = 0.25
+    pull_min_batch: int = 4
 
     def validate(self) -> None:
         if self.direction not in DIRECTIONS:
@@ -48,6 +49,8 @@ class SparseBackendConfig:
             raise ValueError("gather_max_nnz_per_step must be non-negative.")
         if not 0.0 <= self.gather_min_active_fraction <= 1.0:
             raise ValueError("gather_min_active_fraction must lie in [0, 1].")
+        if self.pull_min_batch < 1:
+            raise ValueError("pull_min_batch must be positive.")
 
 
 B200SparseConfig = SparseBackendConfig

@@ -34,134 +34,227 @@ namespace bt {
 
 constexpr int kEngThreads = 256;
 
-struct EngCounters {
-  int32_t list_count[2];  // active-list length, double buffered by step parity
-  int32_t pad[2];
+__host__ __device__ __forceinline__ int mask_words(int64_t batch) { return int((batch + 31) >> 5); }
+
+// Words per neuron in the pull engine's sample masks: the word count rounded up
+// to the vector width the kernel loads with (1, 2 or 4 words), unchanged above 4.
+__host__ __device__ __forceinline__ int mask_stride(int64_t batch) {
+  const int mw = mask_words(batch);
+  return mw <= 1 ? 1 : mw <= 2 ? 2 : mw <= 4 ? 4 : mw;
+}
+
+// Slot indices of one step, computed on the host per launch so that no kernel
+// evaluates a 64-bit modulo per element.
+struct StepIdx {
+  int r_in;    // (t - 1) mod R: ring slot the neuron phase consumes
+  int r_t;     // t mod R:       ring slot of delay bin 0 for spikes of step t
+  int h_t;     // t mod H:       history slot written at step t
+  int h_prev;  // (t - 1) mod H: history slot of step t - 1
+  int par;     // t & 1
 };
 
-__host__ __device__ __forceinline__ int mask_words(int64_t batch) { return int((batch + 31) >> 5); }
+inline StepIdx step_idx(int64_t t, int R, int H) {
+  StepIdx s;
+  s.r_in = int(((t - 1) % R + R) % R);
+  s.r_t = int(((t % R) + R) % R);
+  s.h_t = int(((t % H) + H) % H);
+  s.h_prev = int(((t - 1) % H + H) % H);
+  s.par = int(t & 1);
+  return s;
+}
 
 // ---------------------------------------------------------------- scatter --
 
-template <int KIND, bool HARD, bool USE_REF>
-__global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, int64_t k, int sg) {
-  extern __shared__ uint32_t sh[];
-  const int nt = kEngThreads / sg;
-  const int tid = threadIdx.x;
-  const int tn = tid % nt, g = tid / nt;
-  const int64_t n = d.n, B = d.batch;
-  const int64_t i0 = int64_t(blockIdx.x) * nt;
-  const int64_t i = i0 + tn;
-  const bool valid = i < n;
-  const int mw = mask_words(B);
-  const int64_t words = (n + 31) >> 5;
-  const int64_t t = d.t0 + k;
-  const int R = d.n_bins;
-  const int64_t slot_in = ((t - 1) % R + R) % R;
-  uint32_t* smask = sh;  // [nt][mw]
-  for (int q = tid; q < nt * mw; q += kEngThreads) smask[q] = 0;
-  __syncthreads();
+// Scatter-mode scratch (d.work, int32 words):
+//   [0, 2*kSub)                    active-list counts, [parity][sub-list]
+//   [2*kSub, 2*kSub + 2n)          "listed" flags, [parity][neuron]
+//   next 2*kSub*cap                list entries, [parity][sub-list][cap]
+//   next 2 n S                     sample masks, [parity][neuron][S words], S = mask_stride(batch)
+// Sub-list s only lists neurons [s*cap, (s+1)*cap) and each neuron is listed at
+// most once per step (its flag), so a sub-list never holds more than cap
+// entries.  cap is a multiple of 32, so the 32 neurons of a warp share one
+// sub-list.
+constexpr int kSub = 64;
 
-  for (int64_t b = g; b < B; b += sg) {
+__host__ __device__ __forceinline__ int64_t sub_cap(int64_t n) { return (((n + kSub - 1) / kSub) + 31) / 32 * 32; }
+
+__host__ __device__ __forceinline__ int64_t scatter_work_words(int64_t n, int64_t batch) {
+  return 2 * kSub + 2 * n + 2 * kSub * sub_cap(n) + 2 * n * mask_stride(batch);
+}
+
+struct ScatterScratch {
+  int32_t* count;
+  int32_t* flag;
+  int32_t* list;
+  uint32_t* mask;
+  int64_t cap;
+  int ms;
+};
+
+__device__ __forceinline__ ScatterScratch scatter_scratch(const bt_engine_desc& d, int par) {
+  ScatterScratch w;
+  const int64_t n = d.n;
+  w.ms = mask_stride(d.batch);
+  w.cap = sub_cap(n);
+  w.count = d.work + par * kSub;
+  w.flag = d.work + 2 * kSub + par * n;
+  w.list = d.work + 2 * kSub + 2 * n + par * kSub * w.cap;
+  w.mask = reinterpret_cast<uint32_t*>(d.work + 2 * kSub + 2 * n + 2 * kSub * w.cap) + int64_t(par) * n * w.ms;
+  return w;
+}
+
+// Grid (ceil(n / 256), ceil(batch / S)): a thread owns neuron i for S
+// consecutive samples; a warp covers one 32-neuron bitmap word of each of
+// them.  All S samples' state is loaded before any is updated (memory-level
+// parallelism), and the neuron's parameters are read once for the S samples.
+template <int KIND, bool HARD, bool USE_REF, int S>
+__global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, int64_t k, StepIdx si) {
+  const int64_t n = d.n, B = d.batch;
+  const int64_t words = (n + 31) >> 5;
+  const int64_t i = int64_t(blockIdx.x) * kEngThreads + threadIdx.x;
+  const int64_t b0 = int64_t(blockIdx.y) * S;
+  if ((i & ~int64_t(31)) >= n) return;  // whole warps past the last word
+  const bool valid = i < n;
+  const int nb = int(B - b0 < S ? B - b0 : S);  // samples of this block (uniform)
+  // Row pointers of sample b0 for this neuron; sample u is at +u * n.
+  const int64_t off0 = b0 * n + (valid ? i : 0);
+  float* __restrict__ ring_p = d.ring + int64_t(si.r_in) * B * n + off0;
+  float* __restrict__ psc_p = d.psc + off0;
+  float* __restrict__ v_p = d.v + off0;
+  float* __restrict__ ref_p = USE_REF ? d.refractory + off0 : nullptr;
+  float* __restrict__ gk_p = KIND == BT_NEURON_ALIF ? d.g_k + off0 : nullptr;
+  const float* __restrict__ x_p = d.x ? d.x + k * B * n + off0 : nullptr;
+  float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
+#pragma unroll
+  for (int u = 0; u < S; ++u) {
+    const bool in = valid && u < nb;
+    const int64_t o = int64_t(u) * n;
+    pend[u] = in ? ring_p[o] : 0.0f;
+    pv[u] = in ? psc_p[o] : 0.0f;
+    xv[u] = (in && x_p) ? x_p[o] : 0.0f;
+    vv[u] = in ? v_p[o] : 0.0f;
+    rv[u] = (in && USE_REF) ? ref_p[o] : 0.0f;
+    gv[u] = (in && KIND == BT_NEURON_ALIF) ? gk_p[o] : 0.0f;
+  }
+  const int64_t ip = valid ? i : 0;
+  const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, ip);
+  const float pc = ld(d.psc_coef, ip), pt = ld(d.psc_tau, ip), rpt = pow2_recip(pt);
+  const unsigned lane = lane_id();
+  const bool traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace || d.spikes;
+  uint32_t* hist_p = d.hist + (int64_t(si.h_t) * B + b0) * words + (i >> 5);
+  uint32_t* raster_p = d.raster ? d.raster + (k * B + b0) * words + (i >> 5) : nullptr;
+  uint32_t spiked = 0;  // bit u: spiked in sample b0 + u
+#pragma unroll
+  for (int u = 0; u < S; ++u) {
+    if (u >= nb) break;  // uniform across the block
+    const int64_t o = int64_t(u) * n;
     float s = 0.0f;
     if (valid) {
-      const int64_t idx = b * n + i;
-      float* ring_in = d.ring + (slot_in * B) * n;
-      const float pending = ring_in[idx];
-      ring_in[idx] = 0.0f;
-      const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
+      ring_p[o] = 0.0f;
+      const int64_t len = d.sample_len ? d.sample_len[b0 + u] : INT64_MAX;
+      float v = vv[u], ref = rv[u], gk = gv[u];
+      float P;
       if (k < len) {
-        const float P = add(d.psc[idx], pending);
-        const float I = d.x ? add(P, d.x[(k * B) * n + idx]) : P;
-        float v = d.v[idx];
-        float ref = USE_REF ? d.refractory[idx] : 0.0f;
-        float gk = KIND == BT_NEURON_ALIF ? d.g_k[idx] : 0.0f;
-        const NeuronOut o = neuron_update<KIND, HARD, USE_REF>(d.neuron, i, I, v, ref, gk);
-        s = o.spike;
-        d.v[idx] = v;
-        if (USE_REF) d.refractory[idx] = ref;
-        if (KIND == BT_NEURON_ALIF) d.g_k[idx] = gk;
-        d.psc[idx] = psc_decay(d.psc_coef, d.psc_tau, i, P);
-        if (d.v_trace) d.v_trace[(k * B) * n + idx] = v;
-        if (USE_REF && d.ref_trace) d.ref_trace[(k * B) * n + idx] = ref;
-        if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[(k * B) * n + idx] = gk;
-        if (d.psc_trace && k > 0) d.psc_trace[((k - 1) * B) * n + idx] = P;
+        P = add(pv[u], pend[u]);
+        const float I = x_p ? add(P, xv[u]) : P;
+        const NeuronOut out = neuron_update<KIND, HARD, USE_REF, true>(prm, I, v, ref, gk);
+        s = out.spike;
+        v_p[o] = v;
+        if (USE_REF) ref_p[o] = ref;
+        if (KIND == BT_NEURON_ALIF) gk_p[o] = gk;
+        psc_p[o] = psc_decay(pc, pt, rpt, P);
       } else {
         // Finished sample: its state freezes at its last step.  On the first
         // step past the end the pending sum completes psc of that last step;
         // later arrivals are dropped.
-        if (k == len) d.psc[idx] = add(d.psc[idx], pending);
-        if (d.v_trace) d.v_trace[(k * B) * n + idx] = d.v[idx];
-        if (USE_REF && d.ref_trace) d.ref_trace[(k * B) * n + idx] = d.refractory[idx];
-        if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[(k * B) * n + idx] = d.g_k[idx];
-        if (d.psc_trace && k > 0) d.psc_trace[((k - 1) * B) * n + idx] = d.psc[idx];
+        P = pv[u];
+        if (k == len) {
+          P = add(P, pend[u]);
+          psc_p[o] = P;
+        }
       }
-      if (d.spikes) d.spikes[(k * B) * n + idx] = s;
+      if (traces) {
+        const int64_t tix = (k * B + b0 + u) * n + i;
+        if (d.psc_trace && k > 0) d.psc_trace[tix - B * n] = P;
+        if (d.v_trace) d.v_trace[tix] = v;
+        if (USE_REF && d.ref_trace) d.ref_trace[tix] = ref;
+        if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[tix] = gk;
+        if (d.spikes) d.spikes[tix] = s;
+      }
     }
     const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
-    if ((tid & 31) == 0 && i < n) {
-      const int64_t w = i >> 5;
-      d.hist[((t % d.hist_len) * B + b) * words + w] = word;
-      if (d.raster) d.raster[(k * B + b) * words + w] = word;
+    if (lane == 0) {
+      hist_p[int64_t(u) * words] = word;
+      if (raster_p) raster_p[int64_t(u) * words] = word;
     }
-    if (s != 0.0f) atomicOr(&smask[tn * mw + (b >> 5)], 1u << (b & 31));
+    if (s != 0.0f) spiked |= 1u << u;
   }
-  __syncthreads();
-
-  // Compact the neurons of this tile that spiked in any sample.
-  EngCounters* cnt = reinterpret_cast<EngCounters*>(d.work);
-  int32_t* list_j = d.work + 4;
-  uint32_t* list_m = reinterpret_cast<uint32_t*>(d.work + 4 + 2 * n);  // [2][n][mw]
-  const int par = int(t & 1);
-  __shared__ int32_t warp_tot[kEngThreads / 32];
-  __shared__ int32_t block_base;
-  bool act = false;
-  if (tid < nt) {
-    for (int q = 0; q < mw; ++q) act |= smask[tid * mw + q] != 0;
+  if (__ballot_sync(0xffffffffu, spiked != 0) == 0) return;  // warp-uniform
+  // Publish the samples' bits in the neuron's mask; the first sample to spike
+  // lists the neuron (one atomic per warp on one of kSub counters).
+  const ScatterScratch ws = scatter_scratch(d, si.par);
+  bool first = false;
+  if (spiked) {
+    uint32_t* mrow = ws.mask + i * ws.ms;
+#pragma unroll
+    for (int u = 0; u < S; ++u)
+      if (spiked & (1u << u)) atomicOr(mrow + ((b0 + u) >> 5), 1u << ((b0 + u) & 31));
+    first = atomicOr(ws.flag + i, 1) == 0;
   }
-  const uint32_t bal = __ballot_sync(0xffffffffu, act);
-  const int wid = tid >> 5;
-  if ((tid & 31) == 0) warp_tot[wid] = __popc(bal);
-  __syncthreads();
-  if (tid == 0) {
-    int32_t tot = 0;
-    for (int q = 0; q < kEngThreads / 32; ++q) {
-      const int32_t c = warp_tot[q];
-      warp_tot[q] = tot;
-      tot += c;
-    }
-    block_base = tot ? atomicAdd(&cnt->list_count[par], tot) : 0;
-  }
-  __syncthreads();
-  if (act) {
-    const int32_t pos = block_base + warp_tot[wid] + __popc(bal & ((1u << (tid & 31)) - 1u));
-    list_j[par * n + pos] = int32_t(i);
-    for (int q = 0; q < mw; ++q) list_m[(int64_t(par) * n + pos) * mw + q] = smask[tid * mw + q];
-  }
+  const uint32_t fb = __ballot_sync(0xffffffffu, first);
+  if (fb == 0) return;
+  const int sub = int((i - lane) / ws.cap);  // same for the whole warp (cap % 32 == 0)
+  int32_t base = 0;
+  if (lane == 0) base = atomicAdd(ws.count + sub, __popc(fb));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (first) ws.list[sub * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = int32_t(i);
 }
 
-__global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, int64_t k) {
+__global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, int64_t k, StepIdx si) {
   const int64_t n = d.n, B = d.batch;
-  const int64_t t = d.t0 + k;
   const int R = d.n_bins;
-  const int mw = mask_words(B);
-  EngCounters* cnt = reinterpret_cast<EngCounters*>(d.work);
-  const int par = int(t & 1);
-  const int32_t count = cnt->list_count[par];
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    cnt->list_count[par ^ 1] = 0;  // consumed by the next step's neuron kernel
-    if (d.stats) d.stats[k * 4 + 0] = count;
+  const int par = si.par;
+  const ScatterScratch ws = scatter_scratch(d, par);
+  __shared__ int32_t s_off[kSub + 1];
+  if (threadIdx.x == 0) {
+    int32_t acc = 0;
+    for (int q = 0; q < kSub; ++q) {
+      s_off[q] = acc;
+      acc += ws.count[q];
+    }
+    s_off[kSub] = acc;
   }
-  const int32_t* list_j = d.work + 4 + par * n;
-  const uint32_t* list_m = reinterpret_cast<const uint32_t*>(d.work + 4 + 2 * n) + int64_t(par) * n * mw;
+  __syncthreads();
+  const int32_t count = s_off[kSub];
+  if (blockIdx.x == 0 && threadIdx.x < kSub) {
+    // counts of the other parity were consumed by the previous step's scatter;
+    // clear them for the next step's neuron kernel
+    d.work[(par ^ 1) * kSub + threadIdx.x] = 0;
+    if (threadIdx.x == 0 && d.stats) d.stats[k * 4 + 0] = count;
+  }
   const unsigned lane = lane_id();
   const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const int t_mod_r = si.r_t;  // slot of bin b is t_mod_r + b (mod R), b < R
+  const int ms = ws.ms;
   long long ev = 0, ed = 0;
   for (int64_t it = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; it < count; it += warps) {
-    const int32_t j = list_j[it];
-    const int32_t beg = d.csr_ptr[j], end = d.csr_ptr[j + 1];
+    int sub = 0;
+    while (sub + 1 < kSub && s_off[sub + 1] <= it) ++sub;
+    const int32_t j = ws.list[sub * ws.cap + (it - s_off[sub])];
+    uint32_t mw_local[8];
     int nsamp = 0;
-    for (int q = 0; q < mw; ++q) nsamp += __popc(list_m[it * mw + q]);
+    uint32_t* mrow = ws.mask + int64_t(j) * ms;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      mw_local[q] = q < ms ? mrow[q] : 0u;
+      nsamp += __popc(mw_local[q]);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      for (int q = 0; q < ms; ++q) mrow[q] = 0;  // cleared for the step after next
+      ws.flag[j] = 0;
+    }
+    const int32_t beg = d.csr_ptr[j], end = d.csr_ptr[j + 1];
     ev += (long long)nsamp * (end - beg);
     ed += end - beg;
     for (int32_t gidx = (beg & ~3) + int32_t(lane) * 4; gidx < end; gidx += 128) {
@@ -174,10 +267,12 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, i
         const int32_t e = gidx + qq;
         if (e < beg || e >= end) continue;
         const uint32_t post = dd[qq] & kIdMask;
-        const int64_t slot = (t + (dd[qq] >> BT_BIN_SHIFT)) % R;
-        float* base = d.ring + (slot * B) * n + post;
-        for (int q = 0; q < mw; ++q) {
-          uint32_t m = list_m[it * mw + q];
+        int slot = t_mod_r + int(dd[qq] >> BT_BIN_SHIFT);
+        if (slot >= R) slot -= R;
+        float* base = d.ring + (int64_t(slot) * B) * n + post;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          uint32_t m = mw_local[q];
           while (m) {
             const int l = __ffs(m) - 1;
             m &= m - 1;
@@ -194,13 +289,11 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, i
 }
 
 // psc_{t_end-1} = stored + pending(t_end - 1); clears that slot.
-__global__ void k_eng_scatter_final(bt_engine_desc d) {
+__global__ void k_eng_scatter_final(bt_engine_desc d, StepIdx si) {
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t n = d.n, B = d.batch;
   if (idx >= B * n) return;
-  const int64_t t_last = d.t0 + d.n_steps - 1;
-  const int R = d.n_bins;
-  float* ring = d.ring + (((t_last % R + R) % R) * B) * n;
+  float* ring = d.ring + (int64_t(si.r_t) * B) * n;
   const float pending = ring[idx];
   ring[idx] = 0.0f;
   const int64_t b = idx / n;
@@ -218,10 +311,10 @@ __global__ void k_eng_scatter_final(bt_engine_desc d) {
 
 // Ordered in-edge gather of W z for (b, i) at arrival step `ta`:
 // sum over in-edges (pre, bin) ascending of w * z_{ta - bin}[pre].
-__device__ __forceinline__ float gather_in(const bt_engine_desc& d, int64_t i, int64_t b, int64_t ta, int64_t words) {
+__device__ __forceinline__ float gather_in(const bt_engine_desc& d, int64_t i, int64_t b, int ta_mod_h, int64_t words) {
   const unsigned lane = lane_id();
   const int32_t beg = __ldg(d.csc_ptr + i), end = __ldg(d.csc_ptr + i + 1);
-  const int64_t H = d.hist_len;
+  const int H = d.hist_len;  // slot of bin b is ta_mod_h - b (mod H), b < H
   float acc = 0.0f;
   for (int32_t base = beg; base < end; base += 32) {
     const int32_t e = base + int32_t(lane);
@@ -230,8 +323,9 @@ __device__ __forceinline__ float gather_in(const bt_engine_desc& d, int64_t i, i
     if (e < end) {
       const uint32_t src = __ldg(d.csc_src + e);
       const uint32_t pre = src & kIdMask;
-      const int64_t s = ta - int64_t(src >> BT_BIN_SHIFT);
-      const uint32_t word = d.hist[(((s % H) + H) % H * d.batch + b) * words + (pre >> 5)];
+      int slot = ta_mod_h - int(src >> BT_BIN_SHIFT);
+      if (slot < 0) slot += H;
+      const uint32_t word = d.hist[(int64_t(slot) * d.batch + b) * words + (pre >> 5)];
       act = (word >> (pre & 31)) & 1u;
       if (act) w = __ldg(d.csc_w + e);
     }
@@ -248,16 +342,16 @@ __device__ __forceinline__ float gather_in(const bt_engine_desc& d, int64_t i, i
 // One launch per step.  Block = 32 warps = 32 consecutive neurons, so each
 // (sample, 32-neuron word) of the spike bitmap is written by one thread.
 template <int KIND, bool HARD, bool USE_REF>
-__global__ void __launch_bounds__(1024) k_eng_gather(bt_engine_desc d, int64_t k) {
+__global__ void __launch_bounds__(1024) k_eng_gather(bt_engine_desc d, int64_t k, StepIdx si) {
   extern __shared__ uint32_t sbits[];  // [batch]
   const int64_t n = d.n, B = d.batch;
   const int64_t words = (n + 31) >> 5;
-  const int64_t t = d.t0 + k;
   const int wid = threadIdx.x >> 5;
   const unsigned lane = lane_id();
   const int64_t i = int64_t(blockIdx.x) * 32 + wid;
   for (int64_t b = threadIdx.x; b < B; b += blockDim.x) sbits[b] = 0;
   __syncthreads();
+  int nspk = 0;
   if (i < n) {
     for (int64_t b = 0; b < B; ++b) {
       const int64_t idx = b * n + i;
@@ -266,7 +360,7 @@ __global__ void __launch_bounds__(1024) k_eng_gather(bt_engine_desc d, int64_t k
       // stored psc already is psc_{t0-1}; skipped after a sample's last step)
       float P = d.psc[idx];
       if (k > 0 && k - 1 < len) {
-        const float wz = gather_in(d, i, b, t - 1, words);
+        const float wz = gather_in(d, i, b, si.h_prev, words);
         P = add(psc_decay(d.psc_coef, d.psc_tau, i, P), wz);
       }
       float s = 0.0f;
@@ -276,7 +370,8 @@ __global__ void __launch_bounds__(1024) k_eng_gather(bt_engine_desc d, int64_t k
           float v = d.v[idx];
           float ref = USE_REF ? d.refractory[idx] : 0.0f;
           float gk = KIND == BT_NEURON_ALIF ? d.g_k[idx] : 0.0f;
-          const NeuronOut o = neuron_update<KIND, HARD, USE_REF>(d.neuron, i, I, v, ref, gk);
+          const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, i);
+          const NeuronOut o = neuron_update<KIND, HARD, USE_REF, true>(prm, I, v, ref, gk);
           s = o.spike;
           d.v[idx] = v;
           if (USE_REF) d.refractory[idx] = ref;
@@ -288,24 +383,32 @@ __global__ void __launch_bounds__(1024) k_eng_gather(bt_engine_desc d, int64_t k
         if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[(k * B) * n + idx] = d.g_k[idx];
         if (d.psc_trace && k > 0) d.psc_trace[((k - 1) * B) * n + idx] = P;
         if (d.spikes) d.spikes[(k * B) * n + idx] = s;
-        if (s != 0.0f) atomicOr(&sbits[b], 1u << (i & 31));
+        if (s != 0.0f) {
+          atomicOr(&sbits[b], 1u << (i & 31));
+          ++nspk;
+        }
       }
+    }
+    if (d.stats && lane == 0 && nspk) {
+      const long long deg = d.outdeg ? d.outdeg[i] : 0;
+      atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 0), 1ull);
+      atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 1), (unsigned long long)(nspk * deg));
+      atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 2), (unsigned long long)deg);
     }
   }
   __syncthreads();
   const int64_t w = int64_t(blockIdx.x);
   for (int64_t b = threadIdx.x; b < B; b += blockDim.x) {
-    d.hist[((t % d.hist_len) * B + b) * words + w] = sbits[b];
+    d.hist[(int64_t(si.h_t) * B + b) * words + w] = sbits[b];
     if (d.raster) d.raster[(k * B + b) * words + w] = sbits[b];
   }
 }
 
 // Synapse update of the last step of a call: psc_{t_end-1}.
-__global__ void __launch_bounds__(1024) k_eng_gather_final(bt_engine_desc d) {
+__global__ void __launch_bounds__(1024) k_eng_gather_final(bt_engine_desc d, StepIdx si) {
   const int64_t n = d.n, B = d.batch;
   const int64_t words = (n + 31) >> 5;
   const int64_t k = d.n_steps - 1;
-  const int64_t t = d.t0 + k;
   const int64_t i = int64_t(blockIdx.x) * 32 + (threadIdx.x >> 5);
   if (i >= n) return;
   for (int64_t b = 0; b < B; ++b) {
@@ -315,13 +418,224 @@ __global__ void __launch_bounds__(1024) k_eng_gather_final(bt_engine_desc d) {
       if (lane_id() == 0 && d.psc_trace) d.psc_trace[(k * B) * n + idx] = d.psc[idx];
       continue;
     }
-    const float wz = gather_in(d, i, b, t, words);
+    const float wz = gather_in(d, i, b, si.h_t, words);
     if (lane_id() == 0) {
       const float P = add(psc_decay(d.psc_coef, d.psc_tau, i, d.psc[idx]), wz);
       d.psc[idx] = P;
       if (d.psc_trace) d.psc_trace[(k * B) * n + idx] = P;
     }
   }
+}
+
+// ------------------------------------------------------------ sliced pull --
+//
+// PULL mode, one launch per step for batched runs.  Warp = (slice of 32 posts,
+// 32-sample word q); lane = post.  The warp walks the slice's SELL-32 rows
+// (each post's in-edges in canonical order down its lane), looks up the
+// presynaptic neuron's sample mask for the step the edge's delay bin points
+// at, and adds w into acc[sample][lane] in shared memory -- conflict-free and
+// in ascending in-edge order for every (sample, post), i.e. the reference's
+// fma chain (acc + w == fma(w, 1, acc)).  Then each lane runs the neuron
+// update of its post for the warp's 32 samples and publishes its new mask.
+constexpr int kPullWarps = 8;
+constexpr int kPullUnroll = 8;
+
+template <int MW>
+struct MaskVec;
+template <>
+struct MaskVec<1> {
+  using T = uint32_t;
+  __device__ static void split(T v, uint32_t* m) { m[0] = v; }
+};
+template <>
+struct MaskVec<2> {
+  using T = uint2;
+  __device__ static void split(T v, uint32_t* m) { m[0] = v.x; m[1] = v.y; }
+};
+template <>
+struct MaskVec<4> {
+  using T = uint4;
+  __device__ static void split(T v, uint32_t* m) { m[0] = v.x; m[1] = v.y; m[2] = v.z; m[3] = v.w; }
+};
+
+// MW: sample words a warp covers (1, 2 or 4 -> batch up to 32, 64, 128).  For
+// larger batches MW = 1 and the grid has one warp per (slice, word): `split`.
+template <int KIND, bool HARD, bool USE_REF, bool FINAL, int MW>
+__global__ void __launch_bounds__(kPullWarps * 32, 3) k_eng_pull(bt_engine_desc d, int64_t k, int split, StepIdx si) {
+  extern __shared__ float acc_dyn[];  // [kPullWarps][MW * 32][32]
+  const int wid = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t n = d.n, B = d.batch;
+  const int mw_all = mask_stride(B);
+  const int64_t n_slices = (n + 31) >> 5;
+  const int64_t gw = int64_t(blockIdx.x) * kPullWarps + wid;
+  const int64_t sl = split ? gw / mw_all : gw;
+  const int q0 = split ? int(gw % mw_all) : 0;  // first sample word of this warp
+  if (sl >= n_slices) return;  // warp-uniform; the kernel has no block barrier
+  const int64_t p = sl * 32 + lane;
+  const bool valid = p < n;
+  const int H = d.hist_len;
+  // history slot of the arrival step whose PSC this launch completes
+  const int ta_mod_h = FINAL ? si.h_t : si.h_prev;
+  const bool gather = FINAL || k > 0;
+  float(*acc)[32] = reinterpret_cast<float(*)[32]>(acc_dyn + wid * (MW * 32 * 32));
+  using V = typename MaskVec<MW>::T;
+  const int64_t row_stride = int64_t(n + 1) * mw_all;  // words per history slot
+  if (gather) {
+#pragma unroll 8
+    for (int l = 0; l < MW * 32; ++l) acc[l][lane] = 0.0f;
+    __syncwarp();
+    const int64_t r0 = d.sl_ptr[sl], r1 = d.sl_ptr[sl + 1];
+    const uint32_t sentinel = uint32_t(n);
+    for (int64_t r = r0; r < r1; r += kPullUnroll) {
+      uint32_t src[kPullUnroll];
+      float w[kPullUnroll];
+      V mv[kPullUnroll];
+#pragma unroll
+      for (int u = 0; u < kPullUnroll; ++u) {
+        const bool in = r + u < r1;
+        src[u] = in ? __ldg(d.sl_src + (r + u) * 32 + lane) : sentinel;
+        w[u] = in ? __ldg(d.sl_w + (r + u) * 32 + lane) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < kPullUnroll; ++u) {
+        int slot = ta_mod_h - int(src[u] >> BT_BIN_SHIFT);
+        if (slot < 0) slot += H;
+        const uint32_t* mrow = d.masks + slot * row_stride + int64_t(src[u] & kIdMask) * mw_all + q0;
+        mv[u] = __ldg(reinterpret_cast<const V*>(mrow));
+      }
+#pragma unroll
+      for (int u = 0; u < kPullUnroll; ++u) {
+        uint32_t m[MW];
+        MaskVec<MW>::split(mv[u], m);
+#pragma unroll
+        for (int q = 0; q < MW; ++q) {
+          uint32_t mm = m[q];
+          while (mm) {
+            const int l = __ffs(mm) - 1;
+            mm &= mm - 1;
+            acc[q * 32 + l][lane] = add(acc[q * 32 + l][lane], w[u]);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  const int64_t words = n_slices;
+  uint32_t my_mask[MW];
+#pragma unroll
+  for (int q = 0; q < MW; ++q) my_mask[q] = 0;
+  constexpr int U = 4;
+  const float* __restrict__ xk = d.x ? d.x + (k * B) * n : nullptr;
+  const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, valid ? p : 0);
+  const float pc = ld(d.psc_coef, valid ? p : 0), pt = ld(d.psc_tau, valid ? p : 0), rpt = pow2_recip(pt);
+#pragma unroll
+  for (int q = 0; q < MW; ++q) {
+    for (int l0 = 0; l0 < 32; l0 += U) {
+      const int64_t b0 = int64_t(q0 + q) * 32 + l0;
+      if (b0 >= B) break;  // warp-uniform
+      // load phase: U samples' state at once (independent loads in flight)
+      float pv[U], xv[U], vv[U], rv[U], gv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t b = b0 + u;
+        const bool in = valid && b < B;
+        const int64_t idx = b * n + p;
+        pv[u] = in ? d.psc[idx] : 0.0f;
+        xv[u] = (in && xk && !FINAL) ? xk[idx] : 0.0f;
+        vv[u] = (in && !FINAL) ? d.v[idx] : 0.0f;
+        rv[u] = (in && USE_REF && !FINAL) ? d.refractory[idx] : 0.0f;
+        gv[u] = (in && KIND == BT_NEURON_ALIF && !FINAL) ? d.g_k[idx] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t b = b0 + u;
+        if (b >= B) break;  // warp-uniform
+        const int l = l0 + u;
+        float spk = 0.0f;
+        if (valid) {
+          const int64_t idx = b * n + p;
+          const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
+          float P = pv[u];
+          const bool syn_live = FINAL ? (k < len) : (k - 1 < len);
+          if (gather && syn_live) P = add(psc_decay(pc, pt, rpt, P), acc[q * 32 + l][lane]);
+          if (FINAL) {
+            d.psc[idx] = P;
+            if (d.psc_trace) d.psc_trace[(k * B) * n + idx] = P;
+            continue;
+          }
+          float v = vv[u], ref = rv[u], gk = gv[u];
+          if (k < len) {
+            const float I = xk ? add(P, xv[u]) : P;
+            const NeuronOut o = neuron_update<KIND, HARD, USE_REF, true>(prm, I, v, ref, gk);
+            spk = o.spike;
+            d.v[idx] = v;
+            if (USE_REF) d.refractory[idx] = ref;
+            if (KIND == BT_NEURON_ALIF) d.g_k[idx] = gk;
+          }
+          d.psc[idx] = P;
+          if (d.v_trace) d.v_trace[(k * B) * n + idx] = v;
+          if (USE_REF && d.ref_trace) d.ref_trace[(k * B) * n + idx] = ref;
+          if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[(k * B) * n + idx] = gk;
+          if (d.psc_trace && k > 0) d.psc_trace[((k - 1) * B) * n + idx] = P;
+          if (d.spikes) d.spikes[(k * B) * n + idx] = spk;
+        }
+        if (!FINAL) {
+          const uint32_t word = __ballot_sync(0xffffffffu, spk != 0.0f);
+          if (lane == 0 && d.raster) d.raster[(k * B + b) * words + sl] = word;
+          if (spk != 0.0f) my_mask[q] |= 1u << l;
+        }
+      }
+    }
+  }
+  if (FINAL) return;
+  if (valid) {
+    uint32_t* mrow = d.masks + int64_t(si.h_t) * row_stride + p * mw_all + q0;
+#pragma unroll
+    for (int q = 0; q < MW; ++q) mrow[q] = my_mask[q];
+  }
+  if (d.stats) {
+    // events = spikes x out-degree; union counted by the warp that owns word 0
+    int nspk = 0;
+#pragma unroll
+    for (int q = 0; q < MW; ++q) nspk += __popc(my_mask[q]);
+    const int deg = (valid && d.outdeg) ? d.outdeg[p] : 0;
+    long long ev = (long long)nspk * deg;
+    long long ed = (!split && nspk) ? deg : 0;
+    long long un = (!split && nspk) ? 1 : 0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      ev += __shfl_xor_sync(0xffffffffu, ev, off);
+      ed += __shfl_xor_sync(0xffffffffu, ed, off);
+      un += __shfl_xor_sync(0xffffffffu, un, off);
+    }
+    if (lane == 0) {
+      if (ev) atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 1), (unsigned long long)ev);
+      if (ed) atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 2), (unsigned long long)ed);
+      if (un) atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 0), (unsigned long long)un);
+    }
+  }
+}
+
+// masks[i][q] bit l  <=>  in[(32 q + l) * n + i] != 0   (sample-minor from [B][n]).
+__global__ void k_float_to_masks(int64_t batch, int64_t n, const float* __restrict__ in, uint32_t* __restrict__ masks) {
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int mw = mask_stride(batch);
+  if (idx >= n * mw) return;
+  const int64_t i = idx / mw;
+  const int q = int(idx % mw);
+  uint32_t m = 0;
+  for (int l = 0; l < 32 && int64_t(q) * 32 + l < batch; ++l)
+    if (in[(int64_t(q) * 32 + l) * n + i] != 0.0f) m |= 1u << l;
+  masks[idx] = m;
+}
+
+__global__ void k_masks_to_float(int64_t batch, int64_t n, const uint32_t* __restrict__ masks, float* __restrict__ out) {
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= batch * n) return;
+  const int64_t b = idx / n, i = idx % n;
+  const int mw = mask_stride(batch);
+  out[idx] = float((masks[i * mw + (b >> 5)] >> (b & 31)) & 1u);
 }
 
 // ------------------------------------------------------------ ring rebuild --
@@ -354,47 +668,63 @@ __global__ void k_ring_from_history(bt_engine_desc d) {
 
 // ------------------------------------------------------- input projection --
 
-// Per row r: ascending list of nonzero input channels (warp ballot + prefix).
-__global__ void k_row_nonzeros(int64_t rows, int64_t c_in, const float* __restrict__ xin, int32_t* __restrict__ cnt,
-                               int32_t* __restrict__ idx) {
+// Per row r: its nonzero inputs as (channel, value) pairs in ascending channel
+// order (warp ballot + prefix), and their count.
+__global__ void k_row_pairs(int64_t rows, int64_t c_in, const float* __restrict__ xin, int32_t* __restrict__ cnt,
+                            int2* __restrict__ pairs) {
   const int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   if (r >= rows) return;
   const unsigned lane = lane_id();
   int32_t total = 0;
   for (int64_t c0 = 0; c0 < c_in; c0 += 32) {
     const int64_t c = c0 + lane;
-    const bool nz = c < c_in && xin[r * c_in + c] != 0.0f;
+    const float v = c < c_in ? xin[r * c_in + c] : 0.0f;
+    const bool nz = v != 0.0f;
     const uint32_t m = __ballot_sync(0xffffffffu, nz);
-    if (nz) idx[r * c_in + total + __popc(m & ((1u << lane) - 1u))] = int32_t(c);
+    if (nz) pairs[r * c_in + total + __popc(m & ((1u << lane) - 1u))] = make_int2(int(c), __float_as_int(v));
     total += __popc(m);
   }
   if (lane == 0) cnt[r] = total;
 }
 
-// out[r][i] = sum over nonzero xin[r][c] (ascending c) of xin * w_t[c][i] (+ bias).
-// grid.x walks row blocks fastest so that concurrently resident blocks share a
-// narrow slice of w_t in L2.
+// out[r][i] = sum over the row's pairs (ascending channel) of v * w_t[c][i],
+// as an fmaf chain (+ bias).  Each thread owns kProjNPT neurons spaced by the
+// block size, so one broadcast pair load feeds kProjNPT coalesced weight loads
+// and fmas.  grid.x walks row blocks fastest: the resident blocks then share a
+// narrow column slice of w_t, which stays in L2.
 constexpr int kProjRows = 8;
+constexpr int kProjNPT = 4;
 __global__ void __launch_bounds__(256) k_input_project(int64_t rows, int64_t c_in, int64_t n,
-                                                       const float* __restrict__ xin,
                                                        const float* __restrict__ w_t,
                                                        const float* __restrict__ bias,
                                                        const int32_t* __restrict__ cnt,
-                                                       const int32_t* __restrict__ idx, float* __restrict__ out) {
-  const int64_t i = int64_t(blockIdx.y) * 256 + threadIdx.x;
+                                                       const int2* __restrict__ pairs, float* __restrict__ out) {
+  const int64_t tile = int64_t(blockIdx.y) * (256 * kProjNPT);
   const int64_t r0 = int64_t(blockIdx.x) * kProjRows;
-  if (i >= n) return;
-  const float bi = bias ? bias[i] : 0.0f;
+  int64_t ii[kProjNPT];
+  bool ok[kProjNPT];
+#pragma unroll
+  for (int j = 0; j < kProjNPT; ++j) {
+    ii[j] = tile + threadIdx.x + j * 256;
+    ok[j] = ii[j] < n;
+  }
   for (int64_t r = r0; r < r0 + kProjRows && r < rows; ++r) {
     const int32_t c_n = cnt[r];
-    const int32_t* ri = idx + r * c_in;
-    const float* xr = xin + r * c_in;
-    float acc = 0.0f;
+    const int2* rp = pairs + r * c_in;
+    float acc[kProjNPT];
+#pragma unroll
+    for (int j = 0; j < kProjNPT; ++j) acc[j] = 0.0f;
     for (int32_t q = 0; q < c_n; ++q) {
-      const int32_t c = ri[q];
-      acc = fmaf(xr[c], __ldg(w_t + int64_t(c) * n + i), acc);
+      const int2 pr = __ldg(rp + q);
+      const float v = __int_as_float(pr.y);
+      const float* wr = w_t + int64_t(pr.x) * n;
+#pragma unroll
+      for (int j = 0; j < kProjNPT; ++j)
+        if (ok[j]) acc[j] = fmaf(v, __ldg(wr + ii[j]), acc[j]);
     }
-    out[r * n + i] = bias ? add(acc, bi) : acc;
+#pragma unroll
+    for (int j = 0; j < kProjNPT; ++j)
+      if (ok[j]) out[r * n + ii[j]] = bias ? add(acc[j], bias[ii[j]]) : acc[j];
   }
 }
 
@@ -433,7 +763,8 @@ int engine_check(const bt_engine_desc* d) {
   BT_CHECK_ARG(d->n_bins >= 1 && d->n_bins <= BT_MAX_BINS, "n_bins=%d outside [1, 128]", d->n_bins);
   BT_CHECK_ARG(d->hist_len >= d->n_bins + 2, "hist_len=%d must be >= n_bins + 2", d->hist_len);
   BT_CHECK_ARG(d->n_steps >= 0 && d->t0 >= 0, "negative step index");
-  BT_CHECK_ARG(d->mode == BT_MODE_SCATTER || d->mode == BT_MODE_GATHER, "mode=%d", d->mode);
+  BT_CHECK_ARG(d->mode == BT_MODE_SCATTER || d->mode == BT_MODE_GATHER || d->mode == BT_MODE_PULL, "mode=%d",
+               d->mode);
   BT_CHECK_ARG(d->v && d->psc && d->hist, "state pointer missing (v / psc / hist)");
   BT_CHECK_ARG(!d->neuron.use_refractory || d->refractory, "refractory state missing");
   BT_CHECK_ARG(d->neuron.kind != BT_NEURON_ALIF || d->g_k, "g_k state missing");
@@ -444,54 +775,79 @@ int engine_check(const bt_engine_desc* d) {
     BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->csr_dst) & 15) == 0 &&
                      (reinterpret_cast<uintptr_t>(d->csr_w) & 15) == 0,
                  "CSR edge arrays must be 16-byte aligned and padded to a multiple of 4");
-  } else {
+  } else if (d->mode == BT_MODE_GATHER) {
     BT_CHECK_ARG(d->csc_ptr && d->csc_src && d->csc_w, "gather needs CSC");
+  } else {
+    BT_CHECK_ARG(d->sl_ptr && d->sl_src && d->sl_w && d->masks, "pull needs the sliced layout and masks");
   }
   return BT_OK;
-}
-
-int sample_groups(int64_t batch) {
-  int sg = 1;
-  while (sg * 2 <= 8 && sg * 2 <= batch) sg *= 2;
-  return sg;
 }
 
 template <int KIND, bool HARD, bool USE_REF>
 int run_typed(const bt_engine_desc& d, cudaStream_t s) {
   const int64_t n = d.n;
   if (d.mode == BT_MODE_SCATTER) {
-    const int sg = sample_groups(d.batch);
-    const int nt = kEngThreads / sg;
-    const int grid = int(ceil_div(n, nt));
-    const size_t smem = sizeof(uint32_t) * size_t(nt) * size_t(mask_words(d.batch));
+    BT_CHECK_ARG(mask_stride(d.batch) <= 8, "scatter mode supports up to 256 samples");
+    constexpr int S = 4;
+    const dim3 grid(unsigned(ceil_div(n, kEngThreads)), unsigned(ceil_div(d.batch, S)));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (smem > 48 * 1024) {
-      if (cudaFuncSetAttribute(k_eng_neuron<KIND, HARD, USE_REF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               int(smem)) != cudaSuccess)
-        return bt_set_error(BT_ERR_CUDA, "shared memory request of %zu bytes refused", smem);
-    }
-    if (cudaMemsetAsync(d.work, 0, sizeof(EngCounters), s) != cudaSuccess)
+    const size_t scratch_words = size_t(scatter_work_words(n, d.batch));
+    if (cudaMemsetAsync(d.work, 0, sizeof(int32_t) * scratch_words, s) != cudaSuccess)
       return bt_set_error(BT_ERR_CUDA, "memset failed");
     for (int64_t k = 0; k < d.n_steps; ++k) {
-      k_eng_neuron<KIND, HARD, USE_REF><<<grid, kEngThreads, smem, s>>>(d, k, sg);
-      k_eng_scatter<<<sms * 8, kEngThreads, 0, s>>>(d, k);
+      const StepIdx si = step_idx(d.t0 + k, d.n_bins, d.hist_len);
+      k_eng_neuron<KIND, HARD, USE_REF, S><<<grid, kEngThreads, 0, s>>>(d, k, si);
+      k_eng_scatter<<<sms * 8, kEngThreads, 0, s>>>(d, k, si);
     }
     BT_CHECK_LAUNCH("k_eng_neuron/k_eng_scatter");
     if (d.n_steps > 0) {
-      k_eng_scatter_final<<<int(ceil_div(d.batch * n, 256)), 256, 0, s>>>(d);
+      const StepIdx si = step_idx(d.t0 + d.n_steps - 1, d.n_bins, d.hist_len);
+      k_eng_scatter_final<<<int(ceil_div(d.batch * n, 256)), 256, 0, s>>>(d, si);
       BT_CHECK_LAUNCH("k_eng_scatter_final");
     }
+  } else if (d.mode == BT_MODE_PULL) {
+    // Words of the sample mask per warp: the descriptor may ask for 2 or 4
+    // (fewer warps, one vector mask load per edge); by default every warp
+    // takes one 32-sample word, which gives the most warps in flight.
+    const int mw = mask_stride(d.batch);
+    int MWT = d.pull_words_per_warp > 0 ? d.pull_words_per_warp : 1;
+    if (MWT != 1 && MWT != mw) MWT = 1;
+    const int split = MWT < mw ? 1 : 0;
+    const int64_t warps = ceil_div(n, 32) * (split ? mw : 1);
+    const int grid = int(ceil_div(warps, kPullWarps));
+    const size_t smem = sizeof(float) * kPullWarps * MWT * 32 * 32;
+#define BT_PULL_LAUNCH(M)                                                                                        \
+  do {                                                                                                           \
+    auto kern = k_eng_pull<KIND, HARD, USE_REF, false, M>;                                                      \
+    auto kfin = k_eng_pull<KIND, HARD, USE_REF, true, M>;                                                       \
+    if (smem > 48 * 1024 &&                                                                                      \
+        (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||    \
+         cudaFuncSetAttribute(kfin, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess))     \
+      return bt_set_error(BT_ERR_CUDA, "shared memory request of %zu bytes refused", smem);                     \
+    for (int64_t k = 0; k < d.n_steps; ++k)                                                                     \
+      kern<<<grid, kPullWarps * 32, smem, s>>>(d, k, split, step_idx(d.t0 + k, d.n_bins, d.hist_len));          \
+    BT_CHECK_LAUNCH("k_eng_pull");                                                                               \
+    kfin<<<grid, kPullWarps * 32, smem, s>>>(d, d.n_steps - 1, split,                                           \
+                                             step_idx(d.t0 + d.n_steps - 1, d.n_bins, d.hist_len));              \
+    BT_CHECK_LAUNCH("k_eng_pull final");                                                                         \
+  } while (0)
+    if (d.n_steps > 0) {
+      if (MWT == 1) BT_PULL_LAUNCH(1);
+      else if (MWT == 2) BT_PULL_LAUNCH(2);
+      else BT_PULL_LAUNCH(4);
+    }
+#undef BT_PULL_LAUNCH
   } else {
     const int grid = int(ceil_div(n, 32));
     const size_t smem = sizeof(uint32_t) * size_t(d.batch);
     BT_CHECK_ARG(smem <= 48 * 1024, "batch too large for the gather engine");
     for (int64_t k = 0; k < d.n_steps; ++k)
-      k_eng_gather<KIND, HARD, USE_REF><<<grid, 1024, smem, s>>>(d, k);
+      k_eng_gather<KIND, HARD, USE_REF><<<grid, 1024, smem, s>>>(d, k, step_idx(d.t0 + k, d.n_bins, d.hist_len));
     BT_CHECK_LAUNCH("k_eng_gather");
     if (d.n_steps > 0) {
-      k_eng_gather_final<<<grid, 1024, 0, s>>>(d);
+      k_eng_gather_final<<<grid, 1024, 0, s>>>(d, step_idx(d.t0 + d.n_steps - 1, d.n_bins, d.hist_len));
       BT_CHECK_LAUNCH("k_eng_gather_final");
     }
   }
@@ -537,14 +893,15 @@ extern "C" int bt_input_project(int64_t rows, int64_t c_in, int64_t n, const flo
   if (rows == 0 || n == 0) return BT_OK;
   BT_CHECK_ARG(xin && w_t && out && work, "null pointer");
   BT_CHECK_ARG(rows * c_in < (int64_t(1) << 40), "too large");
+  BT_CHECK_ARG((reinterpret_cast<uintptr_t>(work) & 7) == 0, "work must be 8-byte aligned");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  int32_t* cnt = work;
-  int32_t* idx = work + rows;
-  k_row_nonzeros<<<int(ceil_div(rows * 32, 256)), 256, 0, s>>>(rows, c_in, xin, cnt, idx);
-  BT_CHECK_LAUNCH("k_row_nonzeros");
-  dim3 grid(unsigned(ceil_div(rows, kProjRows)), unsigned(ceil_div(n, 256)));
-  BT_CHECK_ARG(grid.y < 65536, "n too large for the projection grid");
-  k_input_project<<<grid, 256, 0, s>>>(rows, c_in, n, xin, w_t, bias, cnt, idx, out);
+  int2* pairs = reinterpret_cast<int2*>(work);
+  int32_t* cnt = work + 2 * rows * c_in;
+  k_row_pairs<<<int(ceil_div(rows * 32, 256)), 256, 0, s>>>(rows, c_in, xin, cnt, pairs);
+  BT_CHECK_LAUNCH("k_row_pairs");
+  dim3 grid(unsigned(ceil_div(rows, kProjRows)), unsigned(ceil_div(n, 256 * kProjNPT)));
+  BT_CHECK_ARG(grid.y < 65536 && grid.x < (1u << 31), "projection grid too large");
+  k_input_project<<<grid, 256, 0, s>>>(rows, c_in, n, w_t, bias, cnt, pairs, out);
   BT_CHECK_LAUNCH("k_input_project");
   return BT_OK;
 }
@@ -555,6 +912,31 @@ extern "C" int bt_bits_to_float(int64_t rows, int64_t n, const uint32_t* bits, f
   BT_CHECK_ARG(bits && out, "null pointer");
   k_bits_to_float<<<int(ceil_div(rows * n, 256)), 256, 0, static_cast<cudaStream_t>(stream)>>>(rows, n, bits, out);
   BT_CHECK_LAUNCH("k_bits_to_float");
+  return BT_OK;
+}
+
+extern "C" int bt_mask_stride(int64_t batch) { return batch > 0 ? mask_stride(batch) : 0; }
+
+extern "C" int64_t bt_engine_work_words(int64_t n, int64_t batch) {
+  return (n > 0 && batch > 0) ? scatter_work_words(n, batch) : 0;
+}
+
+extern "C" int bt_float_to_masks(int64_t batch, int64_t n, const float* in, uint32_t* masks, void* stream) {
+  BT_CHECK_ARG(batch >= 0 && n >= 0, "negative size");
+  if (batch * n == 0) return BT_OK;
+  BT_CHECK_ARG(in && masks, "null pointer");
+  const int64_t total = n * mask_stride(batch);
+  k_float_to_masks<<<int(ceil_div(total, 256)), 256, 0, static_cast<cudaStream_t>(stream)>>>(batch, n, in, masks);
+  BT_CHECK_LAUNCH("k_float_to_masks");
+  return BT_OK;
+}
+
+extern "C" int bt_masks_to_float(int64_t batch, int64_t n, const uint32_t* masks, float* out, void* stream) {
+  BT_CHECK_ARG(batch >= 0 && n >= 0, "negative size");
+  if (batch * n == 0) return BT_OK;
+  BT_CHECK_ARG(out && masks, "null pointer");
+  k_masks_to_float<<<int(ceil_div(batch * n, 256)), 256, 0, static_cast<cudaStream_t>(stream)>>>(batch, n, masks, out);
+  BT_CHECK_LAUNCH("k_masks_to_float");
   return BT_OK;
 }
 

@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "../../include/btorch_b200.h"
@@ -73,6 +74,50 @@ extern "C" int bt_layout_build(int64_t nnz, const int64_t* post, const int64_t* 
     const int32_t pos = cursor[size_t(j)]++;
     csr_dst[pos] = uint32_t(post[e]) | (uint32_t(s % n_bins) << BT_BIN_SHIFT);
     csr_perm[pos] = int32_t(e);
+  }
+  return BT_OK;
+}
+
+// Sliced post-major view (SELL-32): posts are grouped in slices of 32; slice s
+// holds rows [sl_ptr[s], sl_ptr[s+1]), row r storing entry k of each of its 32
+// posts at [32 r + lane] -- so a warp with lane = post reads one row with one
+// coalesced 128-byte load, and walks each post's in-edges in canonical order.
+// Short posts are padded with `sentinel` (a presynaptic id that never spikes)
+// and perm -1 (weight 0).
+extern "C" int bt_layout_slices(int64_t n_post, const int32_t* csc_ptr, const uint32_t* csc_src, uint32_t sentinel,
+                                int64_t* sl_ptr, uint32_t* sl_src, int32_t* sl_perm, int64_t capacity_rows,
+                                int64_t* rows_out) {
+  g_error[0] = 0;
+  if (n_post < 0 || !csc_ptr || !sl_ptr || !rows_out) return bt_set_error(BT_ERR_INVALID, "null argument");
+  const int64_t n_slices = (n_post + 31) / 32;
+  int64_t rows = 0;
+  sl_ptr[0] = 0;
+  for (int64_t s = 0; s < n_slices; ++s) {
+    int32_t len = 0;
+    for (int64_t p = s * 32; p < std::min<int64_t>(n_post, s * 32 + 32); ++p)
+      len = std::max(len, csc_ptr[p + 1] - csc_ptr[p]);
+    rows += len;
+    sl_ptr[s + 1] = rows;
+  }
+  *rows_out = rows;
+  if (!sl_src || !sl_perm) return BT_OK;  // size query
+  if (capacity_rows < rows) return bt_set_error(BT_ERR_INVALID, "slice capacity %lld < %lld rows",
+                                                (long long)capacity_rows, (long long)rows);
+  for (int64_t s = 0; s < n_slices; ++s) {
+    for (int64_t r = sl_ptr[s]; r < sl_ptr[s + 1]; ++r) {
+      const int64_t k = r - sl_ptr[s];
+      for (int lane = 0; lane < 32; ++lane) {
+        const int64_t p = s * 32 + lane;
+        const int64_t at = r * 32 + lane;
+        if (p < n_post && csc_ptr[p] + k < csc_ptr[p + 1]) {
+          sl_src[at] = csc_src[csc_ptr[p] + k];
+          sl_perm[at] = csc_ptr[p] + int32_t(k);
+        } else {
+          sl_src[at] = sentinel;
+          sl_perm[at] = -1;
+        }
+      }
+    }
   }
   return BT_OK;
 }

@@ -28,40 +28,93 @@ __device__ __forceinline__ float relu_keep_nan(float x) { return (x != x) ? x : 
 
 __device__ __forceinline__ float sigmoidf_dev(float x) { return 1.0f / (1.0f + expf(-x)); }
 
-// One BaseNode.single_step_forward for neuron i with input current I.
-// v, ref, gk are updated in place.  KIND/HARD/USE_REF may be template
-// constants (engine) or runtime values (single-step kernel).
-template <int KIND, bool HARD, bool USE_REF>
-__device__ __forceinline__ NeuronOut neuron_update(const bt_neuron_desc& d, int64_t i, float I, float& v, float& ref,
-                                                   float& gk) {
-  const float vth = ld(d.v_threshold, i);
-  const float vr = ld(d.v_reset, i);
-  const float cm = ld(d.c_m, i);
-  const float dt = d.dt;
+// Exact reciprocal of c if c is a power of two (then x / c == x * (1/c) for
+// every x: both are the correctly rounded value of the same real number), 0
+// otherwise.  Lets the kernels replace IEEE division by a multiply whenever a
+// divisor such as c_m = 1 or (v_threshold - v_reset) = 1 allows it.
+__device__ __forceinline__ float pow2_recip(float c) {
+  // positive normal power of two: zero mantissa, biased exponent e in [1, 253]
+  // so that 1/c = 2^(127 - (e - 127)) has biased exponent 254 - e in [1, 253]
+  const uint32_t u = __float_as_uint(c);
+  const uint32_t e = u >> 23;  // sign bit included: negative c gives e > 255
+  return ((u & 0x7fffffu) == 0u && e >= 1u && e <= 253u) ? __uint_as_float((254u - e) << 23) : 0.0f;
+}
+
+// x / c with the reference's rounding; rc = pow2_recip(c).
+__device__ __forceinline__ float divc(float x, float c, float rc) { return rc != 0.0f ? mul(x, rc) : div(x, c); }
+
+// The parameters of one neuron, read once into registers (the kernels update
+// many samples of the same neuron with them).
+struct NeuronParams {
+  float vth, vr, cm, den, dt;
+  float tau;                           // LIF
+  float tau_ref;
+  float ngl, El, Ek, dgk, tau_a, cgk;  // ALIF: -g_leak, E_leak, E_k, dg_k, tau_adapt, coef_gk
+  float sg_alpha;
+  float r_cm, r_den, r_tau, r_tau_a;   // pow2_recip of the divisors (0: divide)
+  int spiking;
+};
+
+template <int KIND, bool USE_REF>
+__device__ __forceinline__ NeuronParams load_params(const bt_neuron_desc& d, int64_t i) {
+  NeuronParams p;
+  p.vth = ld(d.v_threshold, i);
+  p.vr = ld(d.v_reset, i);
+  p.cm = ld(d.c_m, i);
+  p.den = sub(p.vth, p.vr);  // (v_threshold - v_reset), one torch op in the reference
+  p.dt = d.dt;
+  p.sg_alpha = d.sg_alpha;
+  p.spiking = d.spiking;
+  p.tau = KIND == BT_NEURON_LIF ? ld(d.tau, i) : 0.0f;
+  p.tau_ref = USE_REF ? ld(d.tau_ref, i) : 0.0f;
+  if (KIND == BT_NEURON_ALIF) {
+    p.ngl = -ld(d.g_leak, i);
+    p.El = ld(d.E_leak, i);
+    p.Ek = ld(d.E_k, i);
+    p.dgk = ld(d.dg_k, i);
+    p.tau_a = ld(d.tau_adapt, i);
+    p.cgk = ld(d.coef_gk, i);
+  } else {
+    p.ngl = p.El = p.Ek = p.dgk = p.tau_a = p.cgk = 0.0f;
+  }
+  p.r_cm = pow2_recip(p.cm);
+  p.r_den = pow2_recip(p.den);
+  p.r_tau = pow2_recip(p.tau);
+  p.r_tau_a = pow2_recip(p.tau_a);
+  return p;
+}
+
+// One BaseNode.single_step_forward with input current I.  v, ref, gk are
+// updated in place.  SPIKING selects the Heaviside forward at compile time
+// (the fused engine); otherwise pr.spiking decides at run time.
+template <int KIND, bool HARD, bool USE_REF, bool SPIKING = false>
+__device__ __forceinline__ NeuronOut neuron_update(const NeuronParams& pr, float I, float& v, float& ref, float& gk) {
+  const float dt = pr.dt;
   float v1;
   if (KIND == BT_NEURON_LIF) {
     // euler_step(dV): v + dt * ((-(v - v_reset)) / tau + x / c_m)
-    const float tau = ld(d.tau, i);
-    v1 = add(v, mul(dt, add(div(-sub(v, vr), tau), div(I, cm))));
+    v1 = add(v, mul(dt, add(divc(-sub(v, pr.vr), pr.tau, pr.r_tau), divc(I, pr.cm, pr.r_cm))));
   } else {
     // exp_euler_step(dV): derivative = ((-g_leak)(v - E_leak) + (-g_k)(v - E_k) + x) / c_m
     //                     linear     = ((-g_leak) - g_k) / c_m
-    const float ngl = -ld(d.g_leak, i);
-    const float leak = mul(ngl, sub(v, ld(d.E_leak, i)));
-    const float adapt = mul(-gk, sub(v, ld(d.E_k, i)));
-    const float deriv = div(add(add(leak, adapt), I), cm);
-    const float lin = div(sub(ngl, gk), cm);
+    const float leak = mul(pr.ngl, sub(v, pr.El));
+    const float adapt = mul(-gk, sub(v, pr.Ek));
+    const float deriv = divc(add(add(leak, adapt), I), pr.cm, pr.r_cm);
+    const float lin = divc(sub(pr.ngl, gk), pr.cm, pr.r_cm);
     const float coef = div(expm1f(mul(dt, lin)), lin);
     v1 = add(v, mul(coef, deriv));
     // neuronal_adaptation: g_k + coef_gk * ((-g_k) / tau_adapt)
-    gk = add(gk, mul(ld(d.coef_gk, i), div(-gk, ld(d.tau_adapt, i))));
+    gk = add(gk, mul(pr.cgk, divc(-gk, pr.tau_a, pr.r_tau_a)));
   }
   NeuronOut o;
   o.v_charged = v1;
   // neuronal_fire: surrogate((v - v_th) / (v_th - v_reset)) * (refractory == 0)
-  const float den = sub(vth, vr);
-  o.u = div(sub(v1, vth), den);
-  float s = d.spiking ? (o.u >= 0.0f ? 1.0f : 0.0f) : sigmoidf_dev(mul(d.sg_alpha, o.u));
+  o.u = divc(sub(v1, pr.vth), pr.den, pr.r_den);
+  float s;
+  if (SPIKING || pr.spiking)
+    s = o.u >= 0.0f ? 1.0f : 0.0f;
+  else
+    s = sigmoidf_dev(mul(pr.sg_alpha, o.u));
   o.mask = 1.0f;
   if (USE_REF) {
     o.mask = (ref == 0.0f) ? 1.0f : 0.0f;
@@ -70,17 +123,31 @@ __device__ __forceinline__ NeuronOut neuron_update(const bt_neuron_desc& d, int6
   o.spike = s;
   // neuronal_reset
   if (HARD)
-    v = sub(v1, mul(sub(v1, vr), s));
+    v = sub(v1, mul(sub(v1, pr.vr), s));
   else
-    v = sub(v1, mul(den, s));
-  if (KIND == BT_NEURON_ALIF) gk = add(gk, mul(ld(d.dg_k, i), s));
-  if (USE_REF) ref = relu_keep_nan(sub(add(ref, mul(s, ld(d.tau_ref, i))), dt));
+    v = sub(v1, mul(pr.den, s));
+  if (KIND == BT_NEURON_ALIF) gk = add(gk, mul(pr.dgk, s));
+  if (USE_REF) ref = relu_keep_nan(sub(add(ref, mul(s, pr.tau_ref)), dt));
   return o;
 }
 
+// Convenience overload: parameters read for neuron i.
+template <int KIND, bool HARD, bool USE_REF>
+__device__ __forceinline__ NeuronOut neuron_update(const bt_neuron_desc& d, int64_t i, float I, float& v, float& ref,
+                                                   float& gk) {
+  const NeuronParams pr = load_params<KIND, USE_REF>(d, i);
+  return neuron_update<KIND, HARD, USE_REF>(pr, I, v, ref, gk);
+}
+
 // ExponentialPSC.conductance_charge: psc + coef * ((-psc) / tau_syn)
+__device__ __forceinline__ float psc_decay(float coef, float tau, float rtau, float p) {
+  return add(p, mul(coef, divc(-p, tau, rtau)));
+}
+__device__ __forceinline__ float psc_decay(float coef, float tau, float p) {
+  return psc_decay(coef, tau, pow2_recip(tau), p);
+}
 __device__ __forceinline__ float psc_decay(const bt_param& coef, const bt_param& tau, int64_t i, float p) {
-  return add(p, mul(ld(coef, i), div(-p, ld(tau, i))));
+  return psc_decay(ld(coef, i), ld(tau, i), p);
 }
 
 }  // namespace bt

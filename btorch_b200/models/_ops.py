@@ -69,6 +69,43 @@ def build_layout(indices: torch.Tensor, n_pre: int, n_out: int, n_bins: int = 1)
                         csr_perm=torch.from_numpy(csr_perm[:nnz].astype(np.int64)))
 
 
+@dataclass
+class SliceLayout:
+    """SELL-32 view of a layout's CSC (see bt_layout_slices)."""
+
+    rows: int
+    sl_ptr: torch.Tensor    # int64 [ceil(n/32) + 1]
+    sl_src: torch.Tensor    # int32 (uint32 bits) [rows * 32]
+    sl_index: torch.Tensor  # int64 [rows * 32]: canonical edge index, nnz on padding
+
+
+def build_slices(layout: SparseLayout, device) -> SliceLayout:
+    n = layout.n_out
+    csc_ptr = layout.csc_ptr.cpu().numpy()
+    csc_src = layout.csc_src.cpu().numpy().view(np.uint32)
+    n_sl = (n + 31) // 32
+    sl_ptr = np.zeros(n_sl + 1, np.int64)
+    rows = np.zeros(1, np.int64)
+    lib = L.lib()
+    L.check(lib.bt_layout_slices(n, csc_ptr.ctypes.data, csc_src.ctypes.data, layout.n_pre, sl_ptr.ctypes.data,
+                                 None, None, 0, rows.ctypes.data), "bt_layout_slices")
+    R = int(rows[0])
+    sl_src = np.zeros(max(1, R * 32), np.uint32)
+    sl_perm = np.zeros(max(1, R * 32), np.int32)
+    L.check(lib.bt_layout_slices(n, csc_ptr.ctypes.data, csc_src.ctypes.data, layout.n_pre, sl_ptr.ctypes.data,
+                                 sl_src.ctypes.data, sl_perm.ctypes.data, R, rows.ctypes.data), "bt_layout_slices")
+    idx = sl_perm.astype(np.int64)
+    idx[idx < 0] = layout.nnz
+    return SliceLayout(rows=R, sl_ptr=torch.from_numpy(sl_ptr).to(device),
+                       sl_src=torch.from_numpy(sl_src.view(np.int32)).to(device),
+                       sl_index=torch.from_numpy(idx).to(device))
+
+
+def pack_slice_weights(sl: SliceLayout, w_canonical: torch.Tensor) -> torch.Tensor:
+    w_ext = torch.cat([w_canonical.detach().float().reshape(-1), w_canonical.new_zeros(1, dtype=torch.float32)])
+    return w_ext.index_select(0, sl.sl_index).contiguous()
+
+
 def pack_csr_weights(layout: SparseLayout, w_canonical: torch.Tensor) -> torch.Tensor:
     """Weights in CSR order, padded like csr_dst (zeros in the padding)."""
     out = torch.zeros(pad4(layout.nnz), device=w_canonical.device, dtype=torch.float32)
@@ -147,23 +184,25 @@ def sparse_mm(x2d, w_canon, layout, direction, w_csr=None):
 
 # ----------------------------------------------------------- neuron step --
 
-_coef_cache: dict = {}
-
-
-def exp_euler_coef(tau: torch.Tensor, dt: float) -> torch.Tensor:
+def exp_euler_coef(tau: torch.Tensor, dt: float, owner=None, name: str = "") -> torch.Tensor:
     """expm1(dt * lin) / lin with lin = -1.0 / tau, evaluated by torch on the
     CPU exactly as the reference's exp_euler_step does (ode.py:50), so the
-    device sees the reference's fp32 value."""
-    key = (tau.data_ptr(), getattr(tau, "_version", 0), float(dt), tuple(tau.shape), tau.device)
-    hit = _coef_cache.get(key)
-    if hit is not None:
-        return hit
+    device sees the reference's fp32 value.
+
+    With an `owner` module the result is cached on that module, keyed by dt and
+    the identity and version of its `tau` tensor, so repeated steps do not copy
+    the time constant back to the host."""
+    key = (float(dt), tau.data_ptr(), getattr(tau, "_version", 0), tuple(tau.shape), str(tau.device))
+    slot = f"_bt_coef_{name}"
+    if owner is not None:
+        hit = owner.__dict__.get(slot)
+        if hit is not None and hit[0] == key:
+            return hit[1]
     t_cpu = tau.detach().to("cpu", torch.float32)
     lin = -1.0 / t_cpu
     coef = (torch.expm1(dt * lin) / lin).reshape(-1).contiguous().to(tau.device)
-    if len(_coef_cache) > 256:
-        _coef_cache.clear()
-    _coef_cache[key] = coef
+    if owner is not None:
+        owner.__dict__[slot] = (key, coef)
     return coef
 
 
@@ -203,7 +242,7 @@ def neuron_desc(node, dt: float):
         d.kind = L.BT_NEURON_ALIF
         d.g_leak, d.E_leak, d.E_k, d.dg_k = P(node.g_leak), P(node.E_leak), P(node.E_k), P(node.dg_k)
         d.tau_adapt = P(node.tau_adapt)
-        d.coef_gk = P(exp_euler_coef(node.tau_adapt, dt))
+        d.coef_gk = P(exp_euler_coef(node.tau_adapt, dt, owner=node, name="gk"))
     elif isinstance(node, LIF):
         d.kind = L.BT_NEURON_LIF
         d.tau = P(node.tau)

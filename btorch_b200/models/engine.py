@@ -20,7 +20,7 @@ import torch.nn as nn
 
 from .. import _lib as L
 from . import environ
-from ._ops import exp_euler_coef, neuron_desc, pack_csr_weights
+from ._ops import build_slices, neuron_desc, pack_csr_weights, pack_slice_weights
 from .functional import named_hidden_states
 from .history import SpikeHistory
 from .linear import BaseSparseConn
@@ -166,7 +166,11 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     keep += [coef, tau]
     desc.psc_coef, desc.psc_tau = L.param(coef), L.param(tau)
     direction = conn.direction(B)
-    desc.mode = L.BT_MODE_GATHER if direction == "gather" else L.BT_MODE_SCATTER
+    if direction == "gather":
+        # ordered pull: warp per post for tiny batches, sliced lane-per-post otherwise
+        desc.mode = L.BT_MODE_PULL if B >= conn.sparse_config.pull_min_batch else L.BT_MODE_GATHER
+    else:
+        desc.mode = L.BT_MODE_SCATTER
     lay = conn.engine_layout(plan.n_bins, plan.uniform_delay, dev)
     w = conn._get_effective_weight().detach().float().contiguous()
     keep.append(w)
@@ -179,10 +183,24 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         keep.append(w_csr)
         desc.csr_ptr, desc.csr_dst, desc.csr_w = lay.csr_ptr.data_ptr(), lay.csr_dst.data_ptr(), w_csr.data_ptr()
         ring = torch.zeros((plan.n_bins, B, n), device=dev, dtype=torch.float32)
-        mw = (B + 31) // 32
-        work = torch.empty(4 + 2 * n * (1 + mw), device=dev, dtype=torch.int32)
+        work = torch.empty(L.lib().bt_engine_work_words(n, B), device=dev, dtype=torch.int32)
         keep += [ring, work]
         desc.ring, desc.work = ring.data_ptr(), work.data_ptr()
+    mw = (B + 31) // 32
+    if desc.mode == L.BT_MODE_PULL:
+        sl = getattr(lay, "slices", None)
+        if sl is None:
+            sl = build_slices(lay, dev)
+            lay.slices = sl
+        sl_w = pack_slice_weights(sl, w)
+        masks = torch.zeros((H, n + 1, L.lib().bt_mask_stride(B)), device=dev, dtype=torch.int32)
+        keep += [sl_w, masks]
+        desc.sl_ptr, desc.sl_src, desc.sl_w = sl.sl_ptr.data_ptr(), sl.sl_src.data_ptr(), sl_w.data_ptr()
+        desc.masks = masks.data_ptr()
+    if stats:
+        outdeg = (lay.csr_ptr[1:] - lay.csr_ptr[:-1]).to(torch.int32).contiguous()
+        keep.append(outdeg)
+        desc.outdeg = outdeg.data_ptr()
     desc.v, desc.psc = v.data_ptr(), psc.data_ptr()
     desc.refractory = L.ptr(ref)
     desc.g_k = L.ptr(gk)
@@ -195,10 +213,16 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     want_hist_trace = "history" in plan.paths.values()
     if hist_depth:
         block = plan.history.recent_block(hist_depth).float().contiguous()  # [Dh, B, n], d steps ago
-        bits = torch.empty((hist_depth, B, words), device=dev, dtype=torch.int32)
-        L.check(L.lib().bt_float_to_bits(hist_depth * B, n, block.data_ptr(), bits.data_ptr(), s), "bt_float_to_bits")
-        for d in range(hist_depth):
-            hist[(t0 - 1 - d) % H] = bits[d]
+        if desc.mode == L.BT_MODE_PULL:
+            for d in range(hist_depth):
+                L.check(L.lib().bt_float_to_masks(B, n, block[d].data_ptr(), masks[(t0 - 1 - d) % H].data_ptr(), s),
+                        "bt_float_to_masks")
+        else:
+            bits = torch.empty((hist_depth, B, words), device=dev, dtype=torch.int32)
+            L.check(L.lib().bt_float_to_bits(hist_depth * B, n, block.data_ptr(), bits.data_ptr(), s),
+                    "bt_float_to_bits")
+            for d in range(hist_depth):
+                hist[(t0 - 1 - d) % H] = bits[d]
     desc.t0 = t0
     if desc.mode == L.BT_MODE_SCATTER and plan.n_bins > 1:
         desc.n_steps = 1
@@ -235,7 +259,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             c_in = x3.shape[-1]
             xc = x3[k0:k0 + kc].reshape(kc * B, c_in).float().contiguous()
             xp = torch.empty((kc, B, n), device=dev, dtype=torch.float32)
-            pw = torch.empty(kc * B * (c_in + 1), device=dev, dtype=torch.int32)
+            pw = torch.empty(kc * B * (2 * c_in + 1), device=dev, dtype=torch.int32)
             e0 = _ev() if profile is not None else None
             L.check(L.lib().bt_input_project(kc * B, c_in, n, xc.data_ptr(), w_t.data_ptr(), L.ptr(bias),
                                              xp.data_ptr(), pw.data_ptr(), s), "bt_input_project")
@@ -270,9 +294,15 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     # write the spike history back into the module (last Dh spikes)
     t_end = t0 + T
     if hist_depth:
-        sel = torch.stack([hist[(t_end - 1 - d) % H] for d in range(hist_depth)]).contiguous()
         block = torch.empty((hist_depth, B, n), device=dev, dtype=torch.float32)
-        L.check(L.lib().bt_bits_to_float(hist_depth * B, n, sel.data_ptr(), block.data_ptr(), s), "bt_bits_to_float")
+        if desc.mode == L.BT_MODE_PULL:
+            for d in range(hist_depth):
+                L.check(L.lib().bt_masks_to_float(B, n, masks[(t_end - 1 - d) % H].data_ptr(), block[d].data_ptr(), s),
+                        "bt_masks_to_float")
+        else:
+            sel = torch.stack([hist[(t_end - 1 - d) % H] for d in range(hist_depth)]).contiguous()
+            L.check(L.lib().bt_bits_to_float(hist_depth * B, n, sel.data_ptr(), block.data_ptr(), s),
+                    "bt_bits_to_float")
         init_block = plan.history.recent_block(hist_depth).clone() if want_hist_trace else None
         plan.history.store_recent_block(block, T)
     if plan.hetero:
@@ -288,7 +318,8 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         else:
             states[key] = traces[kind].view(T, *batch_shape, *_nshape(plan, key))
     rnn.last_engine_stats = stat_t
-    rnn.last_engine_direction = direction
+    rnn.last_engine_direction = {L.BT_MODE_SCATTER: "scatter", L.BT_MODE_GATHER: "gather",
+                                 L.BT_MODE_PULL: "pull"}[desc.mode]
     rnn.last_engine_launches = launches
     if z is not None:
         z = z.view(T, *batch_shape, *neuron.n_neuron)

@@ -59,7 +59,7 @@ class ExponentialPSC(BasePSC):
         """(coef, tau) device fp32 vectors for the kernels; coef is rounded on
         the host exactly as the reference computes expm1(dt*lin)/lin."""
         tau = self.tau_syn.detach().float().reshape(-1).contiguous()
-        return exp_euler_coef(self.tau_syn.float(), dt), tau
+        return exp_euler_coef(self.tau_syn, dt, owner=self, name="psc"), tau
 
     def conductance_charge(self):
         coef, tau = self.coefficients(environ.get("dt"))

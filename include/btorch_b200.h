@@ -68,6 +68,16 @@ BT_API int bt_abi_version(void);
 /* and BaseSparseConn._rebuild_triton_layout  linear.py:329-349.        */
 /* ------------------------------------------------------------------ */
 
+/* SELL-32 view of the CSC for BT_MODE_PULL: slice s = posts [32 s, 32 s + 32)
+ * holds rows [sl_ptr[s], sl_ptr[s + 1]); row r stores the k-th in-edge of each
+ * of its posts at [32 r + lane] (k = r - sl_ptr[s]); shorter posts are padded
+ * with src = sentinel (a neuron id that never spikes) and perm = -1.
+ * sl_src / sl_perm NULL: only fill sl_ptr and *rows_out (size query). */
+BT_API int bt_layout_slices(int64_t n_post, const int32_t* csc_ptr,
+                            const uint32_t* csc_src, uint32_t sentinel,
+                            int64_t* sl_ptr, uint32_t* sl_src, int32_t* sl_perm,
+                            int64_t capacity_rows, int64_t* rows_out);
+
 /* Build CSC and CSR views of a canonical COO matrix in one O(nnz) pass.
  * post[e], src[e]: canonical COO (sorted by (post, src)); src is the
  * delay-expanded row index pre*n_bins + bin (n_bins = 1 for a plain
@@ -225,7 +235,9 @@ BT_API int bt_psc_step(int64_t batch, int64_t n, bt_param coef, bt_param tau_syn
 /* ------------------------------------------------------------------ */
 
 #define BT_MODE_SCATTER 0  /* push: 2 launches per step, L2 fp32 reductions */
-#define BT_MODE_GATHER 1   /* pull: 1 launch per step, ordered, bit-exact   */
+#define BT_MODE_GATHER 1   /* pull, warp per post: 1 launch per step, ordered, bit-exact */
+#define BT_MODE_PULL 2     /* pull over SELL-32 slices, lane per post, sample masks:
+                              1 launch per step, ordered, bit-exact, for batches */
 
 typedef struct bt_engine_desc {
   /* sizes */
@@ -263,10 +275,27 @@ typedef struct bt_engine_desc {
   float* ref_trace;       /* [n_steps][batch][n] refractory after each step */
   float* gk_trace;        /* [n_steps][batch][n] g_k after each step (ALIF) */
 
+  /* sliced post-major view and sample masks (pull mode) */
+  const int64_t* sl_ptr;  /* [ceil(n/32) + 1] first row of each 32-post slice */
+  const uint32_t* sl_src; /* [rows * 32] pre | bin << 25, pre = n on padding */
+  const float* sl_w;      /* [rows * 32] weights, 0 on padding */
+  uint32_t* masks;        /* [hist_len][n + 1][S] spikes of each neuron by sample (bit l
+                             of word q = sample 32 q + l), slot = step mod hist_len,
+                             row n stays 0; S = bt_mask_stride(batch) */
+  const int32_t* outdeg;  /* [n] out-degrees, for the stats of pull mode (may be NULL) */
+  int32_t pull_words_per_warp; /* pull mode: 32-sample mask words one warp covers:
+                                  0 or 1 = one word per warp (default), or the whole
+                                  bt_mask_stride(batch) when that is 2 or 4 */
+  int32_t pad1_;
+
   /* scratch (scatter mode) */
-  int32_t* work;          /* 4 + 2 * n * (1 + mask_words) int32 */
+  int32_t* work;          /* bt_engine_work_words(n, batch) int32; the engine clears it
+                             at the start of every call */
   int64_t* stats;         /* [n_steps][4]: active union, events, edges, 0; may be NULL */
 } bt_engine_desc;
+
+/* Scratch words (int32) the scatter mode needs in bt_engine_desc.work. */
+BT_API int64_t bt_engine_work_words(int64_t n, int64_t batch);
 
 /* Run n_steps recurrent steps.  Per step: I = psc + x; neuron update;
  * psc = psc + coef*((-psc)/tau) + W z (z through the delay ring). */
@@ -282,7 +311,8 @@ BT_API int bt_engine_ring_from_history(const bt_engine_desc* d, void* stream);
 /* Input projection for DenseConn as neuron_inp_module (nn.Linear,
  * btorch/models/linear.py:163-228): out[r, i] = bias[i] + sum over nonzero
  * xin[r, c] (ascending c) of xin[r, c] * w_t[c, i].  rows = steps*batch;
- * w_t: [c_in, n] (transpose of the module weight); bias may be NULL. */
+ * w_t: [c_in, n] (transpose of the module weight); bias may be NULL.
+ * work: scratch of rows * (2 * c_in + 1) int32, 8-byte aligned. */
 BT_API int bt_input_project(int64_t rows, int64_t c_in, int64_t n,
                      const float* xin, const float* w_t, const float* bias,
                      float* out, int32_t* work, void* stream);
@@ -291,6 +321,17 @@ BT_API int bt_input_project(int64_t rows, int64_t c_in, int64_t n,
  * bit i%32 of word i/32 is neuron i). */
 BT_API int bt_bits_to_float(int64_t rows, int64_t n, const uint32_t* bits,
                      float* out, void* stream);
+
+/* Words per neuron of the pull engine's sample masks: ceil(batch/32) rounded
+ * up to 1, 2 or 4 (the kernel's vector load width), unchanged above 4. */
+BT_API int bt_mask_stride(int64_t batch);
+
+/* [batch][n] fp32 <-> sample masks [n][bt_mask_stride(batch)] (bit l of word q
+ * set where sample 32 q + l is nonzero) -- the pull engine's history layout. */
+BT_API int bt_float_to_masks(int64_t batch, int64_t n, const float* in,
+                             uint32_t* masks, void* stream);
+BT_API int bt_masks_to_float(int64_t batch, int64_t n, const uint32_t* masks,
+                             float* out, void* stream);
 
 /* Pack fp32 rows [rows][n] into bitmaps (bit set where the value != 0). */
 BT_API int bt_float_to_bits(int64_t rows, int64_t n, const float* in,

@@ -78,7 +78,11 @@ def build_model(d: dict, device="cuda", direction="gather"):
     n = int(d["n"])
     n_bins = int(d["n_bins"])
     conn_m = sp.coo_array((d["w"], (d["src"], d["post"])), shape=(n * n_bins, n))
-    conn = SparseConn(conn_m, sparse_config={"direction": direction})
+    # "gather": ordered pull, warp per post; "pull": ordered pull, sliced lane per post
+    cfg = {"gather": {"direction": "gather", "pull_min_batch": 1 << 30},
+           "pull": {"direction": "gather", "pull_min_batch": 1},
+           "scatter": {"direction": "scatter"}}[direction]
+    conn = SparseConn(conn_m, sparse_config=cfg)
     tau_ref = float(d["tau_ref"]) if int(d["use_ref"]) else None
     if int(d["kind"]) == 0:
         neuron = LIF(n, v_threshold=float(d["vth"]), v_reset=float(d["vr"]), c_m=float(d["cm"]),

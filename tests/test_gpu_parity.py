@@ -95,7 +95,10 @@ def test_spmv_gather_deterministic_and_empty_input():
 BITWISE_LIF = ["lif_dyadic_soft", "lif_dyadic_input", "delayed_psc", "hetero_delay"]
 
 
-@pytest.mark.parametrize("direction", ["gather", "scatter"])
+MODES = ["gather", "pull", "scatter"]
+
+
+@pytest.mark.parametrize("direction", MODES)
 @pytest.mark.parametrize("name", BITWISE_LIF)
 def test_engine_bitwise_vs_reference_dyadic(name, direction):
     """Dyadic weights: spike rasters, traces and final state bit-identical to
@@ -110,13 +113,14 @@ def test_engine_bitwise_vs_reference_dyadic(name, direction):
     np.testing.assert_array_equal(out["v_final"].reshape(d["v_final"].shape), d["v_final"])
 
 
-def test_engine_gather_bitwise_vs_reference_nondyadic_recurrence():
+@pytest.mark.parametrize("direction", ["gather", "pull"])
+def test_engine_gather_bitwise_vs_reference_nondyadic_recurrence(direction):
     """Non-dyadic lognormal weights (C1-shaped): the ordered gather reproduces
     the reference's fmaf order, so with the same projected input the whole
     run is bit-identical.  The projected input comes from the oracle's ordered
     projection, which the CUDA projection matches bit for bit."""
     d = cases.load("lif_c1_small")
-    out = run_engine(d, "gather")
+    out = run_engine(d, direction)
     spec = cases.netspec(d)
     st = O.init_state(spec, int(d["batch"]))
     o = O.run(spec, st, cases.projected_input(d, use_reference_projection=False), want_v=True, want_psc=True)
@@ -146,7 +150,7 @@ def test_engine_scatter_nondyadic_close():
     np.testing.assert_allclose(s["v"][:k], g["v"][:k], rtol=1e-5, atol=1e-5)
 
 
-@pytest.mark.parametrize("direction", ["gather", "scatter"])
+@pytest.mark.parametrize("direction", MODES)
 def test_engine_alif_vs_reference(direction):
     d = cases.load("alif_exppsc")
     out = run_engine(d, direction)
@@ -159,7 +163,7 @@ def test_engine_alif_vs_reference(direction):
 
 
 @pytest.mark.parametrize("name", ["delayed_psc", "hetero_delay", "lif_dyadic_input"])
-@pytest.mark.parametrize("direction", ["gather", "scatter"])
+@pytest.mark.parametrize("direction", MODES)
 def test_engine_split_calls_equal_one_call(name, direction):
     """Two consecutive calls (state, delay history and pending currents carried
     in the modules) equal one call; chunked launches equal one chunk."""
@@ -176,7 +180,7 @@ def test_engine_split_calls_equal_one_call(name, direction):
     np.testing.assert_array_equal(rnn.neuron.v.cpu().numpy(), full["v_final"])
 
 
-@pytest.mark.parametrize("direction", ["gather", "scatter"])
+@pytest.mark.parametrize("direction", MODES)
 def test_engine_uneven_sample_lengths(direction):
     """A batch with per-sample lengths equals each sample run alone for its length."""
     d = cases.load("lif_dyadic_soft")
@@ -197,10 +201,12 @@ def test_engine_uneven_sample_lengths(direction):
         np.testing.assert_array_equal(v_final[b], stb.v[0])
 
 
-def test_modular_path_equals_fused_engine():
+@pytest.mark.parametrize("direction", ["gather", "pull"])
+def test_modular_path_equals_fused_engine(direction):
     """Stepping module by module (each module's own kernel) gives the same run."""
     d = cases.load("hetero_delay")
-    fused = run_engine(d, "gather")
+    fused = run_engine(d, direction)
+    assert fused["rnn"].last_engine_direction == direction
     rnn, psc_name = cases.build_model(d, DEV, "gather")
     rnn.fused = False
     with torch.no_grad(), environ.context(dt=1.0):
@@ -210,11 +216,12 @@ def test_modular_path_equals_fused_engine():
     np.testing.assert_array_equal(st["neuron.v"].cpu().numpy(), fused["v"])
 
 
-def test_engine_state_names_default_all_memories():
+@pytest.mark.parametrize("direction", MODES)
+def test_engine_state_names_default_all_memories(direction):
     """update_state_names=None returns every memory stacked over time, like the
     reference (including the delay history)."""
     d = cases.load("delayed_psc")
-    rnn, _ = cases.build_model(d, DEV, "gather")
+    rnn, _ = cases.build_model(d, DEV, direction)
     rnn.update_state_names = None
     rnn_m, _ = cases.build_model(d, DEV, "gather")
     rnn_m.update_state_names = None

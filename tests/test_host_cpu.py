@@ -22,7 +22,7 @@ ROOT = Path(__file__).resolve().parent.parent
 
 def declared_symbols():
     text = (ROOT / "include" / "btorch_b200.h").read_text()
-    return sorted(set(re.findall(r"BT_API\s+(?:const\s+char\*|int)\s+(bt_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"BT_API\s+(?:const\s+char\*|int64_t|int)\s+(bt_\w+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol():
