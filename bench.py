@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--ncu-window", type=int, default=None,
+                    help="profile only time steps [S, S+64) (S a multiple of 64) of one extra batch after "
+                         "the timed ones (cudaProfilerStart/Stop; use with ncu --profile-from-start off)")
     return ap.parse_args()
 
 
@@ -370,6 +373,21 @@ def main():
             line["e2e"] = {"value": ev / (e2e_ms * 1e-3), "unit": "events/s",
                            "h2d_bytes_per_step": int(x_host.numel() * 4),
                            "d2h_bytes_per_step": int(raster_host.numel() * 4)}
+    if args.ncu_window is not None:
+        w0 = args.ncu_window
+
+        def hook(k0):
+            if k0 == w0:
+                torch.cuda.synchronize()
+                torch.cuda.profiler.start()
+            elif k0 == w0 + 64:
+                torch.cuda.synchronize()
+                torch.cuda.profiler.stop()
+
+        reset_net(rnn, inplace=True)
+        with torch.inference_mode(), environ.context(dt=1.0):
+            rnn(x, sample_len=lens, spikes_out="bitmask", engine_chunk=64, engine_chunk_hook=hook)
+        torch.cuda.synchronize()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         S = args.cpu_sample_steps
         x_cpu = x[:S].cpu().numpy()

@@ -130,12 +130,15 @@ def _state2d(t: torch.Tensor, n: int) -> torch.Tensor:
 
 
 def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None = None,
-        chunk: int | None = None, spikes_out: str = "dense", stats: bool = False, profile: list | None = None):
+        chunk: int | None = None, spikes_out: str = "dense", stats: bool = False, profile: list | None = None,
+        chunk_hook=None):
     """Run T = x.shape[0] steps.  Returns (z [T, *batch, n] or bitmaps, states).
 
     profile: if a list, (kind, start_event, end_event) CUDA-event pairs are
     appended for every input-projection ("project") and recurrent-step
-    ("step") launch group, recorded on the launching stream."""
+    ("step") launch group, recorded on the launching stream.
+    chunk_hook: called as chunk_hook(k0) before the launches of the chunk
+    that starts at step k0 (e.g. to open a profiler window)."""
     launches = 0
 
     def _ev():
@@ -255,6 +258,8 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     K = int(chunk or DEFAULT_CHUNK)
     for k0 in range(0, T, K):
         kc = min(K, T - k0)
+        if chunk_hook is not None:
+            chunk_hook(k0)
         if inp is not None:
             c_in = x3.shape[-1]
             xc = x3[k0:k0 + kc].reshape(kc * B, c_in).float().contiguous()

@@ -158,7 +158,7 @@ class RecurrentNN(RecurrentNNAbstract):
 
     def multi_step_forward(self, *args, loop_args=None, sample_len=None, spikes_out: str = "dense",
                            engine_chunk: int | None = None, engine_stats: bool = False,
-                           engine_profile: list | None = None, **kwargs):
+                           engine_profile: list | None = None, engine_chunk_hook=None, **kwargs):
         """Run T = args[0].shape[0] steps.  Extensions over the reference:
         sample_len ([batch] steps per sample; later steps of a sample freeze its
         state and emit no spikes), spikes_out="bitmask" (return the spike raster
@@ -174,7 +174,8 @@ class RecurrentNN(RecurrentNNAbstract):
         if plan is not None:
             self.last_path = "fused"
             return _engine.run(plan, self, args[0], sample_len=sample_len, chunk=engine_chunk,
-                               spikes_out=spikes_out, stats=engine_stats, profile=engine_profile)
+                               spikes_out=spikes_out, stats=engine_stats, profile=engine_profile,
+                               chunk_hook=engine_chunk_hook)
         if sample_len is not None or spikes_out != "dense":
             raise NotImplementedError(f"sample_len / spikes_out need the fused engine ({reason})")
         self.last_fused_reason = reason
