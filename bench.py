@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="batched", choices=sorted(CONFIGS))
     ap.add_argument("--direction", default="scatter", choices=["scatter", "gather", "auto"])
+    ap.add_argument("--no-cudagraph", action="store_true", help="launch every chunk eagerly")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
@@ -254,6 +255,7 @@ def main():
 
     post, src, w, w_in = make_network(cfg, args.seed)
     rnn = build_model(cfg, post, src, w, w_in, dev, args.direction)
+    rnn.cudagraph = not args.no_cudagraph
     x, lens = make_inputs(cfg, args.seed + rank, dev)
     T, B, n = cfg["t_max"], cfg["batch"], cfg["n"]
     outdeg = torch.bincount(torch.from_numpy(src), minlength=n).to(dev)
@@ -282,14 +284,21 @@ def main():
         ev_start.record(stream)
         stats_list = []
         for _ in range(args.steps):
-            prof = []
-            one_step(x, prof)
-            profiles.append(prof)
+            one_step(x)
             stats_list.append(rnn.last_engine_stats.clone())
         ev_end.record(stream)
         torch.cuda.synchronize()
     elapsed_ms = ev_start.elapsed_time(ev_end)
     launches = rnn.last_engine_launches * args.steps
+    # roofline pass, outside the timed region: the same batch launched eagerly
+    # with CUDA events around every projection and step launch group
+    graph_mode, rnn.cudagraph = rnn.cudagraph, False
+    for _ in range(args.steps):
+        prof = []
+        one_step(x, prof)
+        profiles.append(prof)
+    torch.cuda.synchronize()
+    rnn.cudagraph = graph_mode
     for st in stats_list:
         s = st.cpu().numpy()
         events_total += int(s[:, 1].sum())
@@ -328,6 +337,7 @@ def main():
             "config": {"workload": f"{args.config}: ALIF+ExpPSC N={n} fixed in-degree {cfg['indeg']} "
                                    f"batch {B} durations {cfg['dur']} T_max {T} c_in {cfg['c_in']}",
                        "direction": rnn.last_engine_direction, "parallelism": f"replicas x{world}",
+                       "cudagraph": bool(rnn.cudagraph),
                        "l2": "working set (262 MB weights + 1 GB input) exceeds the 126 MB L2; no flush"},
             "neuron_steps_per_s": n * live_steps / (elapsed_ms * 1e-3) if world == 1 else None,
             "spike_rate_per_step": None,
@@ -385,6 +395,7 @@ def main():
                 torch.cuda.profiler.stop()
 
         reset_net(rnn, inplace=True)
+        rnn.cudagraph = False
         with torch.inference_mode(), environ.context(dt=1.0):
             rnn(x, sample_len=lens, spikes_out="bitmask", engine_chunk=64, engine_chunk_hook=hook)
         torch.cuda.synchronize()

@@ -1,6 +1,7 @@
 """Module API of btorch.models for the recurrent spiking step."""
 
-from . import environ, functional
+from . import cudagraph, environ, functional
+from .cudagraph import CudaGraphRunner
 from .base import BaseNode, MemoryModule, ParamBufferMixin, StepModule
 from .history import SpikeHistory
 from .linear import BaseSparseConn, DenseConn, SparseConn
@@ -9,6 +10,6 @@ from .rnn import RecurrentNN, RecurrentNNAbstract, make_rnn
 from .surrogate import Sigmoid
 from .synapse import BasePSC, DelayedPSC, ExponentialPSC, HeterSynapsePSC
 
-__all__ = ["environ", "functional", "BaseNode", "MemoryModule", "ParamBufferMixin", "StepModule", "SpikeHistory",
+__all__ = ["cudagraph", "CudaGraphRunner", "environ", "functional", "BaseNode", "MemoryModule", "ParamBufferMixin", "StepModule", "SpikeHistory",
            "BaseSparseConn", "DenseConn", "SparseConn", "ALIF", "LIF", "RecurrentNN", "RecurrentNNAbstract",
            "make_rnn", "Sigmoid", "BasePSC", "DelayedPSC", "ExponentialPSC", "HeterSynapsePSC"]

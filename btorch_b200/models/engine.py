@@ -29,6 +29,7 @@ from .neurons.lif import LIF
 from .synapse import DelayedPSC, ExponentialPSC, HeterSynapsePSC
 
 DEFAULT_CHUNK = 512
+DEFAULT_GRAPH_CHUNK = 128  # steps per captured chunk (rounded to a multiple of the slot period)
 
 
 @dataclass
@@ -129,10 +130,62 @@ def _state2d(t: torch.Tensor, n: int) -> torch.Tensor:
     return t.view(-1, n)
 
 
+def graph_hist_len(n_bins: int) -> int:
+    """History ring length for graph replay: the smallest H >= n_bins + 2 that
+    is even and a multiple of n_bins, so that the delay-ring slot (t mod R),
+    the history slot (t mod H) and the scratch parity (t mod 2) all repeat with
+    period H -- every chunk of a multiple of H steps then launches with the
+    same slot arguments, which a captured graph hard-wires."""
+    h = n_bins + 2
+    while h % n_bins or h % 2:
+        h += 1
+    return h
+
+
+class _GraphEntry:
+    """One captured chunk graph and the static buffers it is hard-wired to.
+
+    Replay re-runs the recorded launches with the pointers and slot indices of
+    the capture, so every tensor the chunk reads or writes lives here: the
+    state (copied in from the modules before the first chunk and back out after
+    the last), scratch, packed weights, the chunk's input and its outputs
+    (copied out after each replay)."""
+
+    def __init__(self):
+        self.buf: dict[str, torch.Tensor] = {}
+        self.graph = None
+        self.sig = None
+        self.captures = 0
+        self.replays = 0
+
+    def alloc(self, name, shape, dtype, dev, zero=False):
+        t = self.buf.get(name)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            t = torch.empty(shape, device=dev, dtype=dtype)
+            self.buf[name] = t
+            self.graph = None
+        if zero:
+            t.zero_()
+        return t
+
+
+def graph_entries(rnn) -> dict:
+    """The captured chunk graphs of `rnn`, keyed by launch configuration."""
+    return rnn.__dict__.setdefault("_bt_engine_graphs", {})
+
+
 def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None = None,
         chunk: int | None = None, spikes_out: str = "dense", stats: bool = False, profile: list | None = None,
         chunk_hook=None):
     """Run T = x.shape[0] steps.  Returns (z [T, *batch, n] or bitmaps, states).
+
+    With rnn.cudagraph the steps run in chunks of K (a multiple of the slot
+    period, graph_hist_len) whose launches -- input projection, every step,
+    the final PSC completion -- are captured once into a CUDA graph and
+    replayed for every full chunk (the counterpart of the reference's
+    CudaGraphRunner, btorch/models/cudagraph.py:101-242, with the state copied
+    in once per call rather than once per chunk); a shorter last chunk runs
+    eagerly on the same buffers.
 
     profile: if a list, (kind, start_event, end_event) CUDA-event pairs are
     appended for every input-projection ("project") and recurrent-step
@@ -151,14 +204,54 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     dev = neuron.v.device
     L.require_cuda(x, neuron.v, what="RecurrentNN")
     dt = float(environ.get("dt"))
-    v = _state2d(neuron.v, n)
-    B = v.shape[0]
+    v_mod = _state2d(neuron.v, n)
+    B = v_mod.shape[0]
     batch_shape = neuron.v.shape[:-1] if neuron.v.ndim > 1 else ()
-    ref = _state2d(neuron.refractory, n) if neuron._use_refractory else None
-    gk = _state2d(neuron.g_k, n) if isinstance(neuron, ALIF) else None
-    psc = _state2d(psc_mod.psc, n)
+    ref_mod = _state2d(neuron.refractory, n) if neuron._use_refractory else None
+    gk_mod = _state2d(neuron.g_k, n) if isinstance(neuron, ALIF) else None
+    psc_mod_t = _state2d(psc_mod.psc, n)
     T = int(x.shape[0])
     words = (n + 31) // 32
+    R = plan.n_bins
+    inp = plan.inp
+    c_in = int(x.shape[-1]) if inp is not None else n
+    trace_kinds = sorted(k for k in set(plan.paths.values()) if k != "history")
+
+    direction = conn.direction(B)
+    if direction == "gather":
+        # ordered pull: warp per post for tiny batches, sliced lane-per-post otherwise
+        mode = L.BT_MODE_PULL if B >= conn.sparse_config.pull_min_batch else L.BT_MODE_GATHER
+    else:
+        mode = L.BT_MODE_SCATTER
+
+    use_graph = bool(getattr(rnn, "cudagraph", False))
+    if use_graph:
+        H = graph_hist_len(R)
+        K = H * max(1, round(int(chunk or DEFAULT_GRAPH_CHUNK) / H))
+        gkey = (str(dev), B, n, c_in, mode, R, H, K, spikes_out, tuple(trace_kinds), bool(stats),
+                sample_len is not None, inp is not None)
+        entry = graph_entries(rnn).setdefault(gkey, _GraphEntry())
+
+        def alloc(name, shape, dtype, zero=False):
+            return entry.alloc(name, shape, dtype, dev, zero)
+
+        def static(name, t):
+            """Static copy of t (the graph reads fixed addresses)."""
+            if t is None:
+                return None
+            out = alloc(name, tuple(t.shape), t.dtype)
+            out.copy_(t)
+            return out
+    else:
+        H = R + 2
+        K = int(chunk or DEFAULT_CHUNK)
+        entry = None
+
+        def alloc(name, shape, dtype, zero=False):
+            return (torch.zeros if zero else torch.empty)(shape, device=dev, dtype=dtype)
+
+        def static(name, t):
+            return t
 
     desc = L.BtEngineDesc()
     keep = []
@@ -168,46 +261,41 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     coef, tau = psc_mod.coefficients(dt)
     keep += [coef, tau]
     desc.psc_coef, desc.psc_tau = L.param(coef), L.param(tau)
-    direction = conn.direction(B)
-    if direction == "gather":
-        # ordered pull: warp per post for tiny batches, sliced lane-per-post otherwise
-        desc.mode = L.BT_MODE_PULL if B >= conn.sparse_config.pull_min_batch else L.BT_MODE_GATHER
-    else:
-        desc.mode = L.BT_MODE_SCATTER
-    lay = conn.engine_layout(plan.n_bins, plan.uniform_delay, dev)
-    w = conn._get_effective_weight().detach().float().contiguous()
+    desc.mode = mode
+    lay = conn.engine_layout(R, plan.uniform_delay, dev)
+    w = static("w", conn._get_effective_weight().detach().float().contiguous())
     keep.append(w)
-    desc.n, desc.batch, desc.n_bins = n, B, plan.n_bins
-    H = plan.n_bins + 2
+    desc.n, desc.batch, desc.n_bins = n, B, R
     desc.hist_len = H
     desc.csc_ptr, desc.csc_src, desc.csc_w = lay.csc_ptr.data_ptr(), lay.csc_src.data_ptr(), w.data_ptr()
-    if desc.mode == L.BT_MODE_SCATTER:
-        w_csr = pack_csr_weights(lay, w)
+    if mode == L.BT_MODE_SCATTER:
+        w_csr = static("w_csr", pack_csr_weights(lay, w))
         keep.append(w_csr)
         desc.csr_ptr, desc.csr_dst, desc.csr_w = lay.csr_ptr.data_ptr(), lay.csr_dst.data_ptr(), w_csr.data_ptr()
-        ring = torch.zeros((plan.n_bins, B, n), device=dev, dtype=torch.float32)
-        work = torch.empty(L.lib().bt_engine_work_words(n, B), device=dev, dtype=torch.int32)
+        ring = alloc("ring", (R, B, n), torch.float32, zero=True)
+        work = alloc("work", (L.lib().bt_engine_work_words(n, B),), torch.int32)
         keep += [ring, work]
         desc.ring, desc.work = ring.data_ptr(), work.data_ptr()
-    mw = (B + 31) // 32
-    if desc.mode == L.BT_MODE_PULL:
+    if mode == L.BT_MODE_PULL:
         sl = getattr(lay, "slices", None)
         if sl is None:
             sl = build_slices(lay, dev)
             lay.slices = sl
-        sl_w = pack_slice_weights(sl, w)
-        masks = torch.zeros((H, n + 1, L.lib().bt_mask_stride(B)), device=dev, dtype=torch.int32)
+        sl_w = static("sl_w", pack_slice_weights(sl, w))
+        masks = alloc("masks", (H, n + 1, L.lib().bt_mask_stride(B)), torch.int32, zero=True)
         keep += [sl_w, masks]
         desc.sl_ptr, desc.sl_src, desc.sl_w = sl.sl_ptr.data_ptr(), sl.sl_src.data_ptr(), sl_w.data_ptr()
         desc.masks = masks.data_ptr()
     if stats:
-        outdeg = (lay.csr_ptr[1:] - lay.csr_ptr[:-1]).to(torch.int32).contiguous()
+        outdeg = static("outdeg", (lay.csr_ptr[1:] - lay.csr_ptr[:-1]).to(torch.int32).contiguous())
         keep.append(outdeg)
         desc.outdeg = outdeg.data_ptr()
+    # state: the modules' own tensors, updated in place (graph: static copies)
+    v, ref, gk, psc = static("v", v_mod), static("ref", ref_mod), static("gk", gk_mod), static("psc", psc_mod_t)
     desc.v, desc.psc = v.data_ptr(), psc.data_ptr()
     desc.refractory = L.ptr(ref)
     desc.g_k = L.ptr(gk)
-    hist = torch.zeros((H, B, words), device=dev, dtype=torch.int32)
+    hist = alloc("hist", (H, B, words), torch.int32, zero=True)
     keep.append(hist)
     desc.hist = hist.data_ptr()
     t0 = H
@@ -216,7 +304,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     want_hist_trace = "history" in plan.paths.values()
     if hist_depth:
         block = plan.history.recent_block(hist_depth).float().contiguous()  # [Dh, B, n], d steps ago
-        if desc.mode == L.BT_MODE_PULL:
+        if mode == L.BT_MODE_PULL:
             for d in range(hist_depth):
                 L.check(L.lib().bt_float_to_masks(B, n, block[d].data_ptr(), masks[(t0 - 1 - d) % H].data_ptr(), s),
                         "bt_float_to_masks")
@@ -227,80 +315,152 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             for d in range(hist_depth):
                 hist[(t0 - 1 - d) % H] = bits[d]
     desc.t0 = t0
-    if desc.mode == L.BT_MODE_SCATTER and plan.n_bins > 1:
+    if mode == L.BT_MODE_SCATTER and R > 1:
         desc.n_steps = 1
         L.check(L.lib().bt_engine_ring_from_history(C.byref(desc), s), "bt_engine_ring_from_history")
         launches += 1
 
-    # outputs
+    # outputs (graph: chunk-sized static buffers, copied out after each chunk)
     z = torch.empty((T, B, n), device=dev, dtype=torch.float32) if spikes_out == "dense" else None
     raster = torch.empty((T, B, words), device=dev, dtype=torch.int32)
-    traces = {kind: torch.empty((T, B, n), device=dev, dtype=torch.float32)
-              for kind in set(plan.paths.values()) if kind != "history"}
+    traces = {kind: torch.empty((T, B, n), device=dev, dtype=torch.float32) for kind in trace_kinds}
     stat_t = torch.zeros((T, 4), device=dev, dtype=torch.int64) if stats else None
+    if use_graph:
+        out_c = {"raster": alloc("raster", (K, B, words), torch.int32)}
+        if z is not None:
+            out_c["z"] = alloc("z", (K, B, n), torch.float32)
+        for kind in trace_kinds:
+            out_c[kind] = alloc("trace_" + kind, (K, B, n), torch.float32)
+        if stats:
+            out_c["stats"] = alloc("stats", (K, 4), torch.int64)
+        out_full = {"raster": raster, "z": z, "stats": stat_t, **traces}
 
     # input
-    inp = plan.inp
     if inp is not None:
         x3 = x.reshape(T, B, -1)
-        w_t = inp.weight.detach().float().t().contiguous()
-        bias = inp.bias.detach().float().contiguous() if inp.bias is not None else None
+        w_t = static("w_t", inp.weight.detach().float().t().contiguous())
+        bias = static("bias", inp.bias.detach().float().contiguous() if inp.bias is not None else None)
         keep += [w_t, bias]
     else:
         x3 = x.reshape(T, B, n) if x.numel() == T * B * n else torch.broadcast_to(x.reshape(T, -1, n), (T, B, n))
         if x3.dtype != torch.float32:
             raise TypeError("RecurrentNN input must be float32 for the fused engine.")
         x3 = x3.contiguous()
-    sl = None
     if sample_len is not None:
         sl_full = torch.as_tensor(sample_len, device=dev, dtype=torch.int64).reshape(B)
 
-    K = int(chunk or DEFAULT_CHUNK)
+    def chunk_inputs(k0, kc):
+        """Device inputs of the chunk at k0: (projection input or None, step input, sample lengths)."""
+        if use_graph:
+            xin = alloc("x", (K, B, c_in), torch.float32)
+            xin[:kc].copy_(x3[k0:k0 + kc])
+            xp = alloc("xp", (K, B, n), torch.float32) if inp is not None else xin
+            if inp is None:
+                xin = None
+        elif inp is not None:
+            xin = x3[k0:k0 + kc].float().contiguous()
+            xp = torch.empty((kc, B, n), device=dev, dtype=torch.float32)
+        else:
+            xin, xp = None, x3[k0:k0 + kc]
+        slc = None
+        if sample_len is not None:
+            slv = (sl_full - k0).clamp(0, kc).to(torch.int32)
+            slc = alloc("sl", (B,), torch.int32) if use_graph else slv.contiguous()
+            if use_graph:
+                slc.copy_(slv)
+        return xin, xp, slc
+
+    def set_desc(k0, kc, xp, slc, outs):
+        desc.x = xp.data_ptr()
+        desc.sample_len = L.ptr(slc)
+        desc.t0 = t0 + k0
+        desc.n_steps = kc
+        desc.raster = outs["raster"].data_ptr()
+        desc.spikes = outs["z"].data_ptr() if outs.get("z") is not None else None
+        desc.v_trace = outs["v"].data_ptr() if "v" in outs else None
+        desc.psc_trace = outs["psc"].data_ptr() if "psc" in outs else None
+        desc.ref_trace = outs["ref"].data_ptr() if "ref" in outs and ref is not None else None
+        desc.gk_trace = outs["gk"].data_ptr() if "gk" in outs and gk is not None else None
+        desc.stats = outs["stats"].data_ptr() if outs.get("stats") is not None else None
+
+    def launch(k0, kc, xin, xp, slc, outs, stream):
+        """Projection + steps of one chunk; outs maps output kind -> tensor whose
+        row 0 is the chunk's first step.  Returns the number of kernel launches."""
+        nl = 0
+        if xin is not None:
+            pw = alloc("pw", (K * B * (2 * c_in + 1),), torch.int32) if use_graph else \
+                torch.empty(kc * B * (2 * c_in + 1), device=dev, dtype=torch.int32)
+            keep.append(pw)
+            e0 = _ev() if profile is not None else None
+            L.check(L.lib().bt_input_project(kc * B, c_in, n, xin.data_ptr(), w_t.data_ptr(), L.ptr(bias),
+                                             xp.data_ptr(), pw.data_ptr(), stream), "bt_input_project")
+            nl += 2
+            if profile is not None:
+                profile.append(("project", e0, _ev()))
+        set_desc(k0, kc, xp, slc, outs)
+        e0 = _ev() if profile is not None else None
+        L.check(L.lib().bt_engine_run(C.byref(desc), stream), "bt_engine_run")
+        nl += (2 * kc if mode == L.BT_MODE_SCATTER else kc) + 1
+        if profile is not None:
+            profile.append(("step", e0, _ev()))
+        return nl
+
     for k0 in range(0, T, K):
         kc = min(K, T - k0)
         if chunk_hook is not None:
             chunk_hook(k0)
-        if inp is not None:
-            c_in = x3.shape[-1]
-            xc = x3[k0:k0 + kc].reshape(kc * B, c_in).float().contiguous()
-            xp = torch.empty((kc, B, n), device=dev, dtype=torch.float32)
-            pw = torch.empty(kc * B * (2 * c_in + 1), device=dev, dtype=torch.int32)
-            e0 = _ev() if profile is not None else None
-            L.check(L.lib().bt_input_project(kc * B, c_in, n, xc.data_ptr(), w_t.data_ptr(), L.ptr(bias),
-                                             xp.data_ptr(), pw.data_ptr(), s), "bt_input_project")
-            launches += 2
-            if profile is not None:
-                profile.append(("project", e0, _ev()))
-            keep_chunk = (xc, xp, pw)
+        xin, xp, slc = chunk_inputs(k0, kc)
+        if not use_graph:
+            outs = {"raster": raster[k0], "z": z[k0] if z is not None else None,
+                    "stats": stat_t[k0] if stat_t is not None else None,
+                    **{kind: traces[kind][k0] for kind in trace_kinds}}
+            launches += launch(k0, kc, xin, xp, slc, outs, s)
+            continue
+        if "stats" in out_c:
+            out_c["stats"].zero_()
+        if kc == K and profile is None:
+            # every full chunk starts at the same slot phase (K is a multiple of H):
+            # the capture records the launches of a chunk at k0 = 0
+            set_desc(0, K, xp, slc, out_c)
+            sig = _graph_signature(desc, xin, xp, slc, out_c, w_t if inp is not None else None,
+                                   bias if inp is not None else None)
+            if entry.graph is None or entry.sig != sig:
+                # first full chunk of this configuration: run it eagerly (which
+                # also performs any first-launch setup outside the capture),
+                # then record the same launches for the following chunks
+                nl = launch(k0, kc, xin, xp, slc, out_c, s)
+                torch.cuda.synchronize(dev)
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    if "stats" in out_c:
+                        out_c["stats"].zero_()
+                    entry.nodes = launch(0, K, xin, xp, slc, out_c, L.stream_of(dev))
+                entry.graph, entry.sig = g, sig
+                entry.captures += 1
+            else:
+                entry.graph.replay()
+                entry.replays += 1
+                nl = entry.nodes
+            launches += nl
         else:
-            xp = x3[k0:k0 + kc]
-            keep_chunk = (xp,)
-        if sample_len is not None:
-            sl = (sl_full - k0).clamp(0, kc).to(torch.int32).contiguous()
-            keep_chunk = keep_chunk + (sl,)
-        desc.x = xp.data_ptr()
-        desc.sample_len = L.ptr(sl)
-        desc.t0 = t0 + k0
-        desc.n_steps = kc
-        desc.raster = raster[k0].data_ptr()
-        desc.spikes = z[k0].data_ptr() if z is not None else None
-        desc.v_trace = traces["v"][k0].data_ptr() if "v" in traces else None
-        desc.psc_trace = traces["psc"][k0].data_ptr() if "psc" in traces else None
-        desc.ref_trace = traces["ref"][k0].data_ptr() if "ref" in traces and ref is not None else None
-        desc.gk_trace = traces["gk"][k0].data_ptr() if "gk" in traces and gk is not None else None
-        desc.stats = stat_t[k0].data_ptr() if stat_t is not None else None
-        e0 = _ev() if profile is not None else None
-        L.check(L.lib().bt_engine_run(C.byref(desc), s), "bt_engine_run")
-        launches += (2 * kc if desc.mode == L.BT_MODE_SCATTER else kc) + 1
-        if profile is not None:
-            profile.append(("step", e0, _ev()))
-        del keep_chunk
+            launches += launch(k0, kc, xin, xp, slc, out_c, s)
+        for kind, t in out_c.items():
+            if out_full.get(kind) is not None:
+                out_full[kind][k0:k0 + kc].copy_(t[:kc])
+
+    if use_graph:
+        v_mod.copy_(v)
+        psc_mod_t.copy_(psc)
+        if ref_mod is not None:
+            ref_mod.copy_(ref)
+        if gk_mod is not None:
+            gk_mod.copy_(gk)
 
     # write the spike history back into the module (last Dh spikes)
     t_end = t0 + T
     if hist_depth:
         block = torch.empty((hist_depth, B, n), device=dev, dtype=torch.float32)
-        if desc.mode == L.BT_MODE_PULL:
+        if mode == L.BT_MODE_PULL:
             for d in range(hist_depth):
                 L.check(L.lib().bt_masks_to_float(B, n, masks[(t_end - 1 - d) % H].data_ptr(), block[d].data_ptr(), s),
                         "bt_masks_to_float")
@@ -324,12 +484,24 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             states[key] = traces[kind].view(T, *batch_shape, *_nshape(plan, key))
     rnn.last_engine_stats = stat_t
     rnn.last_engine_direction = {L.BT_MODE_SCATTER: "scatter", L.BT_MODE_GATHER: "gather",
-                                 L.BT_MODE_PULL: "pull"}[desc.mode]
+                                 L.BT_MODE_PULL: "pull"}[mode]
     rnn.last_engine_launches = launches
     if z is not None:
         z = z.view(T, *batch_shape, *neuron.n_neuron)
         return z, states
     return raster, states
+
+
+def _graph_signature(desc, *tensors):
+    """Everything a captured chunk hard-wires: the descriptor's bytes (pointers,
+    sizes, scalars) and the addresses of the projection's operands."""
+    ptrs = []
+    for t in tensors:
+        if isinstance(t, dict):
+            ptrs += [(k, v.data_ptr()) for k, v in sorted(t.items())]
+        else:
+            ptrs.append(t.data_ptr() if t is not None else 0)
+    return bytes(desc), tuple(ptrs)
 
 
 def _nshape(plan: EnginePlan, key: str):

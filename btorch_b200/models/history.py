@@ -54,9 +54,11 @@ class SpikeHistory(MemoryModule):
         spike = spike.to(self.history.dtype)
         nb = self._nb()
         if self.use_circular_buffer:
+            # index ops with a device-side index: no host sync, so the update
+            # can be captured in a CUDA graph
             h = self._delay_first()
-            h[self._cursor] = spike
-            self._cursor.fill_((self._cursor + 1) % self.max_delay)
+            h.index_copy_(0, self._cursor.view(1), spike.unsqueeze(0))
+            self._cursor.copy_((self._cursor + 1) % self.max_delay)
         else:
             h = self._delay_first()
             new = torch.cat([spike.unsqueeze(0), h[:-1]], dim=0)
@@ -69,7 +71,7 @@ class SpikeHistory(MemoryModule):
                              "Increase max_delay_steps or use smaller delays.")
         h = self._delay_first()
         if self.use_circular_buffer:
-            return h[(self._cursor - 1 - delay_steps) % self.max_delay]
+            return h.index_select(0, ((self._cursor - 1 - delay_steps) % self.max_delay).view(1)).squeeze(0)
         return h[delay_steps]
 
     def get_recent(self, n_steps: int) -> list[torch.Tensor]:

@@ -19,6 +19,7 @@ from torch.utils.checkpoint import checkpoint
 
 from . import base, environ
 from . import engine as _engine
+from .cudagraph import CudaGraphRunner
 from .functional import filter_hidden_states, named_hidden_states, prepare_sparse_modules, set_hidden_states
 
 
@@ -39,6 +40,7 @@ class RecurrentNNAbstract(base.MemoryModule):
         self._grad_history = {}
         self.cudagraph = cudagraph
         self.cudagraph_warmup = cudagraph_warmup
+        self._cudagraph_runner = CudaGraphRunner(warmup=cudagraph_warmup)
         self.fused = fused
         self.last_engine_stats = None
         self.last_engine_direction = None
@@ -100,7 +102,14 @@ class RecurrentNNAbstract(base.MemoryModule):
         all_z, all_st = [], {}
         for c in range(n_chunks):
             cargs = tuple(splits[i][c] if i in loop_args else args[i] for i in range(len(args)))
-            if self.grad_checkpoint:
+            if self.cudagraph:
+                def fn(*inner):
+                    zs, sts = self._process_chunk(*inner, loop_args=loop_args, **kwargs)
+                    return torch.stack(zs), {k: torch.stack(v) for k, v in sts.items()}
+
+                # offloading copies out of the graph pool itself
+                z, st = self._cudagraph_runner(self, fn, cargs, clone_outputs=not self.cpu_offload)
+            elif self.grad_checkpoint:
                 z, st = self._checkpointed_chunk(*cargs, loop_args=loop_args, **kwargs)
             else:
                 zs, sts = self._process_chunk(*cargs, loop_args=loop_args, **kwargs)
@@ -169,6 +178,8 @@ class RecurrentNN(RecurrentNNAbstract):
             or any(torch.is_tensor(a) and a.requires_grad for a in args))
         extra = len(args) > 1 and any(a is not None for a in args[1:])
         plan, reason = (None, "disabled")
+        if self.cudagraph:
+            CudaGraphRunner.check_supported(self, args)
         if self.fused and not needs_grad and not extra and not kwargs and loop_args in (None, (0,)):
             plan, reason = _engine.match(self)
         if plan is not None:
