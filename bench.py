@@ -1,13 +1,23 @@
 """Benchmark of the B200 recurrent spiking step (one JSON line on rank 0).
 
-Workload (default, --config batched): the batched-simulation configuration --
-ALIF + exponential synapse (tau_syn 5 ms, adaptation tau 200 ms, dg_k 0.07),
-N = 65536 neurons, fixed in-degree 500 (32.8M fp32 weights), batch 64 samples
-with durations uniform in [200, 2000] steps, Poisson input from 2000 channels
-at per-sample rates uniform in [2, 40] Hz through a dense fp32 input layer,
-dt = 1 ms.  Synthetic, seeded inputs and random weights of that shape.  One
-bench "step" simulates the whole batch (all 2000 time steps, finished samples
-masked) through RecurrentNN's public forward.
+Headline workload (--config batched): ALIF + exponential synapse (tau_syn
+5 ms, adaptation tau 200 ms, dg_k 0.07), N = 65536 neurons, fixed in-degree
+500 (32.8M fp32 weights), batch 64 samples with durations uniform in
+[200, 2000] steps, Poisson input from 2000 channels at per-sample rates
+uniform in [2, 40] Hz through a dense fp32 input layer, dt = 1 ms.  One bench
+"step" simulates the whole batch (all 2000 time steps, finished samples
+masked) through RecurrentNN's public forward, with CUDA-graph chunk replay.
+
+Second workload (--config connectome, and by default appended to the
+headline line as "connectome"): N = 140000 LIF neurons (c_m 64, tau 20,
+refractory 2 ms, hard reset), lognormal in-degree (mean 350, sigma 1.0;
+~49M synapses), weights = geometric synapse counts (mean 4) x +-2^-6 with the
+sign by presynaptic type (70 % excitatory), per-synapse delays uniform in
+1..20 steps (HeterSynapsePSC over the delay-expanded matrix), background
+Poisson drive 8 x Poisson(0.25) per neuron and step (~11 Hz network rate),
+batch 8, T = 2000.  Weights and drive are dyadic, so rasters are exact.  Its
+object also carries the plain step: the same network at batch 1, launched
+eagerly (no graph), on sample 0's input.
 
 metric: synaptic events/s = sum over samples and time steps of the
 out-degree of every neuron that spiked, divided by the device time.
@@ -37,13 +47,14 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 CONFIGS = {
-    # name: N, in-degree, batch, c_in, T, rate range (Hz), duration range
-    "batched": dict(n=65536, indeg=500, batch=64, c_in=2000, t_max=2000, rate=(2.0, 40.0), dur=(200, 2000),
-                    w_scale=0.0030, in_gain=1.0),
-    "small": dict(n=65536, indeg=500, batch=64, c_in=2000, t_max=64, rate=(2.0, 40.0), dur=(64, 64),
-                  w_scale=0.0030, in_gain=1.0),
+    "batched": dict(model="alif_dense_input", n=65536, indeg=500, batch=64, c_in=2000, t_max=2000,
+                    rate=(2.0, 40.0), dur=(200, 2000), w_scale=0.0030, in_gain=1.0, s_state=36),
+    "small": dict(model="alif_dense_input", n=65536, indeg=500, batch=64, c_in=2000, t_max=64,
+                  rate=(2.0, 40.0), dur=(64, 64), w_scale=0.0030, in_gain=1.0, s_state=36),
+    # s_state: v, psc, refractory r/w (24) + drive read (4) + delay-ring slot read and clear (8)
+    "connectome": dict(model="lif_hetero_delay", n=140000, indeg=350, indeg_sigma=1.0, n_bins=20, exc=0.7,
+                       batch=8, t_max=2000, dur=(2000, 2000), c_m=64.0, drive=(0.25, 8.0), s_state=36),
 }
-S_STATE = 36  # bytes per live neuron-sample per step: r/w v, psc, refractory, g_k (32) + input current read (4)
 
 
 def parse():
@@ -53,6 +64,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="batched", choices=sorted(CONFIGS))
+    ap.add_argument("--extra", default="connectome",
+                    help="comma-separated workloads measured after the headline one ('' for none)")
     ap.add_argument("--direction", default="scatter", choices=["scatter", "gather", "auto"])
     ap.add_argument("--no-cudagraph", action="store_true", help="launch every chunk eagerly")
     ap.add_argument("--no-e2e", action="store_true")
@@ -67,54 +80,107 @@ def parse():
 
 # ------------------------------------------------------------- workload --
 
+def _dedupe_sorted(post, pre, n):
+    key = post * n + pre
+    key.sort()
+    keep = np.ones(key.size, bool)
+    keep[1:] = key[1:] != key[:-1]
+    key = key[keep]
+    return key // n, key % n
+
+
 def make_network(cfg, seed=0):
-    """Canonical (post, src) arrays of a fixed in-degree network and ALIF params."""
+    """dict(post, src, pre, w, n_bins, w_in): canonical (post, src) arrays; src
+    is the presynaptic id, or pre * n_bins + delay bin for the delay-expanded
+    matrix."""
     rng = np.random.default_rng(seed)
-    n, k = cfg["n"], cfg["indeg"]
-    src = rng.integers(0, n, size=(n, k), dtype=np.int64)
-    src.sort(axis=1)
-    for _ in range(50):
-        dup = np.zeros_like(src, dtype=bool)
-        dup[:, 1:] = src[:, 1:] == src[:, :-1]
-        if not dup.any():
-            break
-        src[dup] = rng.integers(0, n, size=int(dup.sum()))
+    n = cfg["n"]
+    if cfg["model"] == "alif_dense_input":
+        k = cfg["indeg"]
+        src = rng.integers(0, n, size=(n, k), dtype=np.int64)
         src.sort(axis=1)
+        for _ in range(50):
+            dup = np.zeros_like(src, dtype=bool)
+            dup[:, 1:] = src[:, 1:] == src[:, :-1]
+            if not dup.any():
+                break
+            src[dup] = rng.integers(0, n, size=int(dup.sum()))
+            src.sort(axis=1)
+        post = np.repeat(np.arange(n, dtype=np.int64), k)
+        src = src.reshape(-1)
+        exc = src < int(0.8 * n)
+        w = rng.lognormal(-1.0, 1.0, size=src.size).astype(np.float32) * np.float32(cfg["w_scale"])
+        w = np.where(exc, w, np.float32(-0.4) * w).astype(np.float32)
+        w_in = (rng.normal(0.0, 0.05, size=(cfg["c_in"], n)) * cfg["in_gain"]).astype(np.float32)
+        return dict(post=post, src=src, pre=src, w=w, n_bins=1, w_in=w_in)
+    # connectome-shaped: lognormal in-degree, presynaptic type sets the sign,
+    # per-synapse delay d in 1..R lands in delay bin d - 1
+    R = cfg["n_bins"]
+    sigma = cfg["indeg_sigma"]
+    mu = np.log(cfg["indeg"]) - sigma ** 2 / 2
+    k = np.clip(np.rint(rng.lognormal(mu, sigma, n)), 1, n - 1).astype(np.int64)
     post = np.repeat(np.arange(n, dtype=np.int64), k)
-    src = src.reshape(-1)
-    exc = src < int(0.8 * n)
-    w = rng.lognormal(-1.0, 1.0, size=src.size).astype(np.float32) * np.float32(cfg["w_scale"])
-    w = np.where(exc, w, np.float32(-0.4) * w).astype(np.float32)
-    w_in = (rng.normal(0.0, 0.05, size=(cfg["c_in"], n)) * cfg["in_gain"]).astype(np.float32)
-    return post, src, w, w_in
+    pre = rng.integers(0, n, size=post.size, dtype=np.int64)
+    post, pre = _dedupe_sorted(post, pre, n)
+    delay = rng.integers(1, R + 1, size=post.size)
+    count = rng.geometric(0.25, size=post.size)
+    w = (count * np.where(pre < int(cfg["exc"] * n), 1.0, -1.0) * 2.0 ** -6).astype(np.float32)
+    return dict(post=post, src=pre * R + (delay - 1), pre=pre, delay_bin=delay - 1, w=w, n_bins=R, w_in=None)
 
 
-def build_model(cfg, post, src, w, w_in, device, direction):
-    from btorch_b200.models import ALIF, DenseConn, ExponentialPSC, RecurrentNN, SparseConn
+def build_model(cfg, net, device, direction, batch=None):
+    import pandas as pd
+
+    from btorch_b200.models import (ALIF, LIF, DenseConn, ExponentialPSC, HeterSynapsePSC, RecurrentNN,
+                                    SparseConn)
     from btorch_b200.models.functional import init_net_state
 
-    n = cfg["n"]
-    conn = SparseConn.from_canonical(post, src, w, (n, n), enforce_dale=False,
+    n, R = cfg["n"], net["n_bins"]
+    conn = SparseConn.from_canonical(net["post"], net["src"], net["w"], (n * R, n), enforce_dale=False,
                                      sparse_config={"direction": direction})
-    neuron = ALIF(n, v_threshold=1.0, v_reset=0.0, c_m=1.0, g_leak=0.05, E_leak=0.0, E_k=-1.0, tau_adapt=200.0,
-                  dg_k=0.07, tau_ref=2.0, hard_reset=True)
-    syn = ExponentialPSC(n, tau_syn=5.0, linear=conn)
-    inp = DenseConn(cfg["c_in"], n, weight=torch.from_numpy(w_in))
+    if cfg["model"] == "alif_dense_input":
+        neuron = ALIF(n, v_threshold=1.0, v_reset=0.0, c_m=1.0, g_leak=0.05, E_leak=0.0, E_k=-1.0,
+                      tau_adapt=200.0, dg_k=0.07, tau_ref=2.0, hard_reset=True)
+        syn = ExponentialPSC(n, tau_syn=5.0, linear=conn)
+        inp = DenseConn(cfg["c_in"], n, weight=torch.from_numpy(net["w_in"]))
+    else:
+        neuron = LIF(n, v_threshold=1.0, v_reset=0.0, c_m=cfg["c_m"], tau=20.0, tau_ref=2.0, hard_reset=True)
+        rti = pd.DataFrame({"receptor_type": ["syn"], "receptor_index": [0]})
+        syn = HeterSynapsePSC(n, 1, rti, conn, base_psc=ExponentialPSC, max_delay_steps=R,
+                              use_circular_buffer=True, tau_syn=5.0)
+        inp = None
     rnn = RecurrentNN(neuron, syn, neuron_inp_module=inp, update_state_names=()).to(device)
-    init_net_state(rnn, batch_size=cfg["batch"], dtype=torch.float32, device=device)
+    init_net_state(rnn, batch_size=batch or cfg["batch"], dtype=torch.float32, device=device)
     return rnn
 
 
 def make_inputs(cfg, seed, device):
     g = torch.Generator(device=device).manual_seed(10_000 + seed)
-    B, C, T = cfg["batch"], cfg["c_in"], cfg["t_max"]
-    lo, hi = cfg["rate"]
-    rates = lo + (hi - lo) * torch.rand(B, generator=g, device=device)
-    p = (rates * 1e-3).view(1, B, 1).expand(T, B, C)
-    x = torch.poisson(p.contiguous(), generator=g)
+    B, T = cfg["batch"], cfg["t_max"]
+    if cfg["model"] == "alif_dense_input":
+        C = cfg["c_in"]
+        lo, hi = cfg["rate"]
+        rates = lo + (hi - lo) * torch.rand(B, generator=g, device=device)
+        p = (rates * 1e-3).view(1, B, 1).expand(T, B, C)
+        x = torch.poisson(p.contiguous(), generator=g)
+    else:
+        lam, amp = cfg["drive"]
+        x = torch.empty((T, B, cfg["n"]), device=device, dtype=torch.float32)
+        rate = torch.full((B, cfg["n"]), lam, device=device)
+        for t in range(T):
+            x[t] = torch.poisson(rate, generator=g) * amp
     dlo, dhi = cfg["dur"]
     lens = torch.randint(dlo, dhi + 1, (B,), generator=g, device=device)
     return x, lens
+
+
+def describe(name, cfg):
+    if cfg["model"] == "alif_dense_input":
+        return (f"{name}: ALIF+ExpPSC N={cfg['n']} fixed in-degree {cfg['indeg']} batch {cfg['batch']} "
+                f"durations {cfg['dur']} T_max {cfg['t_max']} c_in {cfg['c_in']}")
+    return (f"{name}: LIF+HeterSynapsePSC(ExpPSC) N={cfg['n']} lognormal in-degree mean {cfg['indeg']} "
+            f"sigma {cfg['indeg_sigma']} delays 1..{cfg['n_bins']} batch {cfg['batch']} T {cfg['t_max']} "
+            f"drive {cfg['drive'][1]} x Poisson({cfg['drive'][0]})")
 
 
 # --------------------------------------------------------------- clocks --
@@ -168,29 +234,45 @@ class ClockSampler:
 
 # -------------------------------------------------------------- oracle --
 
-def cpu_sample(cfg, post, src, w, w_in, x_cpu, steps):
+def oracle_spec(cfg, net):
+    from oracle import oracle as O
+
+    n = cfg["n"]
+    ptr = np.zeros(n + 1, np.int64)
+    ptr[1:] = np.cumsum(np.bincount(net["post"], minlength=n))
+    lin = -1.0 / torch.as_tensor(5.0)
+    coef_syn = float(torch.expm1(1.0 * lin) / lin)
+    if cfg["model"] == "alif_dense_input":
+        lin = -1.0 / torch.as_tensor(200.0)
+        coef_gk = float(torch.expm1(1.0 * lin) / lin)
+        params = {"v_threshold": 1.0, "v_reset": 0.0, "c_m": 1.0, "g_leak": 0.05, "E_leak": 0.0, "E_k": -1.0,
+                  "dg_k": 0.07, "tau_adapt": 200.0, "coef_gk": coef_gk, "tau_ref": 2.0, "psc_coef": coef_syn,
+                  "psc_tau": 5.0}
+        return O.NetSpec(n=n, kind=1, hard_reset=True, use_ref=True, dt=1.0, params=params, ptr=ptr,
+                         pre=net["pre"].astype(np.int32), delay=np.zeros(net["pre"].size, np.int32), w=net["w"])
+    params = {"v_threshold": 1.0, "v_reset": 0.0, "c_m": cfg["c_m"], "tau": 20.0, "tau_ref": 2.0,
+              "psc_coef": coef_syn, "psc_tau": 5.0}
+    return O.NetSpec(n=n, kind=0, hard_reset=True, use_ref=True, dt=1.0, params=params, ptr=ptr,
+                     pre=net["pre"].astype(np.int32), delay=net["delay_bin"].astype(np.int32), w=net["w"],
+                     max_delay=net["n_bins"] - 1)
+
+
+def cpu_sample(cfg, net, x_cpu, steps):
     """Oracle port of the reference's CPU step on the first `steps` time steps
     of the batch; returns (events, seconds, threads)."""
     from oracle import oracle as O
 
     n, B = cfg["n"], cfg["batch"]
-    ptr = np.zeros(n + 1, np.int64)
-    ptr[1:] = np.cumsum(np.bincount(post, minlength=n))
-    lin = -1.0 / torch.as_tensor(200.0)
-    coef_gk = float(torch.expm1(1.0 * lin) / lin)
-    lin = -1.0 / torch.as_tensor(5.0)
-    coef_syn = float(torch.expm1(1.0 * lin) / lin)
-    spec = O.NetSpec(n=n, kind=1, hard_reset=True, use_ref=True, dt=1.0,
-                     params={"v_threshold": 1.0, "v_reset": 0.0, "c_m": 1.0, "g_leak": 0.05, "E_leak": 0.0,
-                             "E_k": -1.0, "dg_k": 0.07, "tau_adapt": 200.0, "coef_gk": coef_gk, "tau_ref": 2.0,
-                             "psc_coef": coef_syn, "psc_tau": 5.0},
-                     ptr=ptr, pre=src.astype(np.int32), delay=np.zeros(src.size, np.int32), w=w)
+    spec = oracle_spec(cfg, net)
     threads = os.cpu_count() or 1
     st = O.init_state(spec, B)
-    outdeg = np.bincount(src, minlength=n).astype(np.int64)
+    outdeg = np.bincount(net["pre"], minlength=n).astype(np.int64)
     t0 = time.perf_counter()
-    xin = x_cpu[:steps].reshape(steps * B, -1)
-    xp = O.linear(xin, w_in.T.copy()).reshape(steps, B, n)
+    if net["w_in"] is not None:
+        xin = x_cpu[:steps].reshape(steps * B, -1)
+        xp = O.linear(xin, net["w_in"].T.copy()).reshape(steps, B, n)
+    else:
+        xp = x_cpu[:steps]
     out = O.run(spec, st, xp, threads=threads)
     dt = time.perf_counter() - t0
     events = int((out["spikes"].astype(np.int64) * outdeg[None, None, :]).sum())
@@ -216,49 +298,67 @@ def dist_setup(args):
 def reference_arm(args, cfg, world, rank):
     if rank != 0:
         return
-    post, src, w, w_in = make_network(cfg, args.seed)
+    net = make_network(cfg, args.seed)
     rng = np.random.default_rng(10_000 + args.seed)
     S = args.cpu_sample_steps
-    rates = rng.uniform(*cfg["rate"], size=cfg["batch"])
-    x = rng.poisson(np.broadcast_to((rates * 1e-3)[None, :, None], (S, cfg["batch"], cfg["c_in"]))).astype(np.float32)
+    B = cfg["batch"]
+    if net["w_in"] is not None:
+        rates = rng.uniform(*cfg["rate"], size=B)
+        x = rng.poisson(np.broadcast_to((rates * 1e-3)[None, :, None], (S, B, cfg["c_in"]))).astype(np.float32)
+    else:
+        lam, amp = cfg["drive"]
+        x = (rng.poisson(lam, (S, B, cfg["n"])) * amp).astype(np.float32)
     for _ in range(min(args.warmup, 1)):
-        cpu_sample(cfg, post, src, w, w_in, x, 1)
+        cpu_sample(cfg, net, x, 1)
     tot_e, tot_t, thr = 0, 0.0, 1
     for _ in range(args.steps):
-        e, t, thr = cpu_sample(cfg, post, src, w, w_in, x, S)
+        e, t, thr = cpu_sample(cfg, net, x, S)
         tot_e += e
         tot_t += t
     val = tot_e / tot_t
-    sample = f"{S} time steps of the {cfg['batch']}-sample batch per step (of up to {cfg['t_max']})"
+    sample = f"{S} time steps of the {B}-sample batch per step (of up to {cfg['t_max']})"
     line = {"metric": "synaptic_events_per_s", "value": val, "unit": "events/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"{args.config}: ALIF+ExpPSC N={cfg['n']} in-degree {cfg['indeg']} "
-                                   f"batch {cfg['batch']} T<= {cfg['t_max']}", "parallelism": "replicas"},
+            "config": {"workload": describe(args.config, cfg), "parallelism": "replicas"},
             "cpu_baseline": {"value": val, "unit": "events/s", "cores": thr, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-def main():
-    args = parse()
-    cfg = CONFIGS[args.config]
-    world, rank, local = dist_setup(args)
-    if args.impl == "reference":
-        reference_arm(args, cfg, world, rank)
-        return
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
+def _peak():
+    f = ROOT / "MEASURED_PEAKS.json"
+    peaks = json.loads(f.read_text()) if f.exists() else {}
+    return float(peaks.get("hbm_gbs", 6650.0)), ("measured" if "hbm_gbs" in peaks else "fallback")
+
+
+def _traffic(name):
+    """DRAM bytes per batch of the step kernels, scaled from an ncu capture
+    (profiles/eng_step_<workload>_traffic.json), or None."""
+    tf = ROOT / "profiles" / f"eng_step_{name}_traffic.json"
+    return json.loads(tf.read_text()).get("dram_bytes_per_batch") if tf.exists() else None
+
+
+def _allreduce(v, dev, op):
+    import torch.distributed as dist
+
+    t = torch.tensor([v], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
+def measure(name, cfg, args, dev, world, rank, local):
+    """Time args.steps whole batches of workload `name`.  Returns (line dict,
+    or None on ranks > 0; model; input; lengths; network; step function)."""
     from btorch_b200.models import environ
     from btorch_b200.models.functional import reset_net
 
-    post, src, w, w_in = make_network(cfg, args.seed)
-    rnn = build_model(cfg, post, src, w, w_in, dev, args.direction)
+    net = make_network(cfg, args.seed)
+    rnn = build_model(cfg, net, dev, args.direction)
     rnn.cudagraph = not args.no_cudagraph
     x, lens = make_inputs(cfg, args.seed + rank, dev)
-    T, B, n = cfg["t_max"], cfg["batch"], cfg["n"]
-    outdeg = torch.bincount(torch.from_numpy(src), minlength=n).to(dev)
+    T, n = cfg["t_max"], cfg["n"]
 
     def one_step(xx, profile=None):
         reset_net(rnn, inplace=True)
@@ -273,16 +373,12 @@ def main():
         torch.distributed.barrier()
 
     stream = torch.cuda.current_stream(dev)
-    profiles = []
     ev_start = torch.cuda.Event(enable_timing=True)
     ev_end = torch.cuda.Event(enable_timing=True)
-    events_total = 0
-    live_steps = 0
-    algo_bytes = 0
+    stats_list = []
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         ev_start.record(stream)
-        stats_list = []
         for _ in range(args.steps):
             one_step(x)
             stats_list.append(rnn.last_engine_stats.clone())
@@ -290,66 +386,106 @@ def main():
         torch.cuda.synchronize()
     elapsed_ms = ev_start.elapsed_time(ev_end)
     launches = rnn.last_engine_launches * args.steps
-    # roofline pass, outside the timed region: the same batch launched eagerly
-    # with CUDA events around every projection and step launch group
+    # roofline pass, outside the timed region: the same batches launched
+    # eagerly with CUDA events around every projection and step launch group
     graph_mode, rnn.cudagraph = rnn.cudagraph, False
+    profiles = []
     for _ in range(args.steps):
         prof = []
         one_step(x, prof)
         profiles.append(prof)
     torch.cuda.synchronize()
     rnn.cudagraph = graph_mode
+
+    events_total = live_steps = algo_bytes = 0
+    live_per_step = torch.clamp(lens.cpu()[None, :] > torch.arange(T)[:, None], 0, 1).sum(1).numpy()
     for st in stats_list:
         s = st.cpu().numpy()
         events_total += int(s[:, 1].sum())
-        live_per_step = torch.clamp(lens.cpu()[None, :] > torch.arange(T)[:, None], 0, 1).sum(1).numpy()
-        algo_bytes += int(8 * s[:, 2].sum() + 8 * s[:, 0].sum() + S_STATE * n * live_per_step.sum())
+        algo_bytes += int(8 * s[:, 2].sum() + 8 * s[:, 0].sum() + cfg["s_state"] * n * live_per_step.sum())
         live_steps += int(live_per_step.sum())
     step_ms = sum(a.elapsed_time(b) for prof in profiles for k, a, b in prof if k == "step")
     proj_ms = sum(a.elapsed_time(b) for prof in profiles for k, a, b in prof if k == "project")
-
     if world > 1:
         import torch.distributed as dist
 
-        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
-        e = torch.tensor([events_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(e)
-        events_total = int(e.item())
+        elapsed_ms = _allreduce(elapsed_ms, dev, dist.ReduceOp.MAX)
+        events_total = int(_allreduce(events_total, dev, dist.ReduceOp.SUM))
     value = events_total / (elapsed_ms * 1e-3)
-
     line = None
     if rank == 0:
-        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-        peak = float(peaks.get("hbm_gbs", 6650.0))
-        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        peak, peak_src = _peak()
         achieved = algo_bytes / (step_ms * 1e-3) / 1e9
-        traffic = None
-        tf = ROOT / "profiles" / "eng_step_batched_traffic.json"
-        if tf.exists():
-            traffic = json.loads(tf.read_text()).get("dram_bytes_per_step")
+        traffic = _traffic(name)
         line = {
             "metric": "synaptic_events_per_s", "value": value, "unit": "events/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Poisson input, random weights of the configuration's shape)",
-            "config": {"workload": f"{args.config}: ALIF+ExpPSC N={n} fixed in-degree {cfg['indeg']} "
-                                   f"batch {B} durations {cfg['dur']} T_max {T} c_in {cfg['c_in']}",
-                       "direction": rnn.last_engine_direction, "parallelism": f"replicas x{world}",
-                       "cudagraph": bool(rnn.cudagraph),
-                       "l2": "working set (262 MB weights + 1 GB input) exceeds the 126 MB L2; no flush"},
+            "config": {"workload": describe(name, cfg), "direction": rnn.last_engine_direction,
+                       "parallelism": f"replicas x{world}", "cudagraph": bool(rnn.cudagraph),
+                       "l2": "working set (weights + input) exceeds the 126 MB L2; no flush"},
             "neuron_steps_per_s": n * live_steps / (elapsed_ms * 1e-3) if world == 1 else None,
-            "spike_rate_per_step": None,
-            "roofline": {"bound": "hbm", "kernel": "recurrent step (k_eng_neuron + k_eng_scatter)",
+            "spike_rate_per_step": events_total / max(1, live_steps) / len(net["w"]),
+            "roofline": {"bound": "hbm", "kernel": "recurrent step (neuron + synapse launches)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_src, "traffic": traffic,
                          "algorithmic_bytes_per_batch": algo_bytes / args.steps,
-                         "step_ms_per_batch": step_ms / args.steps, "projection_ms_per_batch": proj_ms / args.steps},
+                         "step_ms_per_batch": step_ms / args.steps,
+                         "projection_ms_per_batch": proj_ms / args.steps},
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
-        line["spike_rate_per_step"] = events_total / max(1, live_steps) / n / cfg["indeg"]
+    return line, rnn, x, lens, net, one_step
+
+
+def plain_step(cfg, net, x, lens, args, dev):
+    """The plain single-request step: batch 1 (sample 0), eager launches."""
+    from btorch_b200.models import environ
+    from btorch_b200.models.functional import reset_net
+
+    m = build_model(cfg, net, dev, args.direction, batch=1)
+    m.cudagraph = False
+    x1, l1 = x[:, :1].contiguous(), lens[:1]
+
+    def go():
+        reset_net(m, inplace=True)
+        with torch.inference_mode(), environ.context(dt=1.0):
+            m(x1, sample_len=l1, spikes_out="bitmask", engine_stats=True)
+
+    for _ in range(2):
+        go()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream(dev)
+    ev = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        go()
+        ev += m.last_engine_stats[:, 1].sum()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"value": int(ev) / (ms * 1e-3), "unit": "events/s", "ms_per_step": ms / args.steps,
+            "batch": 1, "cudagraph": False, "direction": m.last_engine_direction,
+            "gpu_launches": m.last_engine_launches * args.steps}
+
+
+def main():
+    args = parse()
+    cfg = CONFIGS[args.config]
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        reference_arm(args, cfg, world, rank)
+        return
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from btorch_b200.models import environ
+    from btorch_b200.models.functional import reset_net
+
+    line, rnn, x, lens, net, one_step = measure(args.config, cfg, args, dev, world, rank, local)
+    stream = torch.cuda.current_stream(dev)
+    T, B, n = cfg["t_max"], cfg["batch"], cfg["n"]
     # e2e: host buffers through the public API (H2D of the input, D2H of the raster)
     if not args.no_e2e:
         x_host = x.cpu().pin_memory()
@@ -373,16 +509,13 @@ def main():
         if world > 1:
             import torch.distributed as dist
 
-            t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
-            e = torch.tensor([ev], device=dev, dtype=torch.float64)
-            dist.all_reduce(e)
-            ev = int(e.item())
+            e2e_ms = _allreduce(e2e_ms, dev, dist.ReduceOp.MAX)
+            ev = int(_allreduce(ev, dev, dist.ReduceOp.SUM))
         if rank == 0:
             line["e2e"] = {"value": ev / (e2e_ms * 1e-3), "unit": "events/s",
                            "h2d_bytes_per_step": int(x_host.numel() * 4),
                            "d2h_bytes_per_step": int(raster_host.numel() * 4)}
+        del x_host, raster_host
     if args.ncu_window is not None:
         w0 = args.ncu_window
 
@@ -402,9 +535,24 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         S = args.cpu_sample_steps
         x_cpu = x[:S].cpu().numpy()
-        e, t, thr = cpu_sample(cfg, post, src, w, w_in, x_cpu, S)
+        e, t, thr = cpu_sample(cfg, net, x_cpu, S)
         line["cpu_baseline"] = {"value": e / t, "unit": "events/s", "cores": thr, "kind": "port",
                                 "sample": f"first {S} time steps of the {B}-sample batch ({t:.1f} s)"}
+    del rnn, x, lens, net, one_step
+    torch.cuda.empty_cache()
+    for extra in [e for e in args.extra.split(",") if e and e != args.config]:
+        ecfg = CONFIGS[extra]
+        sub, m, xe, le, ne, _ = measure(extra, ecfg, args, dev, world, rank, local)
+        if rank == 0 and world == 1:
+            sub["plain_step"] = plain_step(ecfg, ne, xe, le, args, dev)
+            sub["vs_plain_step"] = sub["value"] / sub["plain_step"]["value"]
+        if rank == 0:
+            for k in ("metric", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline",
+                      "dtype", "data"):
+                sub.pop(k, None)
+            line[extra] = sub
+        del m, xe, le, ne
+        torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -26,6 +26,9 @@ _i64 = C.c_int64
 _i32 = C.c_int32
 
 
+ABI_VERSION = 2  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
+
+
 class BtParam(C.Structure):
     _fields_ = [("ptr", _vp), ("stride", _i64)]
 
@@ -43,7 +46,7 @@ class BtNeuronDesc(C.Structure):
 class BtEngineDesc(C.Structure):
     _fields_ = [
         ("n", _i64), ("batch", _i64), ("n_bins", _i32), ("mode", _i32), ("t0", _i64), ("n_steps", _i64),
-        ("first_call", _i32), ("hist_len", _i32),
+        ("bin_lo", _i32), ("bin_hi", _i32), ("hist_len", _i32), ("scatter_lanes", _i32),
         ("neuron", BtNeuronDesc), ("psc_coef", BtParam), ("psc_tau", BtParam),
         ("csr_ptr", _vp), ("csr_dst", _vp), ("csr_w", _vp),
         ("csc_ptr", _vp), ("csc_src", _vp), ("csc_w", _vp),
@@ -72,13 +75,13 @@ _PROTOS = {
     "bt_neuron_step_backward": (C.c_int, [C.POINTER(BtNeuronDesc), _i64, _i64] + [_vp] * 13 + [_i32, _vp]),
     "bt_psc_step": (C.c_int, [_i64, _i64, BtParam, BtParam, _vp, _vp, _vp, _vp]),
     "bt_engine_run": (C.c_int, [C.POINTER(BtEngineDesc), _vp]),
-    "bt_engine_ring_from_history": (C.c_int, [C.POINTER(BtEngineDesc), _vp]),
+    "bt_engine_prime": (C.c_int, [C.POINTER(BtEngineDesc), _vp]),
     "bt_input_project": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_bits_to_float": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
     "bt_float_to_bits": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
     "bt_float_to_masks": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
     "bt_mask_stride": (C.c_int, [_i64]),
-    "bt_engine_work_words": (C.c_int64, [_i64, _i64]),
+    "bt_engine_work_words": (C.c_int64, [_i64, _i64, _i32]),
     "bt_masks_to_float": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
 }
 
@@ -107,6 +110,9 @@ def lib():
                 fn = getattr(h, name)
                 fn.restype = res
                 fn.argtypes = args
+            if h.bt_abi_version() != ABI_VERSION:
+                raise RuntimeError(f"{LIB_PATH} has ABI {h.bt_abi_version()}, this package needs {ABI_VERSION}; "
+                                   "rebuild it with `python -m btorch_b200.csrc.build`.")
             _lib = h
     return _lib
 

@@ -11,17 +11,22 @@
 //                                                 connection.py:973-1027)
 //
 // SCATTER mode, two launches per step:
-//   k_eng_neuron  (step t): P = stored + ring[(t-1) mod R]; zero that slot;
-//                 neuron update with I = P + x_t; stored = decay(P); spike
-//                 bitmaps; union of active presynaptic neurons compacted
-//                 (warp ballot + block prefix + one atomic per block).
-//   k_eng_scatter (step t): for each active neuron j (any sample), stream its
-//                 out-edges once with 128-bit loads and add w into
-//                 ring[(t + bin) mod R][b][post] for every sample b that
-//                 spiked (fp32 reductions, resolved in L2).
-//   "stored" holds decay(psc_{t-1}) during a run; the ring holds the pending
-//   sums of W z for every arrival step, so the reference's rounding of
-//   psc = decay(psc) + Wz is kept (exact sums when weights are dyadic).
+//   k_eng_neuron  (step t): P = stored + acc; zero acc; neuron update with
+//                 I = P + x_t; stored = decay(P); spike bitmaps; the step's
+//                 spike set: a mask of spiking samples per neuron and the
+//                 compacted list of neurons that spiked in any sample (warp
+//                 ballot + one warp-aggregated atomic on one of 64 counters).
+//   k_eng_scatter (step t): for every delay bin d and every neuron j in the
+//                 spike set of step t - d, stream the out-edges of row
+//                 j * R + d of the delay-expanded matrix with 128-bit loads
+//                 and add w into acc[b][post] for every sample b in j's mask
+//                 (fp32 reductions, resolved in L2: acc is [B][n], the size
+//                 of one state variable, whatever the delay range).
+//   The spike sets of the last R steps live in a ring of R + 1 slots (slot =
+//   step mod (R + 1)) in the scratch; the last reader of a set clears it.
+//   "stored" holds decay(psc_{t-1}) during a run and acc the sum W z of the
+//   step, so the reference's rounding of psc = decay(psc) + Wz is kept
+//   (exact sums when weights are dyadic).
 //
 // GATHER mode, one launch per step (k_eng_gather): each warp owns a neuron,
 //   computes P_{t-1} = decay(P_{t-2}) + sum over its in-edges (pre, bin) in
@@ -46,30 +51,26 @@ __host__ __device__ __forceinline__ int mask_stride(int64_t batch) {
 // Slot indices of one step, computed on the host per launch so that no kernel
 // evaluates a 64-bit modulo per element.
 struct StepIdx {
-  int r_in;    // (t - 1) mod R: ring slot the neuron phase consumes
-  int r_t;     // t mod R:       ring slot of delay bin 0 for spikes of step t
+  int q_t;     // t mod (R + 1): spike-set slot of step t (scatter)
   int h_t;     // t mod H:       history slot written at step t
   int h_prev;  // (t - 1) mod H: history slot of step t - 1
-  int par;     // t & 1
 };
 
 inline StepIdx step_idx(int64_t t, int R, int H) {
   StepIdx s;
-  s.r_in = int(((t - 1) % R + R) % R);
-  s.r_t = int(((t % R) + R) % R);
-  s.h_t = int(((t % H) + H) % H);
-  s.h_prev = int(((t - 1) % H + H) % H);
-  s.par = int(t & 1);
+  s.q_t = int(t % (R + 1));
+  s.h_t = int(t % H);
+  s.h_prev = int((t - 1) % H);
   return s;
 }
 
 // ---------------------------------------------------------------- scatter --
 
-// Scatter-mode scratch (d.work, int32 words):
-//   [0, 2*kSub)                    active-list counts, [parity][sub-list]
-//   [2*kSub, 2*kSub + 2n)          "listed" flags, [parity][neuron]
-//   next 2*kSub*cap                list entries, [parity][sub-list][cap]
-//   next 2 n S                     sample masks, [parity][neuron][S words], S = mask_stride(batch)
+// Scatter-mode scratch (d.work, int32 words), Q = R + 1 spike-set slots:
+//   [0, Q*kSub)                    active-list counts, [slot][sub-list]
+//   next Q*n                       "listed" flags, [slot][neuron]
+//   next Q*kSub*cap                list entries, [slot][sub-list][cap]
+//   next Q n S                     sample masks, [slot][neuron][S words], S = mask_stride(batch)
 // Sub-list s only lists neurons [s*cap, (s+1)*cap) and each neuron is listed at
 // most once per step (its flag), so a sub-list never holds more than cap
 // entries.  cap is a multiple of 32, so the 32 neurons of a warp share one
@@ -78,8 +79,9 @@ constexpr int kSub = 64;
 
 __host__ __device__ __forceinline__ int64_t sub_cap(int64_t n) { return (((n + kSub - 1) / kSub) + 31) / 32 * 32; }
 
-__host__ __device__ __forceinline__ int64_t scatter_work_words(int64_t n, int64_t batch) {
-  return 2 * kSub + 2 * n + 2 * kSub * sub_cap(n) + 2 * n * mask_stride(batch);
+__host__ __device__ __forceinline__ int64_t scatter_work_words(int64_t n, int64_t batch, int n_bins) {
+  const int64_t Q = int64_t(n_bins) + 1;
+  return Q * (kSub + n + kSub * sub_cap(n) + n * mask_stride(batch));
 }
 
 struct ScatterScratch {
@@ -91,15 +93,16 @@ struct ScatterScratch {
   int ms;
 };
 
-__device__ __forceinline__ ScatterScratch scatter_scratch(const bt_engine_desc& d, int par) {
+__device__ __forceinline__ ScatterScratch scatter_scratch(const bt_engine_desc& d, int q) {
   ScatterScratch w;
   const int64_t n = d.n;
+  const int64_t Q = int64_t(d.n_bins) + 1;
   w.ms = mask_stride(d.batch);
   w.cap = sub_cap(n);
-  w.count = d.work + par * kSub;
-  w.flag = d.work + 2 * kSub + par * n;
-  w.list = d.work + 2 * kSub + 2 * n + par * kSub * w.cap;
-  w.mask = reinterpret_cast<uint32_t*>(d.work + 2 * kSub + 2 * n + 2 * kSub * w.cap) + int64_t(par) * n * w.ms;
+  w.count = d.work + q * kSub;
+  w.flag = d.work + Q * kSub + q * n;
+  w.list = d.work + Q * kSub + Q * n + q * kSub * w.cap;
+  w.mask = reinterpret_cast<uint32_t*>(d.work + Q * kSub + Q * n + Q * kSub * w.cap) + int64_t(q) * n * w.ms;
   return w;
 }
 
@@ -118,7 +121,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   const int nb = int(B - b0 < S ? B - b0 : S);  // samples of this block (uniform)
   // Row pointers of sample b0 for this neuron; sample u is at +u * n.
   const int64_t off0 = b0 * n + (valid ? i : 0);
-  float* __restrict__ ring_p = d.ring + int64_t(si.r_in) * B * n + off0;
+  float* __restrict__ ring_p = d.ring + off0;  // acc: W z of the previous step
   float* __restrict__ psc_p = d.psc + off0;
   float* __restrict__ v_p = d.v + off0;
   float* __restrict__ ref_p = USE_REF ? d.refractory + off0 : nullptr;
@@ -192,7 +195,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   if (__ballot_sync(0xffffffffu, spiked != 0) == 0) return;  // warp-uniform
   // Publish the samples' bits in the neuron's mask; the first sample to spike
   // lists the neuron (one atomic per warp on one of kSub counters).
-  const ScatterScratch ws = scatter_scratch(d, si.par);
+  const ScatterScratch ws = scatter_scratch(d, si.q_t);
   bool first = false;
   if (spiked) {
     uint32_t* mrow = ws.mask + i * ws.ms;
@@ -210,54 +213,97 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   if (first) ws.list[sub * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = int32_t(i);
 }
 
-__global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, int64_t k, StepIdx si) {
-  const int64_t n = d.n, B = d.batch;
-  const int R = d.n_bins;
-  const int par = si.par;
-  const ScatterScratch ws = scatter_scratch(d, par);
-  __shared__ int32_t s_off[kSub + 1];
-  if (threadIdx.x == 0) {
-    int32_t acc = 0;
-    for (int q = 0; q < kSub; ++q) {
-      s_off[q] = acc;
-      acc += ws.count[q];
+// Offsets of the kSub sub-lists of one spike set in shared memory (warp 0
+// scans the counts; two per lane).
+__device__ __forceinline__ void sub_offsets(const int32_t* __restrict__ count, int32_t* s_off) {
+  if (threadIdx.x < 32) {
+    const int l = threadIdx.x;
+    const int32_t c0 = count[2 * l], c1 = count[2 * l + 1];
+    int32_t v = c0 + c1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, v, o);
+      if (l >= o) v += y;
     }
-    s_off[kSub] = acc;
+    s_off[2 * l] = v - c0 - c1;
+    s_off[2 * l + 1] = v - c1;
+    if (l == 31) s_off[kSub] = v;
   }
   __syncthreads();
-  const int32_t count = s_off[kSub];
-  if (blockIdx.x == 0 && threadIdx.x < kSub) {
-    // counts of the other parity were consumed by the previous step's scatter;
-    // clear them for the next step's neuron kernel
-    d.work[(par ^ 1) * kSub + threadIdx.x] = 0;
-    if (threadIdx.x == 0 && d.stats) d.stats[k * 4 + 0] = count;
+}
+
+// Sub-list holding item `it`: the last s with s_off[s] <= it (s_off[kSub] > it).
+__device__ __forceinline__ int find_sub(const int32_t* s_off, int64_t it) {
+  int lo = 0, hi = kSub - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (s_off[mid] <= it) lo = mid;
+    else hi = mid - 1;
   }
+  return lo;
+}
+
+// Grid (x, bin_hi - bin_lo + 1): plane y delivers delay bin d = bin_lo + y,
+// i.e. the spike set of step t - d through rows j * R + d.  G lanes share one
+// row (G = 32 for long rows, 8 for the short rows of a wide delay range), each
+// lane loading 4 edges with one 128-bit load of posts and one of weights.
+template <int G>
+__global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, int64_t k, StepIdx si) {
+  const int64_t n = d.n;
+  const int R = d.n_bins, Q = R + 1;
+  const int bin = d.bin_lo + int(blockIdx.y);
+  int q = si.q_t - bin;
+  if (q < 0) q += Q;
+  const ScatterScratch ws = scatter_scratch(d, q);
+  __shared__ int32_t s_off[kSub + 1];
+  sub_offsets(ws.count, s_off);
+  const int32_t count = s_off[kSub];
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < kSub) {
+    // the counts of slot (t + 1) mod Q, i.e. of step t - R, were last read by
+    // the previous step's scatter: clear them for the next neuron launch
+    const int qc = si.q_t + 1 == Q ? 0 : si.q_t + 1;
+    d.work[qc * kSub + threadIdx.x] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && d.stats)
+    atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 0), (unsigned long long)count);
+  const bool last_use = bin == d.bin_hi;  // this set is not read again: clear it
   const unsigned lane = lane_id();
+  const int grp = int(lane) / G, lig = int(lane) % G;
+  constexpr int kPerWarp = 32 / G;
   const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  const int t_mod_r = si.r_t;  // slot of bin b is t_mod_r + b (mod R), b < R
   const int ms = ws.ms;
   long long ev = 0, ed = 0;
-  for (int64_t it = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; it < count; it += warps) {
-    int sub = 0;
-    while (sub + 1 < kSub && s_off[sub + 1] <= it) ++sub;
-    const int32_t j = ws.list[sub * ws.cap + (it - s_off[sub])];
+  for (int64_t base = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kPerWarp; base < count;
+       base += warps * kPerWarp) {
+    const int64_t it = base + grp;
     uint32_t mw_local[8];
     int nsamp = 0;
-    uint32_t* mrow = ws.mask + int64_t(j) * ms;
+    int32_t beg = 0, end = 0;
+    uint32_t* mrow = nullptr;
+    int32_t j = -1;
+    if (it < count) {
+      const int sub = find_sub(s_off, it);
+      j = ws.list[sub * ws.cap + (it - s_off[sub])];
+      mrow = ws.mask + int64_t(j) * ms;
+      const int64_t row = int64_t(j) * R + bin;
+      beg = d.csr_ptr[row];
+      end = d.csr_ptr[row + 1];
+    }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      mw_local[q] = q < ms ? mrow[q] : 0u;
-      nsamp += __popc(mw_local[q]);
+    for (int w = 0; w < 8; ++w) {
+      mw_local[w] = (mrow && w < ms) ? mrow[w] : 0u;
+      nsamp += __popc(mw_local[w]);
     }
     __syncwarp();
-    if (lane == 0) {
-      for (int q = 0; q < ms; ++q) mrow[q] = 0;  // cleared for the step after next
+    if (last_use && lig == 0 && j >= 0) {
+      for (int w = 0; w < ms; ++w) mrow[w] = 0;
       ws.flag[j] = 0;
     }
-    const int32_t beg = d.csr_ptr[j], end = d.csr_ptr[j + 1];
-    ev += (long long)nsamp * (end - beg);
-    ed += end - beg;
-    for (int32_t gidx = (beg & ~3) + int32_t(lane) * 4; gidx < end; gidx += 128) {
+    if (lig == 0) {
+      ev += (long long)nsamp * (end - beg);
+      ed += end - beg;
+    }
+    for (int32_t gidx = (beg & ~3) + lig * 4; gidx < end; gidx += G * 4) {
       const uint4 d4 = __ldg(reinterpret_cast<const uint4*>(d.csr_dst + gidx));
       const float4 w4 = __ldg(reinterpret_cast<const float4*>(d.csr_w + gidx));
       const uint32_t dd[4] = {d4.x, d4.y, d4.z, d4.w};
@@ -266,36 +312,54 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, i
       for (int qq = 0; qq < 4; ++qq) {
         const int32_t e = gidx + qq;
         if (e < beg || e >= end) continue;
-        const uint32_t post = dd[qq] & kIdMask;
-        int slot = t_mod_r + int(dd[qq] >> BT_BIN_SHIFT);
-        if (slot >= R) slot -= R;
-        float* base = d.ring + (int64_t(slot) * B) * n + post;
+        float* dst = d.ring + (dd[qq] & kIdMask);
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          uint32_t m = mw_local[q];
+        for (int w = 0; w < 8; ++w) {
+          uint32_t m = mw_local[w];
           while (m) {
             const int l = __ffs(m) - 1;
             m &= m - 1;
-            atomicAdd(base + (int64_t(q) * 32 + l) * n, ww[qq]);
+            atomicAdd(dst + (int64_t(w) * 32 + l) * n, ww[qq]);
           }
         }
       }
     }
   }
-  if (d.stats && lane == 0 && ed) {
-    atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 1), (unsigned long long)ev);
-    atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 2), (unsigned long long)ed);
+  if (d.stats) {
+    // one pair of atomics per block: same-address atomics serialise in L2,
+    // so per-warp (or per-group) updates would cost more than the scatter
+    __shared__ long long s_ev[kEngThreads / 32], s_ed[kEngThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ev += __shfl_xor_sync(0xffffffffu, ev, o);
+      ed += __shfl_xor_sync(0xffffffffu, ed, o);
+    }
+    if (lane == 0) {
+      s_ev[threadIdx.x >> 5] = ev;
+      s_ed[threadIdx.x >> 5] = ed;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      long long tev = 0, ted = 0;
+      for (int w = 0; w < kEngThreads / 32; ++w) {
+        tev += s_ev[w];
+        ted += s_ed[w];
+      }
+      if (ted) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 1), (unsigned long long)tev);
+        atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 2), (unsigned long long)ted);
+      }
+    }
   }
 }
 
-// psc_{t_end-1} = stored + pending(t_end - 1); clears that slot.
-__global__ void k_eng_scatter_final(bt_engine_desc d, StepIdx si) {
+// psc_{t_end-1} = stored + acc; clears acc.
+__global__ void k_eng_scatter_final(bt_engine_desc d) {
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t n = d.n, B = d.batch;
   if (idx >= B * n) return;
-  float* ring = d.ring + (int64_t(si.r_t) * B) * n;
-  const float pending = ring[idx];
-  ring[idx] = 0.0f;
+  const float pending = d.ring[idx];
+  d.ring[idx] = 0.0f;
   const int64_t b = idx / n;
   const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
   if (d.n_steps - 1 < len) {
@@ -389,14 +453,21 @@ __global__ void __launch_bounds__(1024) k_eng_gather(bt_engine_desc d, int64_t k
         }
       }
     }
-    if (d.stats && lane == 0 && nspk) {
-      const long long deg = d.outdeg ? d.outdeg[i] : 0;
-      atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 0), 1ull);
-      atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 1), (unsigned long long)(nspk * deg));
-      atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 2), (unsigned long long)deg);
-    }
+  }
+  __shared__ long long s_stat[32][3];  // per warp: union, events, edges
+  if (d.stats && lane == 0) {
+    const long long deg = (i < n && nspk && d.outdeg) ? d.outdeg[i] : 0;
+    s_stat[wid][0] = nspk ? 1 : 0;
+    s_stat[wid][1] = nspk * deg;
+    s_stat[wid][2] = nspk ? deg : 0;
   }
   __syncthreads();
+  if (d.stats && threadIdx.x < 3) {
+    // one atomic per block and counter (same-address atomics serialise in L2)
+    long long tot = 0;
+    for (int q = 0; q < 32; ++q) tot += s_stat[q][threadIdx.x];
+    if (tot) atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + threadIdx.x), (unsigned long long)tot);
+  }
   const int64_t w = int64_t(blockIdx.x);
   for (int64_t b = threadIdx.x; b < B; b += blockDim.x) {
     d.hist[(int64_t(si.h_t) * B + b) * words + w] = sbits[b];
@@ -638,32 +709,49 @@ __global__ void k_masks_to_float(int64_t batch, int64_t n, const uint32_t* __res
   out[idx] = float((masks[i * mw + (b >> 5)] >> (b & 31)) & 1u);
 }
 
-// ------------------------------------------------------------ ring rebuild --
+// ---------------------------------------------------------- run priming --
 
-// One warp per (past step s, presynaptic neuron j): re-add the still-pending
-// contributions of z_s (arrivals >= t0) into the ring.
-__global__ void k_ring_from_history(bt_engine_desc d) {
-  const int64_t gw = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+// One thread per (steps ago a in 1..bin_hi, neuron i): the spike set of step
+// t0 - a rebuilt from the history bitmaps -- the mask of samples in which i
+// spiked, and i listed once if any did (warp-aggregated atomic).  Rows are
+// padded to whole 32-neuron words, so every warp has a single a.
+__global__ void k_prime_history(bt_engine_desc d) {
   const int64_t n = d.n, B = d.batch;
-  const int R = d.n_bins;
-  const int64_t back = R - 1;  // steps t0-1 .. t0-back can still have pending arrivals
-  if (gw >= back * n) return;
-  const int64_t s = d.t0 - 1 - gw / n;
-  const int64_t j = gw % n;
   const int64_t words = (n + 31) >> 5;
-  const int64_t H = d.hist_len;
-  const unsigned lane = lane_id();
-  const int32_t beg = d.csr_ptr[j], end = d.csr_ptr[j + 1];
-  for (int64_t b = 0; b < B; ++b) {
-    const uint32_t word = d.hist[((((s % H) + H) % H) * B + b) * words + (j >> 5)];
-    if (!((word >> (j & 31)) & 1u)) continue;
-    for (int32_t e = beg + int32_t(lane); e < end; e += 32) {
-      const uint32_t dd = d.csr_dst[e];
-      const int64_t arrival = s + (dd >> BT_BIN_SHIFT);
-      if (arrival < d.t0) continue;
-      atomicAdd(d.ring + ((arrival % R) * B + b) * n + (dd & kIdMask), d.csr_w[e]);
+  const int64_t npad = words * 32;
+  const int64_t gid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t a = 1 + gid / npad;
+  const int64_t i = gid - (a - 1) * npad;
+  if (a > d.bin_hi) return;  // whole warps
+  const int64_t s = d.t0 - a;  // >= 0: t0 >= hist_len > n_bins > bin_hi
+  const int64_t hs = s % d.hist_len;
+  const int q = int(s % (d.n_bins + 1));
+  const ScatterScratch ws = scatter_scratch(d, q);
+  uint32_t mw[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  bool any = false;
+  if (i < n) {
+    const uint32_t* h = d.hist + hs * B * words + (i >> 5);
+    for (int64_t b = 0; b < B; ++b) {
+      if ((h[b * words] >> (i & 31)) & 1u) {
+        mw[b >> 5] |= 1u << (b & 31);
+        any = true;
+      }
+    }
+    if (any) {
+#pragma unroll
+      for (int w = 0; w < 8; ++w)
+        if (w < ws.ms) ws.mask[i * ws.ms + w] = mw[w];
+      ws.flag[i] = 1;
     }
   }
+  const unsigned lane = lane_id();
+  const uint32_t fb = __ballot_sync(0xffffffffu, any);
+  if (fb == 0) return;
+  const int sub = int((i - lane) / ws.cap);
+  int32_t base = 0;
+  if (lane == 0) base = atomicAdd(ws.count + sub, __popc(fb));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (any) ws.list[sub * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = int32_t(i);
 }
 
 // ------------------------------------------------------- input projection --
@@ -772,6 +860,11 @@ int engine_check(const bt_engine_desc* d) {
   BT_CHECK_ARG(d->neuron.spiking, "the fused engine needs a spiking (Heaviside) forward");
   if (d->mode == BT_MODE_SCATTER) {
     BT_CHECK_ARG(d->csr_ptr && d->csr_dst && d->csr_w && d->ring && d->work, "scatter needs CSR, ring and work");
+    BT_CHECK_ARG(d->bin_lo >= 0 && d->bin_lo <= d->bin_hi && d->bin_hi < d->n_bins, "bins [%d, %d] outside [0, %d)",
+                 d->bin_lo, d->bin_hi, d->n_bins);
+    BT_CHECK_ARG(d->scatter_lanes == 0 || d->scatter_lanes == 8 || d->scatter_lanes == 32,
+                 "scatter_lanes=%d (0, 8 or 32)", d->scatter_lanes);
+    BT_CHECK_ARG(mask_stride(d->batch) <= 8, "scatter mode supports up to 256 samples");
     BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->csr_dst) & 15) == 0 &&
                      (reinterpret_cast<uintptr_t>(d->csr_w) & 15) == 0,
                  "CSR edge arrays must be 16-byte aligned and padded to a multiple of 4");
@@ -787,24 +880,24 @@ template <int KIND, bool HARD, bool USE_REF>
 int run_typed(const bt_engine_desc& d, cudaStream_t s) {
   const int64_t n = d.n;
   if (d.mode == BT_MODE_SCATTER) {
-    BT_CHECK_ARG(mask_stride(d.batch) <= 8, "scatter mode supports up to 256 samples");
     constexpr int S = 4;
     const dim3 grid(unsigned(ceil_div(n, kEngThreads)), unsigned(ceil_div(d.batch, S)));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t scratch_words = size_t(scatter_work_words(n, d.batch));
-    if (cudaMemsetAsync(d.work, 0, sizeof(int32_t) * scratch_words, s) != cudaSuccess)
-      return bt_set_error(BT_ERR_CUDA, "memset failed");
+    const unsigned planes = unsigned(d.bin_hi - d.bin_lo + 1);
+    const dim3 sgrid(unsigned(ceil_div(int64_t(sms) * 8, planes)), planes);
     for (int64_t k = 0; k < d.n_steps; ++k) {
       const StepIdx si = step_idx(d.t0 + k, d.n_bins, d.hist_len);
       k_eng_neuron<KIND, HARD, USE_REF, S><<<grid, kEngThreads, 0, s>>>(d, k, si);
-      k_eng_scatter<<<sms * 8, kEngThreads, 0, s>>>(d, k, si);
+      if (d.scatter_lanes == 8)
+        k_eng_scatter<8><<<sgrid, kEngThreads, 0, s>>>(d, k, si);
+      else
+        k_eng_scatter<32><<<sgrid, kEngThreads, 0, s>>>(d, k, si);
     }
     BT_CHECK_LAUNCH("k_eng_neuron/k_eng_scatter");
     if (d.n_steps > 0) {
-      const StepIdx si = step_idx(d.t0 + d.n_steps - 1, d.n_bins, d.hist_len);
-      k_eng_scatter_final<<<int(ceil_div(d.batch * n, 256)), 256, 0, s>>>(d, si);
+      k_eng_scatter_final<<<int(ceil_div(d.batch * n, 256)), 256, 0, s>>>(d);
       BT_CHECK_LAUNCH("k_eng_scatter_final");
     }
   } else if (d.mode == BT_MODE_PULL) {
@@ -876,14 +969,20 @@ extern "C" int bt_engine_run(const bt_engine_desc* d, void* stream) {
   return run_typed<BT_NEURON_ALIF, false, false>(*d, s);
 }
 
-extern "C" int bt_engine_ring_from_history(const bt_engine_desc* d, void* stream) {
+extern "C" int bt_engine_prime(const bt_engine_desc* d, void* stream) {
   if (int st = engine_check(d)) return st;
-  BT_CHECK_ARG(d->mode == BT_MODE_SCATTER, "the ring exists in scatter mode only");
-  const int64_t back = d->n_bins - 1;
-  if (back == 0) return BT_OK;
+  if (d->mode != BT_MODE_SCATTER) return BT_OK;
+  BT_CHECK_ARG(d->t0 >= d->hist_len, "t0=%lld must be >= hist_len", (long long)d->t0);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  k_ring_from_history<<<int(ceil_div(back * d->n * 32, 256)), 256, 0, s>>>(*d);
-  BT_CHECK_LAUNCH("k_ring_from_history");
+  const size_t words = size_t(scatter_work_words(d->n, d->batch, d->n_bins));
+  if (cudaMemsetAsync(d->work, 0, sizeof(int32_t) * words, s) != cudaSuccess ||
+      cudaMemsetAsync(d->ring, 0, sizeof(float) * size_t(d->batch * d->n), s) != cudaSuccess)
+    return bt_set_error(BT_ERR_CUDA, "memset failed");
+  if (d->bin_hi > 0) {
+    const int64_t npad = ((d->n + 31) >> 5) * 32;
+    k_prime_history<<<int(ceil_div(int64_t(d->bin_hi) * npad, 256)), 256, 0, s>>>(*d);
+    BT_CHECK_LAUNCH("k_prime_history");
+  }
   return BT_OK;
 }
 
@@ -917,8 +1016,8 @@ extern "C" int bt_bits_to_float(int64_t rows, int64_t n, const uint32_t* bits, f
 
 extern "C" int bt_mask_stride(int64_t batch) { return batch > 0 ? mask_stride(batch) : 0; }
 
-extern "C" int64_t bt_engine_work_words(int64_t n, int64_t batch) {
-  return (n > 0 && batch > 0) ? scatter_work_words(n, batch) : 0;
+extern "C" int64_t bt_engine_work_words(int64_t n, int64_t batch, int32_t n_bins) {
+  return (n > 0 && batch > 0 && n_bins >= 1 && n_bins <= BT_MAX_BINS) ? scatter_work_words(n, batch, n_bins) : 0;
 }
 
 extern "C" int bt_float_to_masks(int64_t batch, int64_t n, const float* in, uint32_t* masks, void* stream) {

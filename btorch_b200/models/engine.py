@@ -131,15 +131,12 @@ def _state2d(t: torch.Tensor, n: int) -> torch.Tensor:
 
 
 def graph_hist_len(n_bins: int) -> int:
-    """History ring length for graph replay: the smallest H >= n_bins + 2 that
-    is even and a multiple of n_bins, so that the delay-ring slot (t mod R),
-    the history slot (t mod H) and the scratch parity (t mod 2) all repeat with
+    """History ring length for graph replay: 2 (R + 1), a multiple of the
+    R + 1 spike-set slots of scatter mode and at least R + 2, so that the
+    spike-set slot (t mod (R + 1)) and the history slot (t mod H) repeat with
     period H -- every chunk of a multiple of H steps then launches with the
     same slot arguments, which a captured graph hard-wires."""
-    h = n_bins + 2
-    while h % n_bins or h % 2:
-        h += 1
-    return h
+    return 2 * (n_bins + 1)
 
 
 class _GraphEntry:
@@ -269,11 +266,14 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     desc.hist_len = H
     desc.csc_ptr, desc.csc_src, desc.csc_w = lay.csc_ptr.data_ptr(), lay.csc_src.data_ptr(), w.data_ptr()
     if mode == L.BT_MODE_SCATTER:
-        w_csr = static("w_csr", pack_csr_weights(lay, w))
+        lay_s = conn.scatter_layout(R, plan.uniform_delay, dev)
+        w_csr = static("w_csr", pack_csr_weights(lay_s, w))
         keep.append(w_csr)
-        desc.csr_ptr, desc.csr_dst, desc.csr_w = lay.csr_ptr.data_ptr(), lay.csr_dst.data_ptr(), w_csr.data_ptr()
-        ring = alloc("ring", (R, B, n), torch.float32, zero=True)
-        work = alloc("work", (L.lib().bt_engine_work_words(n, B),), torch.int32)
+        desc.csr_ptr, desc.csr_dst, desc.csr_w = lay_s.csr_ptr.data_ptr(), lay_s.csr_dst.data_ptr(), w_csr.data_ptr()
+        desc.bin_lo, desc.bin_hi = lay_s.bin_lo, lay_s.bin_hi
+        desc.scatter_lanes = 8 if lay_s.mean_row < 48 else 32
+        ring = alloc("ring", (B, n), torch.float32)  # W z of the step (bt_engine_prime clears it)
+        work = alloc("work", (L.lib().bt_engine_work_words(n, B, R),), torch.int32)
         keep += [ring, work]
         desc.ring, desc.work = ring.data_ptr(), work.data_ptr()
     if mode == L.BT_MODE_PULL:
@@ -315,10 +315,10 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             for d in range(hist_depth):
                 hist[(t0 - 1 - d) % H] = bits[d]
     desc.t0 = t0
-    if mode == L.BT_MODE_SCATTER and R > 1:
-        desc.n_steps = 1
-        L.check(L.lib().bt_engine_ring_from_history(C.byref(desc), s), "bt_engine_ring_from_history")
-        launches += 1
+    if mode == L.BT_MODE_SCATTER:
+        # spike sets of the history steps whose arrivals are still pending
+        L.check(L.lib().bt_engine_prime(C.byref(desc), s), "bt_engine_prime")
+        launches += 1 if desc.bin_hi > 0 else 0
 
     # outputs (graph: chunk-sized static buffers, copied out after each chunk)
     z = torch.empty((T, B, n), device=dev, dtype=torch.float32) if spikes_out == "dense" else None

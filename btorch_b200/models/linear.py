@@ -116,7 +116,31 @@ class BaseSparseConn(nn.Module):
             else:
                 lay = build_layout(self.indices, self.in_features // n_bins, self.out_features, n_bins)
             lay = lay.to(dev)
-            self._engine_layouts = {key: lay}
+            self._engine_layouts[key] = lay
+        return lay
+
+    def scatter_layout(self, n_bins: int, uniform_delay: int, device) -> SparseLayout:
+        """CSR over the rows pre * n_bins + bin of the delay-expanded matrix
+        (the fused engine's scatter mode), with the delay bins that hold edges
+        (`bin_lo`, `bin_hi`) and the mean length of a non-empty row."""
+        dev = torch.device(device)
+        key = ("scatter", n_bins, uniform_delay, str(dev))
+        lay = self._engine_layouts.get(key)
+        if lay is None:
+            if uniform_delay:
+                R = uniform_delay + 1
+                idx = torch.stack([self.indices[0], self.indices[1] * R + uniform_delay])
+                lay = build_layout(idx, self.in_features * R, self.out_features, 1)
+            else:
+                lay = build_layout(self.indices, self.in_features, self.out_features, 1)
+            rows = (lay.csr_ptr[1:] - lay.csr_ptr[:-1]).view(-1, n_bins)
+            per_bin = np.nonzero(rows.sum(0).numpy())[0]
+            bins = (int(per_bin[0]), int(per_bin[-1])) if per_bin.size else (0, 0)
+            mean_row = lay.nnz / max(1, int((rows > 0).sum()))
+            lay = lay.to(dev)
+            lay.bin_lo, lay.bin_hi = bins
+            lay.mean_row = mean_row
+            self._engine_layouts[key] = lay
         return lay
 
     def _apply(self, fn, recurse=True):

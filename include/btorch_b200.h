@@ -44,7 +44,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 1
+#define BT_ABI_VERSION 2
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -248,19 +248,25 @@ typedef struct bt_engine_desc {
   int32_t mode;           /* BT_MODE_SCATTER / BT_MODE_GATHER */
   int64_t t0;             /* absolute index of the first step of this call */
   int64_t n_steps;        /* steps in this call */
-  int32_t first_call;     /* 1: PSC state is psc after step t0-1 (normal) */
-  int32_t hist_len;       /* H: slots of the spike-history bitmap ring (>= n_bins) */
+  int32_t bin_lo;         /* scatter: lowest and highest delay bin that holds */
+  int32_t bin_hi;         /*   edges (0 <= bin_lo <= bin_hi < n_bins)        */
+  int32_t hist_len;       /* H: slots of the spike-history bitmap ring (>= n_bins + 2) */
+  int32_t scatter_lanes;  /* scatter: lanes per active row, 8 or 32 (0 = 32) */
 
   bt_neuron_desc neuron;
   bt_param psc_coef, psc_tau;  /* ExponentialPSC decay */
 
-  /* connectivity (n_pre == n) */
+  /* connectivity (n_pre == n).  Scatter: CSR over the rows pre * n_bins + bin
+     of the delay-expanded matrix, csr_dst = post, both edge arrays 16-byte
+     aligned and padded to a multiple of 4.  Gather: CSC by post with
+     csc_src = pre | bin << BT_BIN_SHIFT. */
   const int32_t* csr_ptr; const uint32_t* csr_dst; const float* csr_w;
   const int32_t* csc_ptr; const uint32_t* csc_src; const float* csc_w;
 
   /* state [batch, n], updated in place */
   float* v; float* refractory; float* g_k; float* psc;
-  float* ring;            /* [n_bins][batch][n] pending currents (scatter) */
+  float* ring;            /* [batch][n] scatter: synaptic input W z accumulated for the
+                             next neuron step (zero between runs) */
   uint32_t* hist;         /* [hist_len][batch][words] spike bitmaps, slot = step mod H */
 
   /* inputs */
@@ -289,24 +295,29 @@ typedef struct bt_engine_desc {
   int32_t pad1_;
 
   /* scratch (scatter mode) */
-  int32_t* work;          /* bt_engine_work_words(n, batch) int32; the engine clears it
-                             at the start of every call */
+  int32_t* work;          /* bt_engine_work_words(n, batch, n_bins) int32: the spike
+                             sets (active lists and sample masks) of the last
+                             n_bins steps; bt_engine_prime initialises it */
   int64_t* stats;         /* [n_steps][4]: active union, events, edges, 0; may be NULL */
 } bt_engine_desc;
 
 /* Scratch words (int32) the scatter mode needs in bt_engine_desc.work. */
-BT_API int64_t bt_engine_work_words(int64_t n, int64_t batch);
+BT_API int64_t bt_engine_work_words(int64_t n, int64_t batch, int32_t n_bins);
 
 /* Run n_steps recurrent steps.  Per step: I = psc + x; neuron update;
- * psc = psc + coef*((-psc)/tau) + W z (z through the delay ring). */
+ * psc = psc + coef*((-psc)/tau) + sum over delay bins d of W_d z_{t-d}.
+ * Scatter mode needs bt_engine_prime once per run. */
 BT_API int bt_engine_run(const bt_engine_desc* d, void* stream);
 
-/* Reload the pending-current ring from the spike-history bitmaps so that a
- * run can resume after the state was reset or replaced: for every spike
- * z_s in history (s in [t0 - n_bins + 1, t0 - 1]) and edge bin d with
- * s + d >= t0, add w into ring slot (s + d) mod n_bins.  The ring must be
- * zero on entry. */
-BT_API int bt_engine_ring_from_history(const bt_engine_desc* d, void* stream);
+/* Start a run in scatter mode (no-op in the other modes): clear work and
+ * ring, and list the spikes of steps t0 - bin_hi .. t0 - 1 (read from the
+ * hist bitmaps, slot = step mod hist_len) in their spike sets, so that their
+ * arrivals at steps >= t0 are delivered.  Call once before the first
+ * bt_engine_run of a run; later calls that continue the run (t0 advanced by
+ * the previous n_steps) must not prime again.  Replaces the reference's
+ * rebuild of the flattened delay history (btorch/models/history.py:299-345)
+ * at the start of a multi-step call. */
+BT_API int bt_engine_prime(const bt_engine_desc* d, void* stream);
 
 /* Input projection for DenseConn as neuron_inp_module (nn.Linear,
  * btorch/models/linear.py:163-228): out[r, i] = bias[i] + sum over nonzero
