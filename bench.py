@@ -423,6 +423,7 @@ def measure(name, cfg, args, dev, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Poisson input, random weights of the configuration's shape)",
             "config": {"workload": describe(name, cfg), "direction": rnn.last_engine_direction,
+                       "tuned": rnn.last_engine_choice.describe(),
                        "parallelism": f"replicas x{world}", "cudagraph": bool(rnn.cudagraph),
                        "l2": "working set (weights + input) exceeds the 126 MB L2; no flush"},
             "neuron_steps_per_s": n * live_steps / (elapsed_ms * 1e-3) if world == 1 else None,

@@ -55,7 +55,7 @@ class BtEngineDesc(C.Structure):
         ("raster", _vp), ("spikes", _vp), ("v_trace", _vp), ("psc_trace", _vp), ("ref_trace", _vp),
         ("gk_trace", _vp),
         ("sl_ptr", _vp), ("sl_src", _vp), ("sl_w", _vp), ("masks", _vp), ("outdeg", _vp),
-        ("pull_words_per_warp", _i32), ("pad1_", _i32),
+        ("pull_words_per_warp", _i32), ("neuron_spt", _i32),
         ("work", _vp), ("stats", _vp),
     ]
 

@@ -42,4 +42,53 @@ __device__ __forceinline__ float ld(const bt_param& p, int64_t i) { return __ldg
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
+// L2 eviction-priority hints (PTX createpolicy + .L2::cache_hint, sm_80+).
+// Data read once per step (edge lists, the step's input current) is loaded
+// evict-first so that it does not push the small, reused accumulators out of
+// L2; reductions into those accumulators are issued evict-last.
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// Read-only (non-coherent) loads with an L2 policy; not volatile, so the
+// compiler may batch them ahead of their uses.
+__device__ __forceinline__ uint4 ld_nc_u4(const void* ptr, uint64_t pol) {
+  uint4 v;
+  asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(ptr), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_nc_u32(const void* ptr, uint64_t pol) {
+  uint32_t v;
+  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(ptr), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_nc_f32(const float* ptr, uint64_t pol) {
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(ptr), "l"(pol));
+  return v;
+}
+// Coherent fp32 load / store with an L2 policy.
+__device__ __forceinline__ float ld_f32(const float* ptr, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(ptr), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_f32(float* ptr, float v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(ptr), "f"(v), "l"(pol) : "memory");
+}
+// fp32 reduction (no return value) with an L2 policy.
+__device__ __forceinline__ void red_add_f32(float* ptr, float v, uint64_t pol) {
+  // no "memory" clobber: nothing in the issuing kernel reads the target, so
+  // independent loads may be scheduled across the reduction
+  asm volatile("red.global.add.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(ptr), "f"(v), "l"(pol));
+}
+
 }  // namespace bt

@@ -33,6 +33,8 @@
 //   ascending canonical order of w * z_{t-1-bin}[pre] (fmaf chain, exactly the
 //   reference's CPU rounding), then runs the neuron update of step t.  The
 //   last synapse update of a run is k_eng_gather_final.
+#include <type_traits>
+
 #include "neuron.cuh"
 
 namespace bt {
@@ -128,13 +130,14 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   float* __restrict__ gk_p = KIND == BT_NEURON_ALIF ? d.g_k + off0 : nullptr;
   const float* __restrict__ x_p = d.x ? d.x + k * B * n + off0 : nullptr;
   float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
+  const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
 #pragma unroll
   for (int u = 0; u < S; ++u) {
     const bool in = valid && u < nb;
     const int64_t o = int64_t(u) * n;
-    pend[u] = in ? ring_p[o] : 0.0f;
+    pend[u] = in ? ld_f32(ring_p + o, pol_keep) : 0.0f;
     pv[u] = in ? psc_p[o] : 0.0f;
-    xv[u] = (in && x_p) ? x_p[o] : 0.0f;
+    xv[u] = (in && x_p) ? ld_nc_f32(x_p + o, pol_stream) : 0.0f;
     vv[u] = in ? v_p[o] : 0.0f;
     rv[u] = (in && USE_REF) ? ref_p[o] : 0.0f;
     gv[u] = (in && KIND == BT_NEURON_ALIF) ? gk_p[o] : 0.0f;
@@ -153,7 +156,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
     const int64_t o = int64_t(u) * n;
     float s = 0.0f;
     if (valid) {
-      ring_p[o] = 0.0f;
+      st_f32(ring_p + o, 0.0f, pol_keep);
       const int64_t len = d.sample_len ? d.sample_len[b0 + u] : INT64_MAX;
       float v = vv[u], ref = rv[u], gk = gv[u];
       float P;
@@ -243,11 +246,41 @@ __device__ __forceinline__ int find_sub(const int32_t* s_off, int64_t it) {
   return lo;
 }
 
+// Block-level sum of per-thread event / edge counts, one pair of atomics per
+// block (same-address atomics serialise in L2).  Every thread of the block
+// must call it.
+__device__ __forceinline__ void block_stats(const bt_engine_desc& d, int64_t k, long long ev, long long ed) {
+  __shared__ long long s_ev[kEngThreads / 32], s_ed[kEngThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ev += __shfl_xor_sync(0xffffffffu, ev, o);
+    ed += __shfl_xor_sync(0xffffffffu, ed, o);
+  }
+  if (lane_id() == 0) {
+    s_ev[threadIdx.x >> 5] = ev;
+    s_ed[threadIdx.x >> 5] = ed;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long tev = 0, ted = 0;
+    for (int w = 0; w < kEngThreads / 32; ++w) {
+      tev += s_ev[w];
+      ted += s_ed[w];
+    }
+    if (ted) {
+      atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 1), (unsigned long long)tev);
+      atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 2), (unsigned long long)ted);
+    }
+  }
+}
+
 // Grid (x, bin_hi - bin_lo + 1): plane y delivers delay bin d = bin_lo + y,
 // i.e. the spike set of step t - d through rows j * R + d.  G lanes share one
 // row (G = 32 for long rows, 8 for the short rows of a wide delay range), each
-// lane loading 4 edges with one 128-bit load of posts and one of weights.
-template <int G>
+// lane loading 4 edges with one 128-bit load of posts and one of weights, then
+// adding them for every sample in the row's mask (MS words; the sample loop is
+// outside the edge loop, so a lane issues 4 reductions per mask bit).
+template <int G, int MS>
 __global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, int64_t k, StepIdx si) {
   const int64_t n = d.n;
   const int R = d.n_bins, Q = R + 1;
@@ -271,86 +304,200 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, i
   const int grp = int(lane) / G, lig = int(lane) % G;
   constexpr int kPerWarp = 32 / G;
   const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  const int ms = ws.ms;
+  const int n32 = int(n);  // batch * n < 2^31 (checked on the host)
+  const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
   long long ev = 0, ed = 0;
   for (int64_t base = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kPerWarp; base < count;
        base += warps * kPerWarp) {
     const int64_t it = base + grp;
-    uint32_t mw_local[8];
-    int nsamp = 0;
+    uint32_t mw_local[MS];
     int32_t beg = 0, end = 0;
     uint32_t* mrow = nullptr;
     int32_t j = -1;
     if (it < count) {
       const int sub = find_sub(s_off, it);
       j = ws.list[sub * ws.cap + (it - s_off[sub])];
-      mrow = ws.mask + int64_t(j) * ms;
+      mrow = ws.mask + int64_t(j) * ws.ms;
       const int64_t row = int64_t(j) * R + bin;
       beg = d.csr_ptr[row];
       end = d.csr_ptr[row + 1];
     }
+    // MS is the compile-time bound (1, 2, 4 or 8); the row holds ws.ms words
+    // (5..8 samples words above 128 samples run with MS = 8)
+    int nsamp = 0;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) {
-      mw_local[w] = (mrow && w < ms) ? mrow[w] : 0u;
+    for (int w = 0; w < MS; ++w) {
+      mw_local[w] = (mrow && w < ws.ms) ? mrow[w] : 0u;
       nsamp += __popc(mw_local[w]);
     }
     __syncwarp();
     if (last_use && lig == 0 && j >= 0) {
-      for (int w = 0; w < ms; ++w) mrow[w] = 0;
+#pragma unroll
+      for (int w = 0; w < MS; ++w)
+        if (w < ws.ms) mrow[w] = 0;
       ws.flag[j] = 0;
     }
     if (lig == 0) {
       ev += (long long)nsamp * (end - beg);
       ed += end - beg;
     }
-    for (int32_t gidx = (beg & ~3) + lig * 4; gidx < end; gidx += G * 4) {
-      const uint4 d4 = __ldg(reinterpret_cast<const uint4*>(d.csr_dst + gidx));
-      const float4 w4 = __ldg(reinterpret_cast<const float4*>(d.csr_w + gidx));
-      const uint32_t dd[4] = {d4.x, d4.y, d4.z, d4.w};
-      const float ww[4] = {w4.x, w4.y, w4.z, w4.w};
+    // U quads per lane in flight: all loads of an iteration are issued before
+    // its reductions
+    constexpr int U = 2;
+    for (int32_t g0 = (beg & ~3) + lig * 4; g0 < end; g0 += G * 4 * U) {
+      uint4 dq[U], wq[U];
 #pragma unroll
-      for (int qq = 0; qq < 4; ++qq) {
-        const int32_t e = gidx + qq;
-        if (e < beg || e >= end) continue;
-        float* dst = d.ring + (dd[qq] & kIdMask);
+      for (int u = 0; u < U; ++u) {
+        const int32_t gi = g0 + u * G * 4;
+        if (gi < end) {
+          dq[u] = ld_nc_u4(d.csr_dst + gi, pol_stream);
+          wq[u] = ld_nc_u4(d.csr_w + gi, pol_stream);
+        } else {
+          dq[u] = make_uint4(0u, 0u, 0u, 0u);
+          wq[u] = dq[u];
+        }
+      }
 #pragma unroll
-        for (int w = 0; w < 8; ++w) {
+      for (int u = 0; u < U; ++u) {
+        const int32_t gidx = g0 + u * G * 4;
+        // edges outside [beg, end) of the first and last quad add nothing
+        const bool v0 = gidx >= beg && gidx < end, v1 = gidx + 1 >= beg && gidx + 1 < end,
+                   v2 = gidx + 2 >= beg && gidx + 2 < end, v3 = gidx + 3 >= beg && gidx + 3 < end;
+        const int p0 = int(dq[u].x & kIdMask), p1 = int(dq[u].y & kIdMask), p2 = int(dq[u].z & kIdMask),
+                  p3 = int(dq[u].w & kIdMask);
+#pragma unroll
+        for (int w = 0; w < MS; ++w) {
           uint32_t m = mw_local[w];
           while (m) {
             const int l = __ffs(m) - 1;
             m &= m - 1;
-            atomicAdd(dst + (int64_t(w) * 32 + l) * n, ww[qq]);
+            float* row = d.ring + (w * 32 + l) * n32;
+            if (v0) red_add_f32(row + p0, __uint_as_float(wq[u].x), pol_keep);
+            if (v1) red_add_f32(row + p1, __uint_as_float(wq[u].y), pol_keep);
+            if (v2) red_add_f32(row + p2, __uint_as_float(wq[u].z), pol_keep);
+            if (v3) red_add_f32(row + p3, __uint_as_float(wq[u].w), pol_keep);
           }
         }
       }
     }
   }
-  if (d.stats) {
-    // one pair of atomics per block: same-address atomics serialise in L2,
-    // so per-warp (or per-group) updates would cost more than the scatter
-    __shared__ long long s_ev[kEngThreads / 32], s_ed[kEngThreads / 32];
+  if (d.stats) block_stats(d, k, ev, ed);
+}
+
+// Scatter for short rows (a wide delay range splits each neuron's out-edges
+// into n_bins rows): a warp takes 32 rows, one per lane, scans their lengths
+// and walks their edges as one flattened range, 32 consecutive edges per
+// iteration -- each lane finds its row by a 5-step binary search over the
+// lanes' exclusive offsets (shuffles), so no lane idles on a short row and
+// consecutive lanes load consecutive edges.  Grid as k_eng_scatter.
+template <int MS>
+__global__ void __launch_bounds__(kEngThreads) k_eng_scatter_flat(bt_engine_desc d, int64_t k, StepIdx si) {
+  const int R = d.n_bins, Q = R + 1;
+  const int bin = d.bin_lo + int(blockIdx.y);
+  int q = si.q_t - bin;
+  if (q < 0) q += Q;
+  const ScatterScratch ws = scatter_scratch(d, q);
+  __shared__ int32_t s_off[kSub + 1];
+  sub_offsets(ws.count, s_off);
+  const int32_t count = s_off[kSub];
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < kSub) {
+    const int qc = si.q_t + 1 == Q ? 0 : si.q_t + 1;  // step t - R: last read by the previous step
+    d.work[qc * kSub + threadIdx.x] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && d.stats)
+    atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 0), (unsigned long long)count);
+  const bool last_use = bin == d.bin_hi;
+  const int lane = int(lane_id());
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const int n32 = int(d.n);  // batch * n < 2^31 (checked on the host)
+  const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
+  long long ev = 0, ed = 0;
+  for (int64_t base = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * 32; base < count;
+       base += warps * 32) {
+    const int64_t it = base + lane;
+    uint32_t mw[MS];
+    int32_t beg = 0, len = 0;
+    if (it < count) {
+      const int sub = find_sub(s_off, it);
+      const int32_t j = ws.list[sub * ws.cap + (it - s_off[sub])];
+      uint32_t* mrow = ws.mask + int64_t(j) * ws.ms;
+      const int64_t row = int64_t(j) * R + bin;
+      beg = d.csr_ptr[row];
+      len = d.csr_ptr[row + 1] - beg;
+      int nsamp = 0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      ev += __shfl_xor_sync(0xffffffffu, ev, o);
-      ed += __shfl_xor_sync(0xffffffffu, ed, o);
-    }
-    if (lane == 0) {
-      s_ev[threadIdx.x >> 5] = ev;
-      s_ed[threadIdx.x >> 5] = ed;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      long long tev = 0, ted = 0;
-      for (int w = 0; w < kEngThreads / 32; ++w) {
-        tev += s_ev[w];
-        ted += s_ed[w];
+      for (int w = 0; w < MS; ++w) {
+        mw[w] = w < ws.ms ? mrow[w] : 0u;
+        nsamp += __popc(mw[w]);
       }
-      if (ted) {
-        atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 1), (unsigned long long)tev);
-        atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 2), (unsigned long long)ted);
+      if (last_use) {
+#pragma unroll
+        for (int w = 0; w < MS; ++w)
+          if (w < ws.ms) mrow[w] = 0;
+        ws.flag[j] = 0;
+      }
+      ev += (long long)nsamp * len;
+      ed += len;
+    } else {
+#pragma unroll
+      for (int w = 0; w < MS; ++w) mw[w] = 0u;
+    }
+    // exclusive offsets of the 32 rows in the flattened edge range
+    int32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int32_t excl = incl - len;
+    const int32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    // U edges per lane in flight: the row searches and loads of an iteration
+    // come before its reductions
+    constexpr int U = 4;
+    for (int32_t e0 = 0; e0 < total; e0 += 32 * U) {
+      int pp[U];
+      float wv[U];
+      uint32_t mm[U][MS];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int32_t e = e0 + u * 32 + lane;
+        // r = the last lane whose excl <= e (rows of length 0 are skipped over)
+        int r = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int32_t x = __shfl_sync(0xffffffffu, excl, r + step);
+          if (x <= e) r += step;
+        }
+        const int32_t rbeg = __shfl_sync(0xffffffffu, beg, r);
+        const int32_t rexcl = __shfl_sync(0xffffffffu, excl, r);
+#pragma unroll
+        for (int w = 0; w < MS; ++w) mm[u][w] = __shfl_sync(0xffffffffu, mw[w], r);
+        pp[u] = 0;
+        wv[u] = 0.0f;
+        if (e < total) {
+          const int32_t g = rbeg + (e - rexcl);
+          pp[u] = int(ld_nc_u32(d.csr_dst + g, pol_stream) & kIdMask);
+          wv[u] = ld_nc_f32(d.csr_w + g, pol_stream);
+        } else {
+#pragma unroll
+          for (int w = 0; w < MS; ++w) mm[u][w] = 0u;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+#pragma unroll
+        for (int w = 0; w < MS; ++w) {
+          uint32_t m = mm[u][w];
+          while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            red_add_f32(d.ring + (w * 32 + l) * n32 + pp[u], wv[u], pol_keep);
+          }
+        }
       }
     }
   }
+  if (d.stats) block_stats(d, k, ev, ed);
 }
 
 // psc_{t_end-1} = stored + acc; clears acc.
@@ -862,9 +1009,12 @@ int engine_check(const bt_engine_desc* d) {
     BT_CHECK_ARG(d->csr_ptr && d->csr_dst && d->csr_w && d->ring && d->work, "scatter needs CSR, ring and work");
     BT_CHECK_ARG(d->bin_lo >= 0 && d->bin_lo <= d->bin_hi && d->bin_hi < d->n_bins, "bins [%d, %d] outside [0, %d)",
                  d->bin_lo, d->bin_hi, d->n_bins);
-    BT_CHECK_ARG(d->scatter_lanes == 0 || d->scatter_lanes == 8 || d->scatter_lanes == 32,
-                 "scatter_lanes=%d (0, 8 or 32)", d->scatter_lanes);
+    BT_CHECK_ARG(d->scatter_lanes == 0 || d->scatter_lanes == 1 || d->scatter_lanes == 8 || d->scatter_lanes == 32,
+                 "scatter_lanes=%d (0, 1, 8 or 32)", d->scatter_lanes);
     BT_CHECK_ARG(mask_stride(d->batch) <= 8, "scatter mode supports up to 256 samples");
+    BT_CHECK_ARG(d->batch * d->n < (int64_t(1) << 31), "scatter mode needs batch * n < 2^31");
+    BT_CHECK_ARG(d->neuron_spt == 0 || d->neuron_spt == 1 || d->neuron_spt == 2 || d->neuron_spt == 4,
+                 "neuron_spt=%d (0, 1, 2 or 4)", d->neuron_spt);
     BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->csr_dst) & 15) == 0 &&
                      (reinterpret_cast<uintptr_t>(d->csr_w) & 15) == 0,
                  "CSR edge arrays must be 16-byte aligned and padded to a multiple of 4");
@@ -880,20 +1030,30 @@ template <int KIND, bool HARD, bool USE_REF>
 int run_typed(const bt_engine_desc& d, cudaStream_t s) {
   const int64_t n = d.n;
   if (d.mode == BT_MODE_SCATTER) {
-    constexpr int S = 4;
+    const int S = d.neuron_spt > 0 ? d.neuron_spt : 4;
     const dim3 grid(unsigned(ceil_div(n, kEngThreads)), unsigned(ceil_div(d.batch, S)));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const unsigned planes = unsigned(d.bin_hi - d.bin_lo + 1);
     const dim3 sgrid(unsigned(ceil_div(int64_t(sms) * 8, planes)), planes);
+    const int ms = mask_stride(d.batch);
+    auto neuron = S == 1 ? k_eng_neuron<KIND, HARD, USE_REF, 1>
+                : S == 2 ? k_eng_neuron<KIND, HARD, USE_REF, 2> : k_eng_neuron<KIND, HARD, USE_REF, 4>;
+    auto pick = [&](auto g) {
+      constexpr int G = decltype(g)::value;
+      // MS >= ms: mask_stride gives 1, 2, 4, or 5..8 words (MS = 8)
+    return ms == 1 ? k_eng_scatter<G, 1> : ms == 2 ? k_eng_scatter<G, 2> : ms <= 4 ? k_eng_scatter<G, 4>
+                                                                                      : k_eng_scatter<G, 8>;
+    };
+    auto scatter = d.scatter_lanes == 1   ? (ms == 1 ? k_eng_scatter_flat<1> : ms == 2 ? k_eng_scatter_flat<2>
+                                             : ms <= 4 ? k_eng_scatter_flat<4> : k_eng_scatter_flat<8>)
+                   : d.scatter_lanes == 8 ? pick(std::integral_constant<int, 8>())
+                                          : pick(std::integral_constant<int, 32>());
     for (int64_t k = 0; k < d.n_steps; ++k) {
       const StepIdx si = step_idx(d.t0 + k, d.n_bins, d.hist_len);
-      k_eng_neuron<KIND, HARD, USE_REF, S><<<grid, kEngThreads, 0, s>>>(d, k, si);
-      if (d.scatter_lanes == 8)
-        k_eng_scatter<8><<<sgrid, kEngThreads, 0, s>>>(d, k, si);
-      else
-        k_eng_scatter<32><<<sgrid, kEngThreads, 0, s>>>(d, k, si);
+      neuron<<<grid, kEngThreads, 0, s>>>(d, k, si);
+      scatter<<<sgrid, kEngThreads, 0, s>>>(d, k, si);
     }
     BT_CHECK_LAUNCH("k_eng_neuron/k_eng_scatter");
     if (d.n_steps > 0) {

@@ -19,6 +19,7 @@ import torch
 import torch.nn as nn
 
 from .. import _lib as L
+from . import autotune as _autotune
 from . import environ
 from ._ops import build_slices, neuron_desc, pack_csr_weights, pack_slice_weights
 from .functional import named_hidden_states
@@ -173,7 +174,7 @@ def graph_entries(rnn) -> dict:
 
 def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None = None,
         chunk: int | None = None, spikes_out: str = "dense", stats: bool = False, profile: list | None = None,
-        chunk_hook=None):
+        chunk_hook=None, choice: _autotune.EngineChoice | None = None):
     """Run T = x.shape[0] steps.  Returns (z [T, *batch, n] or bitmaps, states).
 
     With rnn.cudagraph the steps run in chunks of K (a multiple of the slot
@@ -188,7 +189,9 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     appended for every input-projection ("project") and recurrent-step
     ("step") launch group, recorded on the launching stream.
     chunk_hook: called as chunk_hook(k0) before the launches of the chunk
-    that starts at step k0 (e.g. to open a profiler window)."""
+    that starts at step k0 (e.g. to open a profiler window).
+    choice: delivery mode and tiles (default: the autotuner's cached or fresh
+    choice for this problem shape, see autotune.py)."""
     launches = 0
 
     def _ev():
@@ -214,18 +217,15 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     c_in = int(x.shape[-1]) if inp is not None else n
     trace_kinds = sorted(k for k in set(plan.paths.values()) if k != "history")
 
-    direction = conn.direction(B)
-    if direction == "gather":
-        # ordered pull: warp per post for tiny batches, sliced lane-per-post otherwise
-        mode = L.BT_MODE_PULL if B >= conn.sparse_config.pull_min_batch else L.BT_MODE_GATHER
-    else:
-        mode = L.BT_MODE_SCATTER
+    if choice is None:
+        choice = _autotune.choose(plan, rnn, x, sample_len, run)
+    mode = choice.mode
 
     use_graph = bool(getattr(rnn, "cudagraph", False))
     if use_graph:
         H = graph_hist_len(R)
         K = H * max(1, round(int(chunk or DEFAULT_GRAPH_CHUNK) / H))
-        gkey = (str(dev), B, n, c_in, mode, R, H, K, spikes_out, tuple(trace_kinds), bool(stats),
+        gkey = (str(dev), B, n, c_in, choice, R, H, K, spikes_out, tuple(trace_kinds), bool(stats),
                 sample_len is not None, inp is not None)
         entry = graph_entries(rnn).setdefault(gkey, _GraphEntry())
 
@@ -271,7 +271,8 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         keep.append(w_csr)
         desc.csr_ptr, desc.csr_dst, desc.csr_w = lay_s.csr_ptr.data_ptr(), lay_s.csr_dst.data_ptr(), w_csr.data_ptr()
         desc.bin_lo, desc.bin_hi = lay_s.bin_lo, lay_s.bin_hi
-        desc.scatter_lanes = 8 if lay_s.mean_row < 48 else 32
+        desc.scatter_lanes = choice.scatter_lanes or (1 if lay_s.mean_row < 48 else 32)
+        desc.neuron_spt = choice.neuron_spt or 4
         ring = alloc("ring", (B, n), torch.float32)  # W z of the step (bt_engine_prime clears it)
         work = alloc("work", (L.lib().bt_engine_work_words(n, B, R),), torch.int32)
         keep += [ring, work]
@@ -286,6 +287,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         keep += [sl_w, masks]
         desc.sl_ptr, desc.sl_src, desc.sl_w = sl.sl_ptr.data_ptr(), sl.sl_src.data_ptr(), sl_w.data_ptr()
         desc.masks = masks.data_ptr()
+        desc.pull_words_per_warp = choice.pull_words
     if stats:
         outdeg = static("outdeg", (lay.csr_ptr[1:] - lay.csr_ptr[:-1]).to(torch.int32).contiguous())
         keep.append(outdeg)
@@ -486,6 +488,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     rnn.last_engine_direction = {L.BT_MODE_SCATTER: "scatter", L.BT_MODE_GATHER: "gather",
                                  L.BT_MODE_PULL: "pull"}[mode]
     rnn.last_engine_launches = launches
+    rnn.last_engine_choice = choice
     if z is not None:
         z = z.view(T, *batch_shape, *neuron.n_neuron)
         return z, states

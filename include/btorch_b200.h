@@ -251,7 +251,9 @@ typedef struct bt_engine_desc {
   int32_t bin_lo;         /* scatter: lowest and highest delay bin that holds */
   int32_t bin_hi;         /*   edges (0 <= bin_lo <= bin_hi < n_bins)        */
   int32_t hist_len;       /* H: slots of the spike-history bitmap ring (>= n_bins + 2) */
-  int32_t scatter_lanes;  /* scatter: lanes per active row, 8 or 32 (0 = 32) */
+  int32_t scatter_lanes;  /* scatter: lanes per active row, 8 or 32, or 1 = the 32
+                             rows of a warp walked as one flattened edge range
+                             (short rows); 0 = 32 */
 
   bt_neuron_desc neuron;
   bt_param psc_coef, psc_tau;  /* ExponentialPSC decay */
@@ -292,7 +294,8 @@ typedef struct bt_engine_desc {
   int32_t pull_words_per_warp; /* pull mode: 32-sample mask words one warp covers:
                                   0 or 1 = one word per warp (default), or the whole
                                   bt_mask_stride(batch) when that is 2 or 4 */
-  int32_t pad1_;
+  int32_t neuron_spt;     /* scatter: samples per thread of the neuron launch, 1, 2 or 4
+                             (0 = 4) */
 
   /* scratch (scatter mode) */
   int32_t* work;          /* bt_engine_work_words(n, batch, n_bins) int32: the spike
