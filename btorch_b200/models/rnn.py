@@ -85,14 +85,28 @@ class RecurrentNNAbstract(base.MemoryModule):
         return zs, states
 
     def _checkpointed_chunk(self, *chunk_args, loop_args=(0,), **kwargs):
+        """One chunk under activation checkpointing (rnn.py:177-197): the
+        forward keeps only the chunk's inputs and entry state; backward
+        recomputes the chunk from them.  The recomputation runs on the
+        modules themselves, so it restores the modules' state afterwards --
+        the reference leaves them at wherever the (possibly early-stopped)
+        recomputation got to, which truncated BPTT would then continue from."""
         memories = named_hidden_states(self)
         env = environ.all()
+        calls = [0]
 
         def _pure(env, memories, *inner):
-            set_hidden_states(self, memories)
-            with environ.context(**env):
-                zs, st = self._process_chunk(*inner, loop_args=loop_args, **kwargs)
-            return torch.stack(zs), {k: torch.stack(v) for k, v in st.items()}
+            recompute = calls[0] > 0
+            calls[0] += 1
+            current = dict(named_hidden_states(self)) if recompute else None
+            try:
+                set_hidden_states(self, memories)
+                with environ.context(**env):
+                    zs, st = self._process_chunk(*inner, loop_args=loop_args, **kwargs)
+                return torch.stack(zs), {k: torch.stack(v) for k, v in st.items()}
+            finally:
+                if recompute:
+                    set_hidden_states(self, current)
 
         return checkpoint(_pure, env, memories, *chunk_args, use_reentrant=False)
 

@@ -226,9 +226,87 @@ TRACE_STEPS = 40
 GAIN = {"c1": 1.0, "soft": 0.6, "inp": 4.0, "alif": 0.6, "delay": 0.5}
 
 
+def case_train(rng, *, n, p, batch, steps, windows, c_in, n_out, spiking, chunk, unroll):
+    """Truncated-BPTT training windows: LIF (sigmoid surrogate, alpha 5) +
+    ExponentialPSC + SparseConn, DenseConn input, linear readout of the spikes
+    to sinusoid targets, MSE; RecurrentNN with grad_checkpoint over chunks.
+    Per window: forward, backward, gradients recorded, detach_net (no
+    optimizer step, so every window uses the same weights).
+
+    The backward recomputes the checkpointed chunks through RecurrentNN's
+    _pure (rnn.py:187-195), which rebinds the module state to each chunk's
+    recomputation, and torch's non-reentrant checkpoint may stop a
+    recomputation early -- so after backward the reference's modules hold a
+    state that depends on autograd internals.  The forward's final state is
+    therefore saved before backward and restored after it, which is the
+    state truncated BPTT continues from."""
+    import scipy.sparse as sp
+    import torch
+    from btorch.models import environ
+    from btorch.models.functional import detach_net, init_net_state, named_hidden_states, set_hidden_states
+    from btorch.models.linear import DenseConn, SparseConn
+    from btorch.models.neurons import LIF
+    from btorch.models.rnn import RecurrentNN
+    from btorch.models.surrogate import Sigmoid
+    from btorch.models.synapse import ExponentialPSC
+
+    Wd = make_conn(rng, n, n, p, dyadic=True, dy_exp=-6)
+    conn = SparseConn(sp.coo_array(Wd), sparse_backend="native")
+    neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=2.0, hard_reset=True,
+                 surrogate_function=Sigmoid(alpha=5.0, spiking=spiking))
+    syn = ExponentialPSC(n, tau_syn=5.0, linear=conn)
+    W_in = (np.round(rng.normal(0.0, 0.3, size=(c_in, n)) * 64.0) / 64.0).astype(np.float32)
+    inp = DenseConn(c_in, n, weight=torch.tensor(W_in))
+    W_out = (np.round(rng.normal(0.0, 0.5, size=(n_out, n)) * 64.0) / 64.0).astype(np.float32)
+    b_out = (np.round(rng.normal(0.0, 0.5, size=n_out) * 64.0) / 64.0).astype(np.float32)
+    readout = torch.nn.Linear(n, n_out)
+    with torch.no_grad():
+        readout.weight.copy_(torch.tensor(W_out))
+        readout.bias.copy_(torch.tensor(b_out))
+    brain = RecurrentNN(neuron, syn, neuron_inp_module=inp, update_state_names=("neuron.v",),
+                        grad_checkpoint=True, chunk_size=chunk, unroll=unroll)
+    init_net_state(brain, batch_size=batch, dtype=torch.float32)
+    T = steps * windows
+    x = rng.poisson(0.3, size=(T, batch, c_in)).astype(np.float32)
+    freq = rng.uniform(1.0, 20.0, size=(1, batch, n_out))
+    phase = rng.uniform(0.0, 2 * np.pi, size=(1, batch, n_out))
+    t = np.arange(T, dtype=np.float64)[:, None, None]
+    target = np.sin(2 * np.pi * freq * t * 1e-3 + phase).astype(np.float32)
+    out = dict(n=n, batch=batch, steps=steps, windows=windows, c_in=c_in, n_out=n_out, spiking=int(spiking),
+               chunk=chunk, unroll=unroll, tau=np.float32(20.0), tau_ref=np.float32(2.0), alpha=np.float32(5.0),
+               psc_tau=np.float32(5.0), W_in=W_in, W_out=W_out, b_out=b_out, x=x, target=target)
+    post, src, w = canonical(Wd)
+    out.update(post=post, src=src, w=w)
+    assert np.array_equal(conn.indices[0].numpy(), post) and np.array_equal(conn.indices[1].numpy(), src)
+    zs, losses = [], []
+    with environ.context(dt=1.0):
+        for k in range(windows):
+            sl = slice(k * steps, (k + 1) * steps)
+            z, _ = brain(torch.tensor(x[sl]))
+            y = readout(z)
+            loss = ((y - torch.tensor(target[sl])) ** 2).mean()
+            final = dict(named_hidden_states(brain))
+            for m in (brain, readout):
+                m.zero_grad(set_to_none=True)
+            loss.backward()
+            set_hidden_states(brain, final)
+            out[f"grad_w_{k}"] = conn.magnitude.grad.numpy().copy()
+            out[f"grad_win_{k}"] = inp.weight.grad.numpy().copy()  # (n, c_in) like DenseConn.weight
+            out[f"grad_wout_{k}"] = readout.weight.grad.numpy().copy()
+            out[f"grad_bout_{k}"] = readout.bias.grad.numpy().copy()
+            losses.append(float(loss.detach()))
+            zs.append(z.detach().numpy())
+            detach_net(brain)
+    out["loss"] = np.array(losses, np.float32)
+    out["z"] = np.packbits(np.concatenate(zs).astype(np.uint8) if spiking else (np.concatenate(zs) > 0.5),
+                           axis=-1, bitorder="little")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default="", help="comma-separated case names (default: all)")
     args = ap.parse_args()
     _import_reference(args.ref)
     import torch
@@ -246,14 +324,21 @@ def main():
         "alif_exppsc": lambda r: case_alif(r, n=320, p=0.05, batch=3, steps=150, dyadic=False),
         "delayed_psc": lambda r: case_delayed(r, n=256, p=0.05, batch=2, steps=120, D=3),
         "hetero_delay": lambda r: case_hetero(r, n=256, p=0.05, batch=2, steps=120, D=6),
+        "train_spiking": lambda r: case_train(r, n=96, p=0.1, batch=3, steps=30, windows=2, c_in=16, n_out=4,
+                                              spiking=True, chunk=10, unroll=5),
+        "train_smooth": lambda r: case_train(r, n=96, p=0.1, batch=3, steps=30, windows=2, c_in=16, n_out=4,
+                                             spiking=False, chunk=10, unroll=5),
     }
+    only = set(args.only.split(",")) if args.only else None
     for i, (name, fn) in enumerate(cases.items()):
+        if only is not None and name not in only:
+            continue
         rng = np.random.default_rng(1000 + i)
         d = fn(rng)
         # Full spike rasters (bit-packed) are kept; float traces only for the
         # first TRACE_STEPS steps, plus the state after the last step.
         for key in ("v", "psc", "g_k"):
-            if key in d and "z" in d:
+            if key in d and "z" in d and d[key].ndim == 3:
                 d[key + "_final"] = d[key][-1]
                 d[key] = d[key][:TRACE_STEPS]
         np.savez_compressed(OUT / f"{name}.npz", **d)

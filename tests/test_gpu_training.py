@@ -1,0 +1,127 @@
+"""Surrogate-gradient BPTT through the hand-written backward kernels.
+
+* Against the reference's own autograd (tests/golden/train_*.npz, made by
+  make_golden.py from the reference on the CPU): truncated-BPTT windows with
+  checkpointed chunks, LIF + ExponentialPSC + SparseConn + DenseConn input,
+  linear readout, MSE -- loss and every parameter gradient within 1e-4
+  relative (norm-wise), spike rasters identical.
+* Against finite differences of the smooth-surrogate forward (sigmoid spikes).
+"""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import torch
+
+from btorch_b200.models import LIF, DenseConn, ExponentialPSC, RecurrentNN, Sigmoid, SparseConn, environ
+from btorch_b200.models.functional import detach_net, init_net_state
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+
+
+def build(d, direction="gather", refractory=True, alpha=None):
+    n = int(d["n"])
+    W = sp.coo_array((d["w"], (d["src"], d["post"])), shape=(n, n))
+    conn = SparseConn(W, sparse_config={"direction": direction})
+    tau_ref = float(d["tau_ref"]) if refractory else None
+    neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=float(d["tau"]), tau_ref=tau_ref, hard_reset=True,
+                 surrogate_function=Sigmoid(alpha=float(d["alpha"]) if alpha is None else alpha,
+                                            spiking=bool(d["spiking"])))
+    syn = ExponentialPSC(n, tau_syn=float(d["psc_tau"]), linear=conn)
+    inp = DenseConn(int(d["c_in"]), n, weight=torch.tensor(d["W_in"]))
+    brain = RecurrentNN(neuron, syn, neuron_inp_module=inp, update_state_names=("neuron.v",), grad_checkpoint=True,
+                        chunk_size=int(d["chunk"]), unroll=int(d["unroll"])).to(DEV)
+    readout = torch.nn.Linear(n, int(d["n_out"])).to(DEV)
+    with torch.no_grad():
+        readout.weight.copy_(torch.tensor(d["W_out"]))
+        readout.bias.copy_(torch.tensor(d["b_out"]))
+    init_net_state(brain, batch_size=int(d["batch"]), dtype=torch.float32, device=DEV)
+    return brain, readout, conn, inp
+
+
+def train_windows(d, direction="gather"):
+    brain, readout, conn, inp = build(d, direction)
+    steps, windows = int(d["steps"]), int(d["windows"])
+    x = torch.tensor(d["x"], device=DEV)
+    target = torch.tensor(d["target"], device=DEV)
+    out = {"loss": [], "z": []}
+    with environ.context(dt=1.0):
+        for k in range(windows):
+            sl = slice(k * steps, (k + 1) * steps)
+            z, _ = brain(x[sl])
+            assert brain.last_path == "modular"
+            loss = ((readout(z) - target[sl]) ** 2).mean()
+            for m in (brain, readout):
+                m.zero_grad(set_to_none=True)
+            loss.backward()
+            out[f"grad_w_{k}"] = conn.magnitude.grad.cpu().numpy()
+            out[f"grad_win_{k}"] = inp.weight.grad.cpu().numpy()
+            out[f"grad_wout_{k}"] = readout.weight.grad.cpu().numpy()
+            out[f"grad_bout_{k}"] = readout.bias.grad.cpu().numpy()
+            out["loss"].append(float(loss.detach()))
+            out["z"].append(z.detach().cpu().numpy())
+            detach_net(brain)
+    return out
+
+
+def rel_err(a, b):
+    return float(np.linalg.norm(a.astype(np.float64) - b) / max(np.linalg.norm(b.astype(np.float64)), 1e-30))
+
+
+@pytest.mark.parametrize("direction", ["gather", "scatter"])
+@pytest.mark.parametrize("name", ["train_spiking", "train_smooth"])
+def test_bptt_gradients_match_reference_autograd(name, direction):
+    d = cases.load(name)
+    out = train_windows(d, direction)
+    n = int(d["n"])
+    z = np.concatenate(out["z"])
+    if int(d["spiking"]):
+        ref_z = np.unpackbits(d["z"], axis=-1, bitorder="little")[..., :n]
+        np.testing.assert_array_equal(z.astype(np.uint8), ref_z)
+    np.testing.assert_allclose(out["loss"], d["loss"], rtol=1e-5)
+    for k in range(int(d["windows"])):
+        for g in ("grad_w", "grad_win", "grad_wout", "grad_bout"):
+            key = f"{g}_{k}"
+            assert rel_err(out[key], d[key]) < 1e-4, (key, rel_err(out[key], d[key]))
+
+
+def test_bptt_matches_finite_differences_smooth():
+    """Analytic gradient of the smooth-surrogate forward against central
+    differences of the same forward (fp32, the 6 largest-gradient weights of
+    the recurrent and input layers).  The surrogate backward is
+    4 s (1 - s) with s = sigmoid(k alpha u) (sigmoid.py:17-56) whatever the
+    forward; with k alpha = 4 it is the exact derivative of the smooth
+    forward, so finite differences must agree.  No refractory period: its mask
+    (refractory == 0) is a step function of the smooth spike."""
+    d = cases.load("train_smooth")
+    steps = int(d["steps"])
+    k = 2.0 * np.log(np.sqrt(2.0) + 1.0)
+    brain, readout, conn, inp = build(d, refractory=False, alpha=4.0 / k)
+    x = torch.tensor(d["x"][:steps], device=DEV)
+    target = torch.tensor(d["target"][:steps], device=DEV)
+
+    def loss_fn():
+        init_net_state(brain, batch_size=int(d["batch"]), dtype=torch.float32, device=DEV)
+        with environ.context(dt=1.0):
+            z, _ = brain(x)
+        return ((readout(z) - target) ** 2).mean()
+
+    loss = loss_fn()
+    loss.backward()
+    for param in (conn.magnitude, inp.weight):
+        g = param.grad.detach().flatten()
+        top = torch.topk(g.abs(), 6).indices
+        flat = param.data.view(-1)
+        for i in top.tolist():
+            old = float(flat[i])
+            eps = 1e-2 * max(abs(old), 1e-2)
+            with torch.no_grad():
+                flat[i] = old + eps
+                lp = float(loss_fn())
+                flat[i] = old - eps
+                lm = float(loss_fn())
+                flat[i] = old
+            fd = (lp - lm) / (2 * eps)
+            assert abs(fd - float(g[i])) <= 2e-2 * abs(float(g[i])) + 1e-6, (i, fd, float(g[i]))

@@ -49,3 +49,26 @@ def test_oracle_linear_close_to_reference_mkl():
     T, B, c = x.shape
     ours = O.linear(x.reshape(T * B, c), d["W_in"].T).reshape(T, B, -1)
     np.testing.assert_allclose(ours, d["x_proj_ref"], rtol=1e-5, atol=1e-6)
+
+
+def test_oracle_reproduces_training_forward_raster():
+    """The training fixture's forward (two truncated-BPTT windows, state
+    carried between them) equals the oracle's run over the whole input."""
+    import torch
+
+    d = cases.load("train_spiking")
+    n, B = int(d["n"]), int(d["batch"])
+    ptr = np.zeros(n + 1, np.int64)
+    np.add.at(ptr, d["post"] + 1, 1)
+    lin = -1.0 / torch.as_tensor(float(d["psc_tau"]))
+    coef = float(torch.expm1(lin) / lin)
+    spec = O.NetSpec(n=n, kind=0, hard_reset=True, use_ref=True, dt=1.0,
+                     params={"v_threshold": 1.0, "v_reset": 0.0, "c_m": 1.0, "tau": float(d["tau"]),
+                             "tau_ref": float(d["tau_ref"]), "psc_coef": coef, "psc_tau": float(d["psc_tau"])},
+                     ptr=np.cumsum(ptr), pre=d["src"].astype(np.int32), delay=np.zeros(len(d["src"]), np.int32),
+                     w=d["w"])
+    x = d["x"]
+    T = x.shape[0]
+    xp = O.linear(x.reshape(T * B, -1), d["W_in"].T.copy()).reshape(T, B, n)
+    z = O.run(spec, O.init_state(spec, B), xp)["spikes"]
+    np.testing.assert_array_equal(z, np.unpackbits(d["z"], axis=-1, bitorder="little")[..., :n])
