@@ -54,6 +54,9 @@ CONFIGS = {
     # s_state: v, psc, refractory r/w (24) + drive read (4) + delay-ring slot read and clear (8)
     "connectome": dict(model="lif_hetero_delay", n=140000, indeg=350, indeg_sigma=1.0, n_bins=20, exc=0.7,
                        batch=8, t_max=2000, dur=(2000, 2000), c_m=64.0, drive=(0.25, 8.0), s_state=36),
+    # truncated-BPTT training: windows of `window` steps, checkpointed chunks of `chunk`
+    "training": dict(model="lif_train", n=8192, p=0.05, batch=128, t_max=500, window=100, chunk=20, unroll=10,
+                     c_in=256, in_rate=0.02, in_std=0.1, w_exp=-9, inh_gain=6.0, n_out=10, alpha=5.0, lr=1e-3),
 }
 
 
@@ -64,7 +67,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="batched", choices=sorted(CONFIGS))
-    ap.add_argument("--extra", default="connectome",
+    ap.add_argument("--extra", default="connectome,training",
                     help="comma-separated workloads measured after the headline one ('' for none)")
     ap.add_argument("--direction", default="scatter", choices=["scatter", "gather", "auto"])
     ap.add_argument("--no-cudagraph", action="store_true", help="launch every chunk eagerly")
@@ -126,6 +129,94 @@ def make_network(cfg, seed=0):
     count = rng.geometric(0.25, size=post.size)
     w = (count * np.where(pre < int(cfg["exc"] * n), 1.0, -1.0) * 2.0 ** -6).astype(np.float32)
     return dict(post=post, src=pre * R + (delay - 1), pre=pre, delay_bin=delay - 1, w=w, n_bins=R, w_in=None)
+
+
+def make_training_network(cfg, seed=0):
+    """Fixed-probability recurrent net (binomial in-degree), dyadic weights:
+    geometric synapse counts x 2^w_exp, inhibitory (last 20 % of presynaptic
+    ids) x -inh_gain; dense input weights N(0, in_std); readout targets are 10
+    sinusoids per sample (frequency U[1, 20] Hz, phase U[0, 2 pi))."""
+    rng = np.random.default_rng(seed)
+    n = cfg["n"]
+    k = rng.binomial(n, cfg["p"], size=n)
+    post = np.repeat(np.arange(n, dtype=np.int64), k)
+    pre = rng.integers(0, n, size=post.size, dtype=np.int64)
+    post, pre = _dedupe_sorted(post, pre, n)
+    count = rng.geometric(0.25, size=post.size)
+    w = (count * np.where(pre < int(0.8 * n), 1.0, -cfg["inh_gain"]) * 2.0 ** cfg["w_exp"]).astype(np.float32)
+    w_in = rng.normal(0.0, cfg["in_std"], size=(cfg["c_in"], n)).astype(np.float32)
+    T, B, m = cfg["t_max"], cfg["batch"], cfg["n_out"]
+    freq = rng.uniform(1.0, 20.0, size=(1, B, m))
+    phase = rng.uniform(0.0, 2 * np.pi, size=(1, B, m))
+    target = np.sin(2 * np.pi * freq * np.arange(T)[:, None, None] * 1e-3 + phase).astype(np.float32)
+    return dict(post=post, src=pre, pre=pre, w=w, n_bins=1, w_in=w_in, target=target)
+
+
+def measure_training(cfg, args, dev):
+    """Truncated BPTT on the training workload: per window, forward through
+    the per-module path (hand-written forward and backward kernels, chunks
+    checkpointed), readout + MSE, backward, Adam step, detach_net.  Returns the
+    sub-object of the JSON line (forward synaptic events per second of
+    training time, windows per second)."""
+    from btorch_b200.models import LIF, DenseConn, ExponentialPSC, RecurrentNN, Sigmoid, SparseConn, environ
+    from btorch_b200.models.functional import detach_net, init_net_state
+
+    net = make_training_network(cfg, args.seed)
+    n, B, Wn = cfg["n"], cfg["batch"], cfg["window"]
+    conn = SparseConn.from_canonical(net["post"], net["src"], net["w"], (n, n), enforce_dale=False,
+                                     sparse_config={"direction": args.direction})
+    neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=2.0, hard_reset=True,
+                 surrogate_function=Sigmoid(alpha=cfg["alpha"]))
+    brain = RecurrentNN(neuron, ExponentialPSC(n, tau_syn=5.0, linear=conn),
+                        neuron_inp_module=DenseConn(cfg["c_in"], n, weight=torch.from_numpy(net["w_in"])),
+                        update_state_names=(), grad_checkpoint=True, chunk_size=cfg["chunk"],
+                        unroll=cfg["unroll"]).to(dev)
+    readout = torch.nn.Linear(n, cfg["n_out"]).to(dev)
+    opt = torch.optim.Adam(list(brain.parameters()) + list(readout.parameters()), lr=cfg["lr"])
+    g = torch.Generator(device=dev).manual_seed(20_000 + args.seed)
+    x = torch.poisson(torch.full((cfg["t_max"], B, cfg["c_in"]), cfg["in_rate"], device=dev), generator=g)
+    target = torch.from_numpy(net["target"]).to(dev)
+    outdeg = torch.bincount(torch.from_numpy(net["pre"]), minlength=n).to(dev, torch.float64)
+    n_win = cfg["t_max"] // Wn
+    losses = []
+
+    def window(k, events=None):
+        sl = slice((k % n_win) * Wn, (k % n_win + 1) * Wn)
+        if k % n_win == 0:
+            init_net_state(brain, batch_size=B, dtype=torch.float32, device=dev)
+        with environ.context(dt=1.0):
+            z, _ = brain(x[sl])
+            loss = ((readout(z) - target[sl]) ** 2).mean()
+            opt.zero_grad(set_to_none=True)
+            loss.backward()
+            opt.step()
+        detach_net(brain)
+        if events is not None:
+            events.append((z.detach().sum(dim=(0, 1)).double() * outdeg).sum())
+            losses.append(loss.detach())
+
+    for k in range(max(3, args.warmup)):
+        window(k)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    events = []
+    steps = max(args.steps, 1) * n_win
+    e0.record(stream)
+    for k in range(steps):
+        window(k, events)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ev = float(torch.stack(events).sum())
+    return {"value": ev / (ms * 1e-3), "unit": "forward synaptic events/s of training time",
+            "ms_per_window": ms / steps, "windows": steps, "window_steps": Wn,
+            "neuron_steps_per_s": n * B * Wn * steps / (ms * 1e-3),
+            "loss_first_last": [float(losses[0]), float(losses[-1])], "direction": conn.direction(B),
+            "config": {"workload": f"training: LIF+ExpPSC N={n} p={cfg['p']} ({len(net['w'])} trainable weights) "
+                                   f"batch {B} T {cfg['t_max']} TBPTT windows {Wn} checkpoint chunks "
+                                   f"{cfg['chunk']} sigmoid alpha {cfg['alpha']} readout {cfg['n_out']} "
+                                   f"sinusoids, MSE, Adam"}}
 
 
 def build_model(cfg, net, device, direction, batch=None):
@@ -543,6 +634,12 @@ def main():
     torch.cuda.empty_cache()
     for extra in [e for e in args.extra.split(",") if e and e != args.config]:
         ecfg = CONFIGS[extra]
+        if ecfg["model"] == "lif_train":
+            sub = measure_training(ecfg, args, dev)
+            if rank == 0:
+                line[extra] = sub
+            torch.cuda.empty_cache()
+            continue
         sub, m, xe, le, ne, _ = measure(extra, ecfg, args, dev, world, rank, local)
         if rank == 0 and world == 1:
             sub["plain_step"] = plain_step(ecfg, ne, xe, le, args, dev)
