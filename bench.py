@@ -54,6 +54,11 @@ CONFIGS = {
     # s_state: v, psc, refractory r/w (24) + drive read (4) + delay-ring slot read and clear (8)
     "connectome": dict(model="lif_hetero_delay", n=140000, indeg=350, indeg_sigma=1.0, n_bins=20, exc=0.7,
                        batch=8, t_max=2000, dur=(2000, 2000), c_m=64.0, drive=(0.25, 8.0), s_state=36),
+    # serving: Poisson request stream over a pool of connectome-shaped networks
+    "serving": dict(model="serving", sizes=(16384, 32768, 65536, 140000), indeg=350, indeg_sigma=1.0, n_bins=20,
+                    exc=0.7, c_m=64.0, c_in=4000, in_std=0.05, rate_hz=200.0, n_requests=200,
+                    channels=(500, 4000), stim_hz=(5.0, 50.0), steps=(100, 5000), slots=16, chunk=128,
+                    budget_gb=24.0),
     # truncated-BPTT training: windows of `window` steps, checkpointed chunks of `chunk`
     "training": dict(model="lif_train", n=8192, p=0.05, batch=128, t_max=500, window=100, chunk=20, unroll=10,
                      c_in=256, in_rate=0.02, in_std=0.1, w_exp=-9, inh_gain=6.0, n_out=10, alpha=5.0, lr=1e-3),
@@ -67,7 +72,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="batched", choices=sorted(CONFIGS))
-    ap.add_argument("--extra", default="connectome,training",
+    ap.add_argument("--extra", default="connectome,training,serving",
                     help="comma-separated workloads measured after the headline one ('' for none)")
     ap.add_argument("--direction", default="scatter", choices=["scatter", "gather", "auto"])
     ap.add_argument("--no-cudagraph", action="store_true", help="launch every chunk eagerly")
@@ -217,6 +222,66 @@ def measure_training(cfg, args, dev):
                                    f"batch {B} T {cfg['t_max']} TBPTT windows {Wn} checkpoint chunks "
                                    f"{cfg['chunk']} sigmoid alpha {cfg['alpha']} readout {cfg['n_out']} "
                                    f"sinusoids, MSE, Adam"}}
+
+
+def measure_serving(cfg, args, dev):
+    """Continuous batching (btorch_b200.serving) of a seeded Poisson request
+    stream over four connectome-shaped networks (the connectome generator at
+    each size, plus a dense input layer of c_in channels with half-normal
+    weights).  Each request drives a random number of channels at its own
+    rate for its own number of steps; stimuli are synthesised on the device
+    before the run (they stand in for client uploads).  Returns p50/p99
+    latency (arrival to completion) and aggregate synaptic events/s."""
+    from btorch_b200.models import DenseConn
+    from btorch_b200.serving import NetworkPool, SimRequest, SimulationServer
+
+    pools = {}
+    rng = np.random.default_rng(30_000 + args.seed)
+    for i, n in enumerate(cfg["sizes"]):
+        ncfg = dict(CONFIGS["connectome"], n=n, batch=cfg["slots"])
+        net = make_network(ncfg, args.seed + i)
+        rnn = build_model(ncfg, net, dev, args.direction)
+        w_in = np.abs(rng.normal(0.0, cfg["in_std"], size=(cfg["c_in"], n))).astype(np.float32)
+        w_in = (np.round(w_in * 256.0) / 256.0).astype(np.float32)  # dyadic: exact sums
+        rnn.neuron_inp_module = DenseConn(cfg["c_in"], n, weight=torch.from_numpy(w_in)).to(dev)
+        pools[f"n{n}"] = NetworkPool(f"n{n}", rnn, slots=cfg["slots"], chunk=cfg["chunk"], device=dev)
+    names = list(pools)
+    g = torch.Generator(device=dev).manual_seed(40_000 + args.seed)
+    t = 0.0
+    reqs = []
+    for i in range(cfg["n_requests"]):
+        t += rng.exponential(1.0 / cfg["rate_hz"])
+        T = int(rng.integers(cfg["steps"][0], cfg["steps"][1] + 1))
+        c = int(rng.integers(cfg["channels"][0], cfg["channels"][1] + 1))
+        hz = float(rng.uniform(*cfg["stim_hz"]))
+        stim = torch.zeros((T, cfg["c_in"]), device=dev)
+        stim[:, :c] = torch.poisson(torch.full((T, c), hz * 1e-3, device=dev), generator=g)
+        reqs.append(SimRequest(network=names[int(rng.integers(len(names)))], stimulus=stim, arrival=t, rid=i))
+    # warm-up: one tick per pool (graph capture) outside the measured run
+    warm = [SimRequest(network=nm, stimulus=torch.zeros((p.chunk, cfg["c_in"]), device=dev), rid=-1 - j)
+            for j, (nm, p) in enumerate(pools.items())]
+    SimulationServer(pools, hbm_budget_bytes=int(cfg["budget_gb"] * 2**30)).run(warm)
+    for p in pools.values():
+        p.drain_events()
+        p.events = 0
+        p.ticks = 0
+    server = SimulationServer(pools, hbm_budget_bytes=int(cfg["budget_gb"] * 2**30))
+    rep = server.run(reqs)
+    out = rep.summary()
+    lat = np.array([r.latency for r in rep.requests]) * 1e3
+    wait = np.array([r.t_admit - r.arrival for r in rep.requests]) * 1e3
+    steps = sum(r.steps for r in rep.requests)
+    out.update({"unit": "ms (latency), events/s", "mean_latency_ms": float(lat.mean()),
+                "p50_wait_ms": float(np.percentile(wait, 50)), "p99_wait_ms": float(np.percentile(wait, 99)),
+                "sample_steps_per_s": steps / rep.wall_s, "offered_rate_req_per_s": cfg["rate_hz"],
+                "direction": args.direction,
+                "config": {"workload": f"serving: {cfg['n_requests']} requests, Poisson arrivals "
+                                       f"{cfg['rate_hz']} req/s over networks N={list(cfg['sizes'])} "
+                                       f"(connectome-shaped, delays 1..{cfg['n_bins']}), {cfg['slots']} slots "
+                                       f"each, ticks of {[p.chunk for p in pools.values()]} steps, stimulus "
+                                       f"{cfg['channels']} channels at {cfg['stim_hz']} Hz for {cfg['steps']} "
+                                       f"steps, HBM budget {cfg['budget_gb']} GiB"}})
+    return out
 
 
 def build_model(cfg, net, device, direction, batch=None):
@@ -634,8 +699,8 @@ def main():
     torch.cuda.empty_cache()
     for extra in [e for e in args.extra.split(",") if e and e != args.config]:
         ecfg = CONFIGS[extra]
-        if ecfg["model"] == "lif_train":
-            sub = measure_training(ecfg, args, dev)
+        if ecfg["model"] in ("lif_train", "serving"):
+            sub = (measure_training if ecfg["model"] == "lif_train" else measure_serving)(ecfg, args, dev)
             if rank == 0:
                 line[extra] = sub
             torch.cuda.empty_cache()

@@ -287,6 +287,38 @@ class MemoryModule(StepModule, torch.nn.Module):
                                      f"to {tuple(v.shape)}; call reset()/init_state() to (re)allocate.")
                 buf.copy_(v)
 
+    @torch.no_grad()
+    def reset_rows(self, rows) -> None:
+        """Reset rows `rows` (ints) of the batch dimension of every memory to the
+        registered value, in place; other rows are untouched.  Used to recycle
+        one sample slot of a batched model for a new request.  Scalar reset
+        values are written with fill_ (no host-to-device copy, so the call does
+        not wait for work queued on the stream); array values are moved to the
+        device once and cached."""
+        cache = self.__dict__.setdefault("_bt_row_reset", {})
+        for key, rv in self._memories_rv.items():
+            buf = self._buffers.get(key)
+            if buf is None:
+                continue
+            bd = self._batch_dims(key)
+            if bd is None:
+                continue
+            if len(bd) != 1:
+                raise ValueError(f"reset_rows needs one batch dimension, memory '{key}' has {bd}")
+            scalar = rv.value is not None and not callable(rv.value) and np.asarray(rv.value).size == 1
+            val = None
+            if not scalar:
+                val = cache.get(key)
+                if val is None or val.device != buf.device or val.dtype != buf.dtype:
+                    val = _memory_var(rv, None, dtype=buf.dtype, device=buf.device)
+                    cache[key] = val
+            for r in rows:
+                row = buf.select(0, int(r))
+                if scalar:
+                    row.fill_(float(np.asarray(rv.value).reshape(())))
+                else:
+                    row.copy_(val)
+
     def memories(self):
         for name in self._memories_rv:
             yield self._buffers[name]

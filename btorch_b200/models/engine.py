@@ -140,6 +140,14 @@ def graph_hist_len(n_bins: int) -> int:
     return 2 * (n_bins + 1)
 
 
+def graph_chunk(n_bins: int, chunk: int | None = None) -> int:
+    """Steps per captured chunk: `chunk` (default DEFAULT_GRAPH_CHUNK) rounded
+    to a multiple of graph_hist_len(n_bins).  Calls whose length is a multiple
+    of it replay graphs only (no eager remainder)."""
+    H = graph_hist_len(n_bins)
+    return H * max(1, round(int(chunk or DEFAULT_GRAPH_CHUNK) / H))
+
+
 class _GraphEntry:
     """One captured chunk graph and the static buffers it is hard-wired to.
 
@@ -224,7 +232,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     use_graph = bool(getattr(rnn, "cudagraph", False))
     if use_graph:
         H = graph_hist_len(R)
-        K = H * max(1, round(int(chunk or DEFAULT_GRAPH_CHUNK) / H))
+        K = graph_chunk(R, chunk)
         gkey = (str(dev), B, n, c_in, choice, R, H, K, spikes_out, tuple(trace_kinds), bool(stats),
                 sample_len is not None, inp is not None)
         entry = graph_entries(rnn).setdefault(gkey, _GraphEntry())

@@ -121,3 +121,14 @@ def detach_net(net: nn.Module):
 
 __all__ = ["init_net_state", "reset_net", "reset_net_state", "prepare_sparse_modules", "named_hidden_states",
            "filter_hidden_states", "set_hidden_states", "detach_net"]
+
+
+@torch.no_grad()
+def reset_rows(net: nn.Module, rows) -> None:
+    """Reset batch rows `rows` of every memory in `net` to its registered
+    value (MemoryModule.reset_rows): recycles sample slots of a batched model
+    without touching the other samples' state."""
+    rows = [int(r) for r in (rows.tolist() if torch.is_tensor(rows) else rows)]
+    for m in net.modules():
+        if isinstance(m, base.MemoryModule):
+            m.reset_rows(rows)
