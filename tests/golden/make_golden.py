@@ -303,6 +303,53 @@ def case_train(rng, *, n, p, batch, steps, windows, c_in, n_out, spiking, chunk,
     return out
 
 
+def case_fp64(rng, *, n, p, steps, c_in, rate, scale, in_gain):
+    """The C1 configuration's model (LIF tau 20, refractory 2, hard reset,
+    ExponentialPSC 5, lognormal E/I SparseConn, DenseConn input from Poisson
+    channels, batch 1) at a reduced size with C1's in-degree (82) and active
+    input channels per step (10), run by the reference twice on the same
+    inputs: in fp32 and in fp64 (dtype=torch.float64 on every module and the
+    state).  The fp64 membrane trace is the yardstick for the fp32 error of
+    the first `steps` steps: per-step max |v32 - v64| over all neurons and the
+    first raster divergence are stored, with the traces of 64 neurons."""
+    import scipy.sparse as sp
+    import torch
+    from btorch.models import environ
+    from btorch.models.functional import init_net_state
+    from btorch.models.linear import DenseConn, SparseConn
+    from btorch.models.neurons import LIF
+    from btorch.models.rnn import RecurrentNN
+    from btorch.models.synapse import ExponentialPSC
+
+    Wd = make_conn(rng, n, n, p, dyadic=False, scale=scale)
+    W_in = (rng.normal(0.0, 0.05, size=(c_in, n)) * in_gain).astype(np.float32)
+    x = rng.poisson(rate, size=(steps, 1, c_in)).astype(np.float32)
+    out = {}
+    for dt_name, dtype in (("32", torch.float32), ("64", torch.float64)):
+        conn = SparseConn(sp.coo_array(Wd.astype(np.float64) if dtype == torch.float64 else Wd),
+                          sparse_backend="native", dtype=dtype)
+        neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=2.0, hard_reset=True, dtype=dtype)
+        syn = ExponentialPSC(n, tau_syn=5.0, linear=conn)
+        inp = DenseConn(c_in, n, weight=torch.tensor(W_in, dtype=dtype), dtype=dtype)
+        brain = RecurrentNN(neuron, syn, neuron_inp_module=inp, update_state_names=("neuron.v",))
+        init_net_state(brain, batch_size=1, dtype=dtype)
+        with torch.no_grad(), environ.context(dt=1.0):
+            z, st = brain(torch.tensor(x, dtype=dtype))
+        out["v" + dt_name] = st["neuron.v"].numpy()
+        out["z" + dt_name] = np.packbits(z.numpy().astype(np.uint8), axis=-1, bitorder="little")
+    post, src, w = canonical(Wd)
+    z32 = np.unpackbits(out["z32"], axis=-1, bitorder="little")[..., :n]
+    z64 = np.unpackbits(out["z64"], axis=-1, bitorder="little")[..., :n]
+    bad = np.nonzero((z32 != z64).reshape(steps, -1).any(1))[0]
+    k = int(bad[0]) if bad.size else steps
+    err = np.abs(out["v32"].astype(np.float64) - out["v64"]).reshape(steps, -1)
+    keep = slice(0, 64)  # traces of the first 64 neurons; error statistics over all
+    out.update(n=n, batch=1, x=x, W_in=W_in, post=post.astype(np.int32), src=src.astype(np.int32), w=w,
+               steps=steps, first_divergence=k, err_max=err.max(axis=1),
+               v32=out["v32"][:, :, keep], v64=out["v64"][:, :, keep])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -328,6 +375,8 @@ def main():
                                               spiking=True, chunk=10, unroll=5),
         "train_smooth": lambda r: case_train(r, n=96, p=0.1, batch=3, steps=30, windows=2, c_in=16, n_out=4,
                                              spiking=False, chunk=10, unroll=5),
+        "fp64_c1": lambda r: case_fp64(r, n=1024, p=0.08, steps=200, c_in=250, rate=0.04, scale=0.01,
+                                       in_gain=GAIN["c1"]),
     }
     only = set(args.only.split(",")) if args.only else None
     for i, (name, fn) in enumerate(cases.items()):
