@@ -54,6 +54,11 @@ CONFIGS = {
     # s_state: v, psc, refractory r/w (24) + drive read (4) + delay-ring slot read and clear (8)
     "connectome": dict(model="lif_hetero_delay", n=140000, indeg=350, indeg_sigma=1.0, n_bins=20, exc=0.7,
                        batch=8, t_max=2000, dur=(2000, 2000), c_m=64.0, drive=(0.25, 8.0), s_state=36),
+    # shorter runs of the same workloads, for profiler captures (a few GB on the device)
+    "batched_short": dict(model="alif_dense_input", n=65536, indeg=500, batch=64, c_in=2000, t_max=512,
+                          rate=(2.0, 40.0), dur=(512, 512), w_scale=0.0030, in_gain=1.0, s_state=36),
+    "connectome_short": dict(model="lif_hetero_delay", n=140000, indeg=350, indeg_sigma=1.0, n_bins=20, exc=0.7,
+                             batch=8, t_max=256, dur=(256, 256), c_m=64.0, drive=(0.25, 8.0), s_state=36),
     # serving: Poisson request stream over a pool of connectome-shaped networks
     "serving": dict(model="serving", sizes=(16384, 32768, 65536, 140000), indeg=350, indeg_sigma=1.0, n_bins=20,
                     exc=0.7, c_m=64.0, c_in=4000, in_std=0.05, rate_hz=200.0, n_requests=200,

@@ -26,7 +26,7 @@ _i64 = C.c_int64
 _i32 = C.c_int32
 
 
-ABI_VERSION = 2  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
+ABI_VERSION = 3  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
 
 
 class BtParam(C.Structure):
@@ -56,7 +56,7 @@ class BtEngineDesc(C.Structure):
         ("gk_trace", _vp),
         ("sl_ptr", _vp), ("sl_src", _vp), ("sl_w", _vp), ("masks", _vp), ("outdeg", _vp),
         ("pull_words_per_warp", _i32), ("neuron_spt", _i32),
-        ("work", _vp), ("stats", _vp),
+        ("work", _vp), ("stats", _vp), ("dense_rows", _i64),
     ]
 
 

@@ -69,28 +69,36 @@ inline StepIdx step_idx(int64_t t, int R, int H) {
 // ---------------------------------------------------------------- scatter --
 
 // Scatter-mode scratch (d.work, int32 words), Q = R + 1 spike-set slots:
-//   [0, Q*kSub)                    active-list counts, [slot][sub-list]
+//   [0, 2*Q*kSub)                  active-list counts and spike totals,
+//                                  [slot][count | spikes][sub-list]
 //   next Q*n                       "listed" flags, [slot][neuron]
 //   next Q*kSub*cap                list entries, [slot][sub-list][cap]
 //   next Q n S                     sample masks, [slot][neuron][S words], S = mask_stride(batch)
+//   next kSub                      control words (ctrl[0]: blocks done with a dense step)
 // Sub-list s only lists neurons [s*cap, (s+1)*cap) and each neuron is listed at
 // most once per step (its flag), so a sub-list never holds more than cap
 // entries.  cap is a multiple of 32, so the 32 neurons of a warp share one
 // sub-list.
 constexpr int kSub = 64;
+// Dense delivery needs at least this many spiking samples per listed neuron on
+// average: below it the per-event reductions of the list path are cheaper
+// than the dense pull's random mask reads (measured crossover about 2.5).
+constexpr int kDenseSpikesPerRow = 3;
 
 __host__ __device__ __forceinline__ int64_t sub_cap(int64_t n) { return (((n + kSub - 1) / kSub) + 31) / 32 * 32; }
 
 __host__ __device__ __forceinline__ int64_t scatter_work_words(int64_t n, int64_t batch, int n_bins) {
   const int64_t Q = int64_t(n_bins) + 1;
-  return Q * (kSub + n + kSub * sub_cap(n) + n * mask_stride(batch));
+  return Q * (2 * kSub + n + kSub * sub_cap(n) + n * mask_stride(batch)) + kSub;
 }
 
 struct ScatterScratch {
   int32_t* count;
+  int32_t* spk;   // spikes (sample-neuron pairs) listed per sub-list
   int32_t* flag;
   int32_t* list;
   uint32_t* mask;
+  int32_t* ctrl;
   int64_t cap;
   int ms;
 };
@@ -101,10 +109,12 @@ __device__ __forceinline__ ScatterScratch scatter_scratch(const bt_engine_desc& 
   const int64_t Q = int64_t(d.n_bins) + 1;
   w.ms = mask_stride(d.batch);
   w.cap = sub_cap(n);
-  w.count = d.work + q * kSub;
-  w.flag = d.work + Q * kSub + q * n;
-  w.list = d.work + Q * kSub + Q * n + q * kSub * w.cap;
-  w.mask = reinterpret_cast<uint32_t*>(d.work + Q * kSub + Q * n + Q * kSub * w.cap) + int64_t(q) * n * w.ms;
+  w.count = d.work + q * 2 * kSub;
+  w.spk = w.count + kSub;
+  w.flag = d.work + Q * 2 * kSub + q * n;
+  w.list = d.work + Q * 2 * kSub + Q * n + q * kSub * w.cap;
+  w.mask = reinterpret_cast<uint32_t*>(d.work + Q * 2 * kSub + Q * n + Q * kSub * w.cap) + int64_t(q) * n * w.ms;
+  w.ctrl = d.work + Q * (2 * kSub + n + kSub * w.cap + n * w.ms);
   return w;
 }
 
@@ -208,8 +218,10 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
     first = atomicOr(ws.flag + i, 1) == 0;
   }
   const uint32_t fb = __ballot_sync(0xffffffffu, first);
-  if (fb == 0) return;
   const int sub = int((i - lane) / ws.cap);  // same for the whole warp (cap % 32 == 0)
+  const int nspk = __reduce_add_sync(0xffffffffu, unsigned(__popc(spiked)));
+  if (lane == 0 && nspk) atomicAdd(ws.spk + sub, nspk);
+  if (fb == 0) return;
   int32_t base = 0;
   if (lane == 0) base = atomicAdd(ws.count + sub, __popc(fb));
   base = __shfl_sync(0xffffffffu, base, 0);
@@ -218,19 +230,22 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
 
 // Offsets of the kSub sub-lists of one spike set in shared memory (warp 0
 // scans the counts; two per lane).
-__device__ __forceinline__ void sub_offsets(const int32_t* __restrict__ count, int32_t* s_off) {
+__device__ __forceinline__ void sub_offsets(const ScatterScratch& ws, int32_t* s_off, int32_t* s_spk) {
   if (threadIdx.x < 32) {
     const int l = threadIdx.x;
-    const int32_t c0 = count[2 * l], c1 = count[2 * l + 1];
+    const int32_t c0 = ws.count[2 * l], c1 = ws.count[2 * l + 1];
     int32_t v = c0 + c1;
+    int32_t sp = ws.spk[2 * l] + ws.spk[2 * l + 1];
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int32_t y = __shfl_up_sync(0xffffffffu, v, o);
       if (l >= o) v += y;
+      sp += __shfl_xor_sync(0xffffffffu, sp, o);
     }
     s_off[2 * l] = v - c0 - c1;
     s_off[2 * l + 1] = v - c1;
     if (l == 31) s_off[kSub] = v;
+    if (l == 0) *s_spk = sp;
   }
   __syncthreads();
 }
@@ -274,6 +289,95 @@ __device__ __forceinline__ void block_stats(const bt_engine_desc& d, int64_t k, 
   }
 }
 
+// Dense delivery of one spike set (single delay bin): a block owns a slice of
+// 32 posts (lane = post); its 8 warps split the slice's rows of the sliced
+// in-edge view and accumulate, one 32-sample mask word per pass, into
+// per-warp shared-memory columns (no conflicts, no atomics); the block then
+// sums the 8 partial columns and stores the totals into acc with plain
+// stores (acc is zero on entry, each (sample, post) has one writer).  Used
+// for steps where most neurons spike in some sample, where per-event
+// reductions would cost more than reading every in-edge once.  The spike
+// set's masks and flags are then cleared by the last block to finish
+// (block-completion counter in ctrl[0]; no block waits for another).
+template <int MS>
+__device__ void scatter_dense(const bt_engine_desc& d, int64_t k, const ScatterScratch& ws, long long& ev,
+                              long long& ed) {
+  constexpr int W = kEngThreads / 32;
+  __shared__ float s_acc[W][32][32];
+  const int lane = int(lane_id()), wid = int(threadIdx.x >> 5);
+  const int64_t n = d.n, B = d.batch;
+  const int n32 = int(n);
+  const int64_t n_slices = (n + 31) >> 5;
+  const int64_t nblocks = int64_t(gridDim.x) * gridDim.y;
+  const int64_t bid = int64_t(blockIdx.y) * gridDim.x + blockIdx.x;
+  float(*acc)[32] = s_acc[wid];
+  const uint64_t pol_stream = l2_evict_first();
+  const uint32_t sentinel = uint32_t(n);
+  for (int64_t sl = bid; sl < n_slices; sl += nblocks) {  // uniform per block
+    const int64_t r0 = d.sl_ptr[sl], r1 = d.sl_ptr[sl + 1];
+    const int64_t per = (r1 - r0 + W - 1) / W;
+    const int64_t ra = r0 + wid * per, rb = ra + per < r1 ? ra + per : r1;
+    for (int w = 0; w < ws.ms; ++w) {
+#pragma unroll 8
+      for (int l = 0; l < 32; ++l) acc[l][lane] = 0.0f;
+      __syncwarp();
+      constexpr int U = 8;
+      for (int64_t r = ra; r < rb; r += U) {
+        uint32_t src[U];
+        float wg[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const bool in = r + u < rb;
+          src[u] = in ? ld_nc_u32(d.sl_src + (r + u) * 32 + lane, pol_stream) & kIdMask : sentinel;
+          wg[u] = in ? ld_nc_f32(d.sl_w + (r + u) * 32 + lane, pol_stream) : 0.0f;
+        }
+        uint32_t m[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) m[u] = src[u] < sentinel ? ws.mask[int64_t(src[u]) * ws.ms + w] : 0u;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (w == 0 && src[u] < sentinel) {
+            bool any = m[u] != 0;
+            for (int x = 1; x < ws.ms && !any; ++x) any = ws.mask[int64_t(src[u]) * ws.ms + x] != 0;
+            ed += any ? 1 : 0;
+          }
+          ev += __popc(m[u]);
+          uint32_t mm = m[u];
+          while (mm) {
+            const int l = __ffs(mm) - 1;
+            mm &= mm - 1;
+            acc[l][lane] = add(acc[l][lane], wg[u]);
+          }
+        }
+      }
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < 32 * 32; idx += blockDim.x) {
+        const int l = idx >> 5, ln = idx & 31;
+        float sum = 0.0f;
+#pragma unroll
+        for (int v = 0; v < W; ++v) sum = add(sum, s_acc[v][l][ln]);
+        const int64_t b = int64_t(w) * 32 + l, p = sl * 32 + ln;
+        if (b < B && p < n && sum != 0.0f) d.ring[b * n32 + p] = sum;
+      }
+      __syncthreads();
+    }
+  }
+  // the last block to finish clears the spike set (no other block reads it)
+  __shared__ int s_last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int done = atomicAdd(ws.ctrl, 1);
+    s_last = done == int(nblocks) - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    for (int64_t i = threadIdx.x; i < n * ws.ms; i += blockDim.x) ws.mask[i] = 0u;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) ws.flag[i] = 0;
+    if (threadIdx.x == 0) ws.ctrl[0] = 0;
+  }
+}
+
 // Grid (x, bin_hi - bin_lo + 1): plane y delivers delay bin d = bin_lo + y,
 // i.e. the spike set of step t - d through rows j * R + d.  G lanes share one
 // row (G = 32 for long rows, 8 for the short rows of a wide delay range), each
@@ -289,16 +393,25 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, i
   if (q < 0) q += Q;
   const ScatterScratch ws = scatter_scratch(d, q);
   __shared__ int32_t s_off[kSub + 1];
-  sub_offsets(ws.count, s_off);
+  __shared__ int32_t s_spk;
+  sub_offsets(ws, s_off, &s_spk);
   const int32_t count = s_off[kSub];
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < kSub) {
     // the counts of slot (t + 1) mod Q, i.e. of step t - R, were last read by
     // the previous step's scatter: clear them for the next neuron launch
     const int qc = si.q_t + 1 == Q ? 0 : si.q_t + 1;
-    d.work[qc * kSub + threadIdx.x] = 0;
+    d.work[qc * 2 * kSub + threadIdx.x] = 0;
+    d.work[qc * 2 * kSub + kSub + threadIdx.x] = 0;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && d.stats)
     atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 0), (unsigned long long)count);
+  // dense when most neurons spike and they do so in several samples each
+  if (d.dense_rows > 0 && count >= d.dense_rows && s_spk >= kDenseSpikesPerRow * count) {  // grid-uniform
+    long long ev = 0, ed = 0;
+    scatter_dense<MS>(d, k, ws, ev, ed);
+    if (d.stats) block_stats(d, k, ev, ed);
+    return;
+  }
   const bool last_use = bin == d.bin_hi;  // this set is not read again: clear it
   const unsigned lane = lane_id();
   const int grp = int(lane) / G, lig = int(lane) % G;
@@ -398,14 +511,23 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter_flat(bt_engine_desc
   if (q < 0) q += Q;
   const ScatterScratch ws = scatter_scratch(d, q);
   __shared__ int32_t s_off[kSub + 1];
-  sub_offsets(ws.count, s_off);
+  __shared__ int32_t s_spk;
+  sub_offsets(ws, s_off, &s_spk);
   const int32_t count = s_off[kSub];
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < kSub) {
     const int qc = si.q_t + 1 == Q ? 0 : si.q_t + 1;  // step t - R: last read by the previous step
-    d.work[qc * kSub + threadIdx.x] = 0;
+    d.work[qc * 2 * kSub + threadIdx.x] = 0;
+    d.work[qc * 2 * kSub + kSub + threadIdx.x] = 0;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && d.stats)
     atomicAdd(reinterpret_cast<unsigned long long*>(d.stats + k * 4 + 0), (unsigned long long)count);
+  // dense when most neurons spike and they do so in several samples each
+  if (d.dense_rows > 0 && count >= d.dense_rows && s_spk >= kDenseSpikesPerRow * count) {  // grid-uniform
+    long long ev = 0, ed = 0;
+    scatter_dense<MS>(d, k, ws, ev, ed);
+    if (d.stats) block_stats(d, k, ev, ed);
+    return;
+  }
   const bool last_use = bin == d.bin_hi;
   const int lane = int(lane_id());
   const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
@@ -1013,6 +1135,8 @@ int engine_check(const bt_engine_desc* d) {
                  "scatter_lanes=%d (0, 1, 8 or 32)", d->scatter_lanes);
     BT_CHECK_ARG(mask_stride(d->batch) <= 8, "scatter mode supports up to 256 samples");
     BT_CHECK_ARG(d->batch * d->n < (int64_t(1) << 31), "scatter mode needs batch * n < 2^31");
+    BT_CHECK_ARG(d->dense_rows == 0 || (d->bin_lo == d->bin_hi && d->sl_ptr && d->sl_src && d->sl_w),
+                 "dense delivery needs a single delay bin and the sliced in-edge view");
     BT_CHECK_ARG(d->neuron_spt == 0 || d->neuron_spt == 1 || d->neuron_spt == 2 || d->neuron_spt == 4,
                  "neuron_spt=%d (0, 1, 2 or 4)", d->neuron_spt);
     BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->csr_dst) & 15) == 0 &&

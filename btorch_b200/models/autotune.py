@@ -39,11 +39,13 @@ class EngineChoice:
     scatter_lanes: int = 0     # scatter: lanes per active row, 8 or 32, or 1 = rows of a warp flattened
                                # into one edge range (0 = by mean row length)
     pull_words: int = 0        # pull: 32-sample mask words per warp (0 = one)
+    dense_rows: int = -1       # scatter, one delay bin: spiking neurons from which a step is pulled
+                               # densely (-1 = n / engine.DENSE_FRACTION, 0 = never)
 
     def describe(self) -> dict:
         name = {L.BT_MODE_SCATTER: "scatter", L.BT_MODE_GATHER: "gather", L.BT_MODE_PULL: "pull"}[self.mode]
         return {"mode": name, "neuron_spt": self.neuron_spt, "scatter_lanes": self.scatter_lanes,
-                "pull_words": self.pull_words}
+                "pull_words": self.pull_words, "dense_rows": self.dense_rows}
 
 
 def allowed_modes(conn, batch: int) -> list[int]:

@@ -30,6 +30,7 @@ from .neurons.lif import LIF
 from .synapse import DelayedPSC, ExponentialPSC, HeterSynapsePSC
 
 DEFAULT_CHUNK = 512
+DENSE_FRACTION = 4  # scatter steps with at least n / DENSE_FRACTION spiking neurons are pulled densely
 DEFAULT_GRAPH_CHUNK = 128  # steps per captured chunk (rounded to a multiple of the slot period)
 
 
@@ -281,6 +282,18 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         desc.bin_lo, desc.bin_hi = lay_s.bin_lo, lay_s.bin_hi
         desc.scatter_lanes = choice.scatter_lanes or (1 if lay_s.mean_row < 48 else 32)
         desc.neuron_spt = choice.neuron_spt or 4
+        dense = choice.dense_rows if choice.dense_rows >= 0 else n // DENSE_FRACTION
+        if dense > 0 and lay_s.bin_lo == lay_s.bin_hi:
+            # steps where at least `dense` neurons spike are pulled over the
+            # sliced in-edge view instead of scattered
+            sl = getattr(lay, "slices", None)
+            if sl is None:
+                sl = build_slices(lay, dev)
+                lay.slices = sl
+            sl_w_d = static("sl_w", pack_slice_weights(sl, w))
+            keep.append(sl_w_d)
+            desc.sl_ptr, desc.sl_src, desc.sl_w = sl.sl_ptr.data_ptr(), sl.sl_src.data_ptr(), sl_w_d.data_ptr()
+            desc.dense_rows = dense
         ring = alloc("ring", (B, n), torch.float32)  # W z of the step (bt_engine_prime clears it)
         work = alloc("work", (L.lib().bt_engine_work_words(n, B, R),), torch.int32)
         keep += [ring, work]

@@ -44,7 +44,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 2
+#define BT_ABI_VERSION 3
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -302,6 +302,12 @@ typedef struct bt_engine_desc {
                              sets (active lists and sample masks) of the last
                              n_bins steps; bt_engine_prime initialises it */
   int64_t* stats;         /* [n_steps][4]: active union, events, edges, 0; may be NULL */
+
+  /* scatter with a single delay bin (bin_lo == bin_hi): a step whose spike
+     set lists at least dense_rows neurons is delivered by a dense pull over
+     the sliced in-edge view sl_ptr / sl_src / sl_w instead (lane per post,
+     ascending in-edge order, plain stores), 0 = never */
+  int64_t dense_rows;
 } bt_engine_desc;
 
 /* Scratch words (int32) the scatter mode needs in bt_engine_desc.work. */
