@@ -26,7 +26,7 @@ _i64 = C.c_int64
 _i32 = C.c_int32
 
 
-ABI_VERSION = 3  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
+ABI_VERSION = 4  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
 
 
 class BtParam(C.Structure):
@@ -40,6 +40,7 @@ class BtNeuronDesc(C.Structure):
         ("v_threshold", BtParam), ("v_reset", BtParam), ("c_m", BtParam), ("tau", BtParam),
         ("tau_ref", BtParam), ("g_leak", BtParam), ("E_leak", BtParam), ("E_k", BtParam),
         ("dg_k", BtParam), ("tau_adapt", BtParam), ("coef_gk", BtParam),
+        ("uniform", _i32), ("sv", C.c_float * 11),
     ]
 
 
@@ -57,6 +58,7 @@ class BtEngineDesc(C.Structure):
         ("sl_ptr", _vp), ("sl_src", _vp), ("sl_w", _vp), ("masks", _vp), ("outdeg", _vp),
         ("pull_words_per_warp", _i32), ("neuron_spt", _i32),
         ("work", _vp), ("stats", _vp), ("dense_rows", _i64),
+        ("psc_uniform", _i32), ("psc_coef_s", C.c_float), ("psc_tau_s", C.c_float), ("pad4_", _i32),
     ]
 
 

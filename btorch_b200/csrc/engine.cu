@@ -85,7 +85,13 @@ constexpr int kSub = 64;
 // than the dense pull's random mask reads (measured crossover about 2.5).
 constexpr int kDenseSpikesPerRow = 3;
 
-__host__ __device__ __forceinline__ int64_t sub_cap(int64_t n) { return (((n + kSub - 1) / kSub) + 31) / 32 * 32; }
+// A power of two (>= 32), so the sub-list of neuron i is i >> log2(cap).
+__host__ __device__ __forceinline__ int64_t sub_cap(int64_t n) {
+  const int64_t c = (n + kSub - 1) / kSub;
+  int64_t p = 32;
+  while (p < c) p <<= 1;
+  return p;
+}
 
 __host__ __device__ __forceinline__ int64_t scatter_work_words(int64_t n, int64_t batch, int n_bins) {
   const int64_t Q = int64_t(n_bins) + 1;
@@ -100,6 +106,7 @@ struct ScatterScratch {
   uint32_t* mask;
   int32_t* ctrl;
   int64_t cap;
+  int cap_shift;  // log2(cap)
   int ms;
 };
 
@@ -109,6 +116,7 @@ __device__ __forceinline__ ScatterScratch scatter_scratch(const bt_engine_desc& 
   const int64_t Q = int64_t(d.n_bins) + 1;
   w.ms = mask_stride(d.batch);
   w.cap = sub_cap(n);
+  w.cap_shift = __ffsll(w.cap) - 1;
   w.count = d.work + q * 2 * kSub;
   w.spk = w.count + kSub;
   w.flag = d.work + Q * 2 * kSub + q * n;
@@ -141,10 +149,11 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   const float* __restrict__ x_p = d.x ? d.x + k * B * n + off0 : nullptr;
   float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
   const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
+  const int n32 = int(n);  // batch * n < 2^31 in scatter mode (checked on the host)
 #pragma unroll
   for (int u = 0; u < S; ++u) {
     const bool in = valid && u < nb;
-    const int64_t o = int64_t(u) * n;
+    const int o = u * n32;
     pend[u] = in ? ld_f32(ring_p + o, pol_keep) : 0.0f;
     pv[u] = in ? psc_p[o] : 0.0f;
     xv[u] = (in && x_p) ? ld_nc_f32(x_p + o, pol_stream) : 0.0f;
@@ -154,7 +163,9 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   }
   const int64_t ip = valid ? i : 0;
   const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, ip);
-  const float pc = ld(d.psc_coef, ip), pt = ld(d.psc_tau, ip), rpt = pow2_recip(pt);
+  const float pc = d.psc_uniform ? d.psc_coef_s : ld(d.psc_coef, ip);
+  const float pt = d.psc_uniform ? d.psc_tau_s : ld(d.psc_tau, ip);
+  const float rpt = pow2_recip(pt);
   const unsigned lane = lane_id();
   const bool traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace || d.spikes;
   uint32_t* hist_p = d.hist + (int64_t(si.h_t) * B + b0) * words + (i >> 5);
@@ -163,7 +174,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
 #pragma unroll
   for (int u = 0; u < S; ++u) {
     if (u >= nb) break;  // uniform across the block
-    const int64_t o = int64_t(u) * n;
+    const int o = u * n32;
     float s = 0.0f;
     if (valid) {
       st_f32(ring_p + o, 0.0f, pol_keep);
@@ -200,8 +211,8 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
     }
     const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
     if (lane == 0) {
-      hist_p[int64_t(u) * words] = word;
-      if (raster_p) raster_p[int64_t(u) * words] = word;
+      hist_p[u * int(words)] = word;
+      if (raster_p) raster_p[u * int(words)] = word;
     }
     if (s != 0.0f) spiked |= 1u << u;
   }
@@ -218,7 +229,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
     first = atomicOr(ws.flag + i, 1) == 0;
   }
   const uint32_t fb = __ballot_sync(0xffffffffu, first);
-  const int sub = int((i - lane) / ws.cap);  // same for the whole warp (cap % 32 == 0)
+  const int sub = int((i - lane) >> ws.cap_shift);  // same for the whole warp (cap % 32 == 0)
   const int nspk = __reduce_add_sync(0xffffffffu, unsigned(__popc(spiked)));
   if (lane == 0 && nspk) atomicAdd(ws.spk + sub, nspk);
   if (fb == 0) return;
@@ -1016,7 +1027,7 @@ __global__ void k_prime_history(bt_engine_desc d) {
   const unsigned lane = lane_id();
   const uint32_t fb = __ballot_sync(0xffffffffu, any);
   if (fb == 0) return;
-  const int sub = int((i - lane) / ws.cap);
+  const int sub = int((i - lane) >> ws.cap_shift);
   int32_t base = 0;
   if (lane == 0) base = atomicAdd(ws.count + sub, __popc(fb));
   base = __shfl_sync(0xffffffffu, base, 0);

@@ -58,6 +58,32 @@ struct NeuronParams {
 template <int KIND, bool USE_REF>
 __device__ __forceinline__ NeuronParams load_params(const bt_neuron_desc& d, int64_t i) {
   NeuronParams p;
+  if (d.uniform) {  // scalar parameters passed by value: no parameter loads
+    p.vth = d.sv[0];
+    p.vr = d.sv[1];
+    p.cm = d.sv[2];
+    p.den = sub(p.vth, p.vr);
+    p.dt = d.dt;
+    p.sg_alpha = d.sg_alpha;
+    p.spiking = d.spiking;
+    p.tau = KIND == BT_NEURON_LIF ? d.sv[3] : 0.0f;
+    p.tau_ref = USE_REF ? d.sv[4] : 0.0f;
+    if (KIND == BT_NEURON_ALIF) {
+      p.ngl = -d.sv[5];
+      p.El = d.sv[6];
+      p.Ek = d.sv[7];
+      p.dgk = d.sv[8];
+      p.tau_a = d.sv[9];
+      p.cgk = d.sv[10];
+    } else {
+      p.ngl = p.El = p.Ek = p.dgk = p.tau_a = p.cgk = 0.0f;
+    }
+    p.r_cm = pow2_recip(p.cm);
+    p.r_den = pow2_recip(p.den);
+    p.r_tau = pow2_recip(p.tau);
+    p.r_tau_a = pow2_recip(p.tau_a);
+    return p;
+  }
   p.vth = ld(d.v_threshold, i);
   p.vr = ld(d.v_reset, i);
   p.cm = ld(d.c_m, i);

@@ -5,6 +5,7 @@ on the CPU or falls back to torch math."""
 
 from __future__ import annotations
 
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -192,15 +193,16 @@ def exp_euler_coef(tau: torch.Tensor, dt: float, owner=None, name: str = "") -> 
     With an `owner` module the result is cached on that module, keyed by dt and
     the identity and version of its `tau` tensor, so repeated steps do not copy
     the time constant back to the host."""
-    key = (float(dt), tau.data_ptr(), getattr(tau, "_version", 0), tuple(tau.shape), str(tau.device))
+    key = (float(dt), tau.data_ptr(), _version(tau), tuple(tau.shape), str(tau.device))
     slot = f"_bt_coef_{name}"
     if owner is not None:
         hit = owner.__dict__.get(slot)
         if hit is not None and hit[0] == key:
             return hit[1]
-    t_cpu = tau.detach().to("cpu", torch.float32)
-    lin = -1.0 / t_cpu
-    coef = (torch.expm1(dt * lin) / lin).reshape(-1).contiguous().to(tau.device)
+    with torch.inference_mode(False):  # a normal tensor, so its version is tracked
+        t_cpu = tau.detach().to("cpu", torch.float32)
+        lin = -1.0 / t_cpu
+        coef = (torch.expm1(dt * lin) / lin).reshape(-1).contiguous().to(tau.device)
     if owner is not None:
         owner.__dict__[slot] = (key, coef)
     return coef
@@ -213,16 +215,60 @@ def _flat(t: torch.Tensor) -> torch.Tensor:
     return t.reshape(-1).contiguous()
 
 
+_SCALARS: dict = {}  # id(tensor) -> (weakref to it, (address, version), value)
+
+
+def _version(t: torch.Tensor) -> int:
+    # inference tensors keep no version counter (they cannot be modified
+    # outside inference mode)
+    return -1 if t.is_inference() else t._version
+
+
+def scalar_values(tensors) -> list[float] | None:
+    """Host copies of one-element tensors, or None if any has more elements.
+
+    Cached per tensor object (by identity, never by tensor equality, which
+    would synchronise) and keyed by its storage address and version counter,
+    so a value is copied to the host once (one synchronisation for all
+    misses) and again only after the tensor is modified in place or rebound
+    to new storage."""
+    if any(t.numel() != 1 for t in tensors):
+        return None
+    out, missing = [None] * len(tensors), []
+    for i, t in enumerate(tensors):
+        hit = _SCALARS.get(id(t))
+        if hit is not None and hit[0]() is t and hit[1] == (t.data_ptr(), _version(t)):
+            out[i] = hit[2]
+        else:
+            missing.append(i)
+    if missing:
+        vals = torch.stack([tensors[i].detach().reshape(()).to(torch.float32) for i in missing]).cpu().tolist()
+        if len(_SCALARS) > 4096:  # drop entries of collected tensors
+            for key in [k for k, v in _SCALARS.items() if v[0]() is None]:
+                del _SCALARS[key]
+        for i, v in zip(missing, vals):
+            t = tensors[i]
+            _SCALARS[id(t)] = (weakref.ref(t), (t.data_ptr(), _version(t)), v)
+            out[i] = v
+    return out
+
+
 def neuron_desc(node, dt: float):
-    """bt_neuron_desc for an LIF/ALIF module; returns (desc, keepalive)."""
+    """bt_neuron_desc for an LIF/ALIF module; returns (desc, keepalive).  When
+    every parameter is a scalar, their values are also passed by value
+    (desc.uniform), so the kernels read no parameter memory."""
     from .neurons.alif import ALIF
     from .neurons.lif import LIF
 
     keep = []
+    sources = {}
 
-    def P(t):
-        f = _flat(torch.as_tensor(t))
+    def P(t, slot=None):
+        t = torch.as_tensor(t)
+        f = _flat(t)
         keep.append(f)
+        if slot is not None:
+            sources[slot] = t
         return L.param(f)
 
     d = L.BtNeuronDesc()
@@ -233,21 +279,28 @@ def neuron_desc(node, dt: float):
     d.dt = float(dt)
     d.sg_alpha = float(getattr(sg, "slope", 2.0 * 1.7627471740390859))
     d.sg_damping = float(getattr(sg, "damping_factor", 1.0))
-    d.v_threshold = P(node.v_threshold)
-    d.v_reset = P(node.v_reset)
-    d.c_m = P(node.c_m)
+    d.v_threshold = P(node.v_threshold, 0)
+    d.v_reset = P(node.v_reset, 1)
+    d.c_m = P(node.c_m, 2)
     if node._use_refractory:
-        d.tau_ref = P(node.tau_ref)
+        d.tau_ref = P(node.tau_ref, 4)
     if isinstance(node, ALIF):
         d.kind = L.BT_NEURON_ALIF
-        d.g_leak, d.E_leak, d.E_k, d.dg_k = P(node.g_leak), P(node.E_leak), P(node.E_k), P(node.dg_k)
-        d.tau_adapt = P(node.tau_adapt)
-        d.coef_gk = P(exp_euler_coef(node.tau_adapt, dt, owner=node, name="gk"))
+        d.g_leak, d.E_leak = P(node.g_leak, 5), P(node.E_leak, 6)
+        d.E_k, d.dg_k = P(node.E_k, 7), P(node.dg_k, 8)
+        d.tau_adapt = P(node.tau_adapt, 9)
+        d.coef_gk = P(exp_euler_coef(node.tau_adapt, dt, owner=node, name="gk"), 10)
     elif isinstance(node, LIF):
         d.kind = L.BT_NEURON_LIF
-        d.tau = P(node.tau)
+        d.tau = P(node.tau, 3)
     else:
         raise NotImplementedError(f"{type(node).__name__} has no B200 kernel")
+    slots = sorted(sources)
+    vals = scalar_values([sources[k] for k in slots])
+    if vals is not None:
+        d.uniform = 1
+        for k, v in zip(slots, vals):
+            d.sv[k] = v
     return d, keep
 
 

@@ -21,7 +21,7 @@ import torch.nn as nn
 from .. import _lib as L
 from . import autotune as _autotune
 from . import environ
-from ._ops import build_slices, neuron_desc, pack_csr_weights, pack_slice_weights
+from ._ops import build_slices, neuron_desc, pack_csr_weights, pack_slice_weights, scalar_values
 from .functional import named_hidden_states
 from .history import SpikeHistory
 from .linear import BaseSparseConn
@@ -267,6 +267,9 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     coef, tau = psc_mod.coefficients(dt)
     keep += [coef, tau]
     desc.psc_coef, desc.psc_tau = L.param(coef), L.param(tau)
+    pvals = scalar_values([coef, psc_mod.tau_syn])  # the module's own tensors: cached host copies
+    if pvals is not None:
+        desc.psc_uniform, desc.psc_coef_s, desc.psc_tau_s = 1, pvals[0], pvals[1]
     desc.mode = mode
     lay = conn.engine_layout(R, plan.uniform_delay, dev)
     w = static("w", conn._get_effective_weight().detach().float().contiguous())

@@ -44,7 +44,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 3
+#define BT_ABI_VERSION 4
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -186,6 +186,13 @@ typedef struct bt_neuron_desc {
   bt_param tau_ref;
   bt_param g_leak, E_leak, E_k, dg_k, tau_adapt; /* ALIF */
   bt_param coef_gk;        /* ALIF: expm1(dt * (-1/tau_adapt)) / (-1/tau_adapt), host-rounded */
+  /* When every parameter above is a scalar (stride 0) the caller may set
+     uniform = 1 and copy the values into sv[] = {v_threshold, v_reset, c_m,
+     tau, tau_ref, g_leak, E_leak, E_k, dg_k, tau_adapt, coef_gk} (unused
+     entries 0): the kernels then read no parameter memory.  The copies must
+     equal the pointed-to values. */
+  int32_t uniform;
+  float sv[11];
 } bt_neuron_desc;
 
 /* One BaseNode.single_step_forward (charge -> adaptation -> fire -> reset),
@@ -308,6 +315,11 @@ typedef struct bt_engine_desc {
      the sliced in-edge view sl_ptr / sl_src / sl_w instead (lane per post,
      ascending in-edge order, plain stores), 0 = never */
   int64_t dense_rows;
+  /* scalar PSC coefficients (psc_coef, psc_tau of stride 0): psc_uniform = 1
+     and their values, which must equal the pointed-to ones */
+  int32_t psc_uniform;
+  float psc_coef_s, psc_tau_s;
+  int32_t pad4_;
 } bt_engine_desc;
 
 /* Scratch words (int32) the scatter mode needs in bt_engine_desc.work. */
