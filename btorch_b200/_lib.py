@@ -26,7 +26,7 @@ _i64 = C.c_int64
 _i32 = C.c_int32
 
 
-ABI_VERSION = 4  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
+ABI_VERSION = 5  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
 
 
 class BtParam(C.Structure):
@@ -40,7 +40,7 @@ class BtNeuronDesc(C.Structure):
         ("v_threshold", BtParam), ("v_reset", BtParam), ("c_m", BtParam), ("tau", BtParam),
         ("tau_ref", BtParam), ("g_leak", BtParam), ("E_leak", BtParam), ("E_k", BtParam),
         ("dg_k", BtParam), ("tau_adapt", BtParam), ("coef_gk", BtParam),
-        ("uniform", _i32), ("sv", C.c_float * 11),
+        ("uniform", _i32), ("sv", C.c_float * 11), ("fast_div", _i32), ("rcp", C.c_float * 4),
     ]
 
 
@@ -58,7 +58,8 @@ class BtEngineDesc(C.Structure):
         ("sl_ptr", _vp), ("sl_src", _vp), ("sl_w", _vp), ("masks", _vp), ("outdeg", _vp),
         ("pull_words_per_warp", _i32), ("neuron_spt", _i32),
         ("work", _vp), ("stats", _vp), ("dense_rows", _i64),
-        ("psc_uniform", _i32), ("psc_coef_s", C.c_float), ("psc_tau_s", C.c_float), ("pad4_", _i32),
+        ("psc_uniform", _i32), ("psc_coef_s", C.c_float), ("psc_tau_s", C.c_float), ("psc_fast_div", _i32),
+        ("psc_rcp", C.c_float), ("pad5_", _i32),
     ]
 
 
@@ -73,6 +74,7 @@ _PROTOS = {
     "bt_spmv_grad_input": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_spmv_grad_weight": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_check_neuron_desc": (C.c_int, [C.POINTER(BtNeuronDesc)]),
+    "bt_fast_div_check": (C.c_int, [C.c_float, C.c_float, _vp, _vp]),
     "bt_neuron_step": (C.c_int, [C.POINTER(BtNeuronDesc), _i64, _i64] + [_vp] * 11 + [_vp]),
     "bt_neuron_step_backward": (C.c_int, [C.POINTER(BtNeuronDesc), _i64, _i64] + [_vp] * 13 + [_i32, _vp]),
     "bt_psc_step": (C.c_int, [_i64, _i64, BtParam, BtParam, _vp, _vp, _vp, _vp]),

@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, ip);
   const float pc = d.psc_uniform ? d.psc_coef_s : ld(d.psc_coef, ip);
   const float pt = d.psc_uniform ? d.psc_tau_s : ld(d.psc_tau, ip);
-  const float rpt = pow2_recip(pt);
+  const Div dpt = make_div(pt, d.psc_uniform && d.psc_fast_div, d.psc_rcp);
   const unsigned lane = lane_id();
   const bool traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace || d.spikes;
   uint32_t* hist_p = d.hist + (int64_t(si.h_t) * B + b0) * words + (i >> 5);
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
         v_p[o] = v;
         if (USE_REF) ref_p[o] = ref;
         if (KIND == BT_NEURON_ALIF) gk_p[o] = gk;
-        psc_p[o] = psc_decay(pc, pt, rpt, P);
+        psc_p[o] = psc_decay(pc, dpt, P);
       } else {
         // Finished sample: its state freezes at its last step.  On the first
         // step past the end the pending sum completes psc of that last step;

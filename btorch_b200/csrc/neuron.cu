@@ -128,6 +128,34 @@ int check_neuron_desc(const bt_neuron_desc* d) {
 
 extern "C" int bt_check_neuron_desc(const bt_neuron_desc* d) { return check_neuron_desc(d); }
 
+namespace {
+
+// Every fp32 bit pattern x once: fast quotient vs IEEE quotient.
+__global__ void k_fast_div_check(float c, float r, int32_t* mismatches) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  int bad = 0;
+  for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < (uint64_t(1) << 32); u += stride) {
+    const float x = __uint_as_float(uint32_t(u));
+    const float f = bt::div_recip(x, c, r), g = bt::div(x, c);
+    bad += (__float_as_uint(f) == __float_as_uint(g) || (f != f && g != g)) ? 0 : 1;
+  }
+  // a flag, not a count: up to 2^32 mismatches would overflow an int32 sum
+  if (__any_sync(0xffffffffu, bad != 0) && (threadIdx.x & 31) == 0) atomicOr(mismatches, 1);
+}
+
+}  // namespace
+
+extern "C" int bt_fast_div_check(float c, float rcp, int32_t* mismatches, void* stream) {
+  BT_CHECK_ARG(mismatches, "null mismatches");
+  BT_CHECK_ARG(c == c && c != 0.0f && c - c == 0.0f, "divisor must be finite and nonzero");
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_fast_div_check<<<sms * 16, 256, 0, static_cast<cudaStream_t>(stream)>>>(c, rcp, mismatches);
+  BT_CHECK_LAUNCH("k_fast_div_check");
+  return BT_OK;
+}
+
 extern "C" int bt_neuron_step(const bt_neuron_desc* d, int64_t batch, int64_t n, const float* x, const float* v_in,
                               const float* ref_in, const float* gk_in, float* v_out, float* ref_out, float* gk_out,
                               float* spike, float* u_save, float* mask_save, float* vch_save, void* stream) {

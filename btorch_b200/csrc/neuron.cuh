@@ -43,6 +43,43 @@ __device__ __forceinline__ float pow2_recip(float c) {
 // x / c with the reference's rounding; rc = pow2_recip(c).
 __device__ __forceinline__ float divc(float x, float c, float rc) { return rc != 0.0f ? mul(x, rc) : div(x, c); }
 
+// x / c from the correctly rounded reciprocal r of c: q = x r, then one FMA
+// correction with the exact remainder x - q c (Markstein's division step,
+// IBM J. Res. Dev. 34(1), 1990).  Outside 2^-100 <= |q| <= 2^100 (zeros,
+// subnormal or huge quotients, inf, nan) it divides.  Whether this equals the
+// IEEE quotient for every x depends on c; the host enables it only for
+// divisors checked exhaustively against __fdiv_rn (bt_fast_div_check).
+__device__ __forceinline__ float div_recip(float x, float c, float r) {
+  const float q = mul(x, r);
+  const float aq = fabsf(q);
+  if (!(aq >= 0x1p-100f && aq <= 0x1p100f)) return div(x, c);
+  const float e = __fmaf_rn(-q, c, x);
+  return __fmaf_rn(e, r, q);
+}
+
+// A divisor with its exact evaluation: kind 1 = power of two (multiply by the
+// exact reciprocal), 2 = verified reciprocal (div_recip), 0 = IEEE division.
+struct Div {
+  float c, r;
+  int kind;
+};
+
+__device__ __forceinline__ Div make_div(float c, bool verified, float rcp) {
+  Div d;
+  d.c = c;
+  d.r = pow2_recip(c);
+  d.kind = d.r != 0.0f ? 1 : 0;
+  if (d.kind == 0 && verified) {
+    d.r = rcp;
+    d.kind = 2;
+  }
+  return d;
+}
+
+__device__ __forceinline__ float divc(float x, const Div& d) {
+  return d.kind == 1 ? mul(x, d.r) : d.kind == 2 ? div_recip(x, d.c, d.r) : div(x, d.c);
+}
+
 // The parameters of one neuron, read once into registers (the kernels update
 // many samples of the same neuron with them).
 struct NeuronParams {
@@ -51,7 +88,7 @@ struct NeuronParams {
   float tau_ref;
   float ngl, El, Ek, dgk, tau_a, cgk;  // ALIF: -g_leak, E_leak, E_k, dg_k, tau_adapt, coef_gk
   float sg_alpha;
-  float r_cm, r_den, r_tau, r_tau_a;   // pow2_recip of the divisors (0: divide)
+  Div d_cm, d_den, d_tau, d_tau_a;     // the divisors with their evaluation
   int spiking;
 };
 
@@ -78,10 +115,10 @@ __device__ __forceinline__ NeuronParams load_params(const bt_neuron_desc& d, int
     } else {
       p.ngl = p.El = p.Ek = p.dgk = p.tau_a = p.cgk = 0.0f;
     }
-    p.r_cm = pow2_recip(p.cm);
-    p.r_den = pow2_recip(p.den);
-    p.r_tau = pow2_recip(p.tau);
-    p.r_tau_a = pow2_recip(p.tau_a);
+    p.d_cm = make_div(p.cm, d.fast_div & 1, d.rcp[0]);
+    p.d_den = make_div(p.den, d.fast_div & 2, d.rcp[1]);
+    p.d_tau = make_div(p.tau, d.fast_div & 4, d.rcp[2]);
+    p.d_tau_a = make_div(p.tau_a, d.fast_div & 8, d.rcp[3]);
     return p;
   }
   p.vth = ld(d.v_threshold, i);
@@ -103,10 +140,10 @@ __device__ __forceinline__ NeuronParams load_params(const bt_neuron_desc& d, int
   } else {
     p.ngl = p.El = p.Ek = p.dgk = p.tau_a = p.cgk = 0.0f;
   }
-  p.r_cm = pow2_recip(p.cm);
-  p.r_den = pow2_recip(p.den);
-  p.r_tau = pow2_recip(p.tau);
-  p.r_tau_a = pow2_recip(p.tau_a);
+  p.d_cm = make_div(p.cm, false, 0.0f);
+  p.d_den = make_div(p.den, false, 0.0f);
+  p.d_tau = make_div(p.tau, false, 0.0f);
+  p.d_tau_a = make_div(p.tau_a, false, 0.0f);
   return p;
 }
 
@@ -119,23 +156,23 @@ __device__ __forceinline__ NeuronOut neuron_update(const NeuronParams& pr, float
   float v1;
   if (KIND == BT_NEURON_LIF) {
     // euler_step(dV): v + dt * ((-(v - v_reset)) / tau + x / c_m)
-    v1 = add(v, mul(dt, add(divc(-sub(v, pr.vr), pr.tau, pr.r_tau), divc(I, pr.cm, pr.r_cm))));
+    v1 = add(v, mul(dt, add(divc(-sub(v, pr.vr), pr.d_tau), divc(I, pr.d_cm))));
   } else {
     // exp_euler_step(dV): derivative = ((-g_leak)(v - E_leak) + (-g_k)(v - E_k) + x) / c_m
     //                     linear     = ((-g_leak) - g_k) / c_m
     const float leak = mul(pr.ngl, sub(v, pr.El));
     const float adapt = mul(-gk, sub(v, pr.Ek));
-    const float deriv = divc(add(add(leak, adapt), I), pr.cm, pr.r_cm);
-    const float lin = divc(sub(pr.ngl, gk), pr.cm, pr.r_cm);
+    const float deriv = divc(add(add(leak, adapt), I), pr.d_cm);
+    const float lin = divc(sub(pr.ngl, gk), pr.d_cm);
     const float coef = div(expm1f(mul(dt, lin)), lin);
     v1 = add(v, mul(coef, deriv));
     // neuronal_adaptation: g_k + coef_gk * ((-g_k) / tau_adapt)
-    gk = add(gk, mul(pr.cgk, divc(-gk, pr.tau_a, pr.r_tau_a)));
+    gk = add(gk, mul(pr.cgk, divc(-gk, pr.d_tau_a)));
   }
   NeuronOut o;
   o.v_charged = v1;
   // neuronal_fire: surrogate((v - v_th) / (v_th - v_reset)) * (refractory == 0)
-  o.u = divc(sub(v1, pr.vth), pr.den, pr.r_den);
+  o.u = divc(sub(v1, pr.vth), pr.d_den);
   float s;
   if (SPIKING || pr.spiking)
     s = o.u >= 0.0f ? 1.0f : 0.0f;
@@ -168,6 +205,9 @@ __device__ __forceinline__ NeuronOut neuron_update(const bt_neuron_desc& d, int6
 // ExponentialPSC.conductance_charge: psc + coef * ((-psc) / tau_syn)
 __device__ __forceinline__ float psc_decay(float coef, float tau, float rtau, float p) {
   return add(p, mul(coef, divc(-p, tau, rtau)));
+}
+__device__ __forceinline__ float psc_decay(float coef, const Div& tau, float p) {
+  return add(p, mul(coef, divc(-p, tau)));
 }
 __device__ __forceinline__ float psc_decay(float coef, float tau, float p) {
   return psc_decay(coef, tau, pow2_recip(tau), p);

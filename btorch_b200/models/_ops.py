@@ -253,6 +253,31 @@ def scalar_values(tensors) -> list[float] | None:
     return out
 
 
+_FAST_DIV: dict = {}  # fp32 bit pattern of a divisor -> verified on the device
+
+
+def fast_division(c: float, device) -> tuple[bool, float]:
+    """(usable, reciprocal) for the reciprocal division of the kernels by the
+    scalar divisor c: its correctly rounded reciprocal, and whether
+    bt_fast_div_check found the fast quotient equal to the IEEE quotient for
+    every fp32 input (checked once per divisor value and process; powers of
+    two need no check, the kernels multiply by their exact reciprocal)."""
+    c32 = np.float32(c)
+    if not np.isfinite(c32) or c32 == 0:
+        return False, 0.0
+    r32 = np.float32(1.0) / c32
+    mant = int(c32.view(np.uint32)) & 0x7FFFFF
+    if mant == 0:
+        return False, float(r32)
+    key = int(c32.view(np.uint32))
+    if key not in _FAST_DIV:
+        m = torch.zeros(1, dtype=torch.int32, device=device)
+        L.check(L.lib().bt_fast_div_check(float(c32), float(r32), m.data_ptr(), L.stream_of(device)),
+                "bt_fast_div_check")
+        _FAST_DIV[key] = int(m.item()) == 0
+    return _FAST_DIV[key], float(r32)
+
+
 def neuron_desc(node, dt: float):
     """bt_neuron_desc for an LIF/ALIF module; returns (desc, keepalive).  When
     every parameter is a scalar, their values are also passed by value
@@ -301,6 +326,16 @@ def neuron_desc(node, dt: float):
         d.uniform = 1
         for k, v in zip(slots, vals):
             d.sv[k] = v
+        dev = sources[0].device
+        den = float(np.float32(d.sv[0]) - np.float32(d.sv[1]))  # v_threshold - v_reset in fp32
+        divisors = [(0, d.sv[2]), (1, den)]
+        divisors.append((2, d.sv[3]) if d.kind == L.BT_NEURON_LIF else (3, d.sv[9]))
+        if dev.type == "cuda":
+            for bit, c in divisors:
+                ok, r = fast_division(c, dev)
+                if ok:
+                    d.fast_div |= 1 << bit
+                    d.rcp[bit] = r
     return d, keep
 
 

@@ -21,6 +21,7 @@ import torch.nn as nn
 from .. import _lib as L
 from . import autotune as _autotune
 from . import environ
+from . import _ops
 from ._ops import build_slices, neuron_desc, pack_csr_weights, pack_slice_weights, scalar_values
 from .functional import named_hidden_states
 from .history import SpikeHistory
@@ -270,6 +271,8 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     pvals = scalar_values([coef, psc_mod.tau_syn])  # the module's own tensors: cached host copies
     if pvals is not None:
         desc.psc_uniform, desc.psc_coef_s, desc.psc_tau_s = 1, pvals[0], pvals[1]
+        ok, r = _ops.fast_division(pvals[1], psc_mod.tau_syn.device)
+        desc.psc_fast_div, desc.psc_rcp = int(ok), r
     desc.mode = mode
     lay = conn.engine_layout(R, plan.uniform_delay, dev)
     w = static("w", conn._get_effective_weight().detach().float().contiguous())

@@ -44,7 +44,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 4
+#define BT_ABI_VERSION 5
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -193,6 +193,13 @@ typedef struct bt_neuron_desc {
      equal the pointed-to values. */
   int32_t uniform;
   float sv[11];
+  /* With uniform = 1: bit k of fast_div says that x / divisor_k equals
+     fma(fma(-q, c, x), rcp[k], q) with q = x * rcp[k] for every fp32 x that
+     gives 2^-100 <= |q| <= 2^100 (IEEE division otherwise), as verified for
+     that divisor by bt_fast_div_check; divisors {c_m, v_threshold - v_reset,
+     tau, tau_adapt}, rcp = the correctly rounded reciprocal. */
+  int32_t fast_div;
+  float rcp[4];
 } bt_neuron_desc;
 
 /* One BaseNode.single_step_forward (charge -> adaptation -> fire -> reset),
@@ -228,6 +235,15 @@ BT_API int bt_neuron_step_backward(const bt_neuron_desc* d, int64_t batch, int64
 
 /* Validate a neuron descriptor without launching anything. */
 BT_API int bt_check_neuron_desc(const bt_neuron_desc* d);
+
+/* Exhaustive check of the reciprocal division for one divisor c (finite,
+ * nonzero) with rcp = the correctly rounded 1/c: over all 2^32 fp32 bit
+ * patterns x, sets *mismatches (device int32, zeroed by the caller) to 1 if
+ * the fast quotient of any x (as in bt_neuron_desc.fast_div) differs from the
+ * IEEE quotient x / c (NaN results compare equal).  0 makes the fast path
+ * bit-identical to division for that divisor.  About 2 ms on one B200;
+ * asynchronous on `stream`. */
+BT_API int bt_fast_div_check(float c, float rcp, int32_t* mismatches, void* stream);
 
 /* Exponential PSC step (btorch/models/synapse.py:99-103,171-178):
  * out = psc + coef * ((-psc) / tau_syn), then out = out + wz (wz may be
@@ -319,7 +335,9 @@ typedef struct bt_engine_desc {
      and their values, which must equal the pointed-to ones */
   int32_t psc_uniform;
   float psc_coef_s, psc_tau_s;
-  int32_t pad4_;
+  int32_t psc_fast_div;   /* 1: psc_tau verified as above, reciprocal psc_rcp */
+  float psc_rcp;
+  int32_t pad5_;
 } bt_engine_desc;
 
 /* Scratch words (int32) the scatter mode needs in bt_engine_desc.work. */
