@@ -494,11 +494,17 @@ def _peak():
     return float(peaks.get("hbm_gbs", 6650.0)), ("measured" if "hbm_gbs" in peaks else "fallback")
 
 
-def _traffic(name):
-    """DRAM bytes per batch of the step kernels, scaled from an ncu capture
-    (profiles/eng_step_<workload>_traffic.json), or None."""
-    tf = ROOT / "profiles" / f"eng_step_{name}_traffic.json"
-    return json.loads(tf.read_text()).get("dram_bytes_per_batch") if tf.exists() else None
+def _traffic(name, live_sample_steps):
+    """Estimated DRAM bytes per batch of the step launches: the bytes per step
+    of a warm steady-state ncu window (profiles/eng_step_<workload>_traffic.json,
+    neuron + scatter launches, `window_batch` live samples) scaled by the
+    batch's live sample-steps, or None without a capture."""
+    base = name.removesuffix("_short")
+    tf = ROOT / "profiles" / f"eng_step_{base}_traffic.json"
+    if not tf.exists():
+        return None
+    t = json.loads(tf.read_text())
+    return t["dram_bytes_per_step"] * live_sample_steps / t["window_batch"]
 
 
 def _allreduce(v, dev, op):
@@ -577,7 +583,7 @@ def measure(name, cfg, args, dev, world, rank, local):
     if rank == 0:
         peak, peak_src = _peak()
         achieved = algo_bytes / (step_ms * 1e-3) / 1e9
-        traffic = _traffic(name)
+        traffic = _traffic(name, live_steps / args.steps)
         line = {
             "metric": "synaptic_events_per_s", "value": value, "unit": "events/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
@@ -592,6 +598,7 @@ def measure(name, cfg, args, dev, world, rank, local):
             "roofline": {"bound": "hbm", "kernel": "recurrent step (neuron + synapse launches)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_src, "traffic": traffic,
+                         "traffic_note": "DRAM bytes per batch, scaled from profiles/eng_step_*_traffic.json",
                          "algorithmic_bytes_per_batch": algo_bytes / args.steps,
                          "step_ms_per_batch": step_ms / args.steps,
                          "projection_ms_per_batch": proj_ms / args.steps},
