@@ -65,6 +65,11 @@ __device__ __forceinline__ uint4 ld_nc_u4(const void* ptr, uint64_t pol) {
                : "l"(ptr), "l"(pol));
   return v;
 }
+__device__ __forceinline__ uint2 ld_nc_u2(const void* ptr, uint64_t pol) {
+  uint2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(ptr), "l"(pol));
+  return v;
+}
 __device__ __forceinline__ uint32_t ld_nc_u32(const void* ptr, uint64_t pol) {
   uint32_t v;
   asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(ptr), "l"(pol));

@@ -474,8 +474,11 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, i
       for (int u = 0; u < U; ++u) {
         const int32_t gi = g0 + u * G * 4;
         if (gi < end) {
-          dq[u] = ld_nc_u4(d.csr_dst + gi, pol_stream);
-          wq[u] = ld_nc_u4(d.csr_w + gi, pol_stream);
+          // edges gi .. gi+3 as (post, weight) records: two 128-bit loads
+          const uint4 a = ld_nc_u4(d.csr_edges + 2 * int64_t(gi), pol_stream);
+          const uint4 b = ld_nc_u4(d.csr_edges + 2 * int64_t(gi) + 4, pol_stream);
+          dq[u] = make_uint4(a.x, a.z, b.x, b.z);
+          wq[u] = make_uint4(a.y, a.w, b.y, b.w);
         } else {
           dq[u] = make_uint4(0u, 0u, 0u, 0u);
           wq[u] = dq[u];
@@ -609,8 +612,9 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter_flat(bt_engine_desc
         wv[u] = 0.0f;
         if (e < total) {
           const int32_t g = rbeg + (e - rexcl);
-          pp[u] = int(ld_nc_u32(d.csr_dst + g, pol_stream) & kIdMask);
-          wv[u] = ld_nc_f32(d.csr_w + g, pol_stream);
+          const uint2 e = ld_nc_u2(d.csr_edges + 2 * int64_t(g), pol_stream);
+          pp[u] = int(e.x & kIdMask);
+          wv[u] = __uint_as_float(e.y);
         } else {
 #pragma unroll
           for (int w = 0; w < MS; ++w) mm[u][w] = 0u;
@@ -1139,7 +1143,8 @@ int engine_check(const bt_engine_desc* d) {
   BT_CHECK_ARG(d->psc_coef.ptr && d->psc_tau.ptr, "PSC coefficients missing");
   BT_CHECK_ARG(d->neuron.spiking, "the fused engine needs a spiking (Heaviside) forward");
   if (d->mode == BT_MODE_SCATTER) {
-    BT_CHECK_ARG(d->csr_ptr && d->csr_dst && d->csr_w && d->ring && d->work, "scatter needs CSR, ring and work");
+    BT_CHECK_ARG(d->csr_ptr && d->csr_edges && d->ring && d->work, "scatter needs CSR, ring and work");
+    BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->csr_edges) & 15) == 0, "csr_edges must be 16-byte aligned");
     BT_CHECK_ARG(d->bin_lo >= 0 && d->bin_lo <= d->bin_hi && d->bin_hi < d->n_bins, "bins [%d, %d] outside [0, %d)",
                  d->bin_lo, d->bin_hi, d->n_bins);
     BT_CHECK_ARG(d->scatter_lanes == 0 || d->scatter_lanes == 1 || d->scatter_lanes == 8 || d->scatter_lanes == 32,
@@ -1150,9 +1155,6 @@ int engine_check(const bt_engine_desc* d) {
                  "dense delivery needs a single delay bin and the sliced in-edge view");
     BT_CHECK_ARG(d->neuron_spt == 0 || d->neuron_spt == 1 || d->neuron_spt == 2 || d->neuron_spt == 4,
                  "neuron_spt=%d (0, 1, 2 or 4)", d->neuron_spt);
-    BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->csr_dst) & 15) == 0 &&
-                     (reinterpret_cast<uintptr_t>(d->csr_w) & 15) == 0,
-                 "CSR edge arrays must be 16-byte aligned and padded to a multiple of 4");
   } else if (d->mode == BT_MODE_GATHER) {
     BT_CHECK_ARG(d->csc_ptr && d->csc_src && d->csc_w, "gather needs CSC");
   } else {

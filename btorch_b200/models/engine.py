@@ -282,9 +282,11 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     desc.csc_ptr, desc.csc_src, desc.csc_w = lay.csc_ptr.data_ptr(), lay.csc_src.data_ptr(), w.data_ptr()
     if mode == L.BT_MODE_SCATTER:
         lay_s = conn.scatter_layout(R, plan.uniform_delay, dev)
-        w_csr = static("w_csr", pack_csr_weights(lay_s, w))
-        keep.append(w_csr)
-        desc.csr_ptr, desc.csr_dst, desc.csr_w = lay_s.csr_ptr.data_ptr(), lay_s.csr_dst.data_ptr(), w_csr.data_ptr()
+        w_csr = pack_csr_weights(lay_s, w)
+        # one (post, weight) record per edge, interleaved
+        edges = static("csr_edges", torch.stack([lay_s.csr_dst, w_csr.view(torch.int32)], 1).reshape(-1))
+        keep += [w_csr, edges]
+        desc.csr_ptr, desc.csr_edges = lay_s.csr_ptr.data_ptr(), edges.data_ptr()
         desc.bin_lo, desc.bin_hi = lay_s.bin_lo, lay_s.bin_hi
         desc.scatter_lanes = choice.scatter_lanes or (1 if lay_s.mean_row < 48 else 32)
         desc.neuron_spt = choice.neuron_spt or 4

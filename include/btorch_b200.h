@@ -44,7 +44,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 5
+#define BT_ABI_VERSION 6
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -338,6 +338,10 @@ typedef struct bt_engine_desc {
   int32_t psc_fast_div;   /* 1: psc_tau verified as above, reciprocal psc_rcp */
   float psc_rcp;
   int32_t pad5_;
+  /* scatter: the expanded CSR's edges interleaved, [2 * len(csr_dst)] words:
+     post, weight bits, post, weight bits, ... (one 8-byte record per edge, so
+     a short row occupies the fewest memory sectors); 16-byte aligned */
+  const uint32_t* csr_edges;
 } bt_engine_desc;
 
 /* Scratch words (int32) the scatter mode needs in bt_engine_desc.work. */
