@@ -83,6 +83,8 @@ _PROTOS = {
     "bt_input_project": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_bits_to_float": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
     "bt_float_to_bits": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
+    "bt_raster_count": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
+    "bt_raster_coords": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_float_to_masks": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
     "bt_mask_stride": (C.c_int, [_i64]),
     "bt_engine_work_words": (C.c_int64, [_i64, _i64, _i32]),

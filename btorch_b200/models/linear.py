@@ -21,6 +21,7 @@ import torch.nn as nn
 from .. import config as bt_config
 from .._sparse_config import BACKEND_NAMES, SparseBackendConfig
 from . import _ops
+from .constrain import HasConstraint
 from ._ops import SparseLayout, build_layout, pack_csr_weights
 
 
@@ -38,7 +39,7 @@ def available_sparse_backends(*, include_experimental: bool = False) -> list[str
     return list(BACKEND_NAMES)
 
 
-class DenseConn(nn.Linear):
+class DenseConn(nn.Linear, HasConstraint):
     """Dense connection y = x @ W (+ b) with optional mask and Dale sign
     (linear.py:163-228).  Inside the fused engine its projection runs as an
     event-driven kernel over the nonzero inputs; stepped alone it is nn.Linear."""
@@ -216,7 +217,7 @@ class BaseSparseConn(nn.Module):
         return out
 
 
-class SparseConn(BaseSparseConn):
+class SparseConn(BaseSparseConn, HasConstraint):
     """Sparse linear map with a learnable magnitude per stored nonzero and an
     optional Dale sign (linear.py:535-591)."""
 
@@ -263,4 +264,113 @@ class SparseConn(BaseSparseConn):
             self.magnitude.data = (self.magnitude * self.initial_sign).relu() * self.initial_sign
 
 
-__all__ = ["DenseConn", "BaseSparseConn", "SparseConn", "available_sparse_backends"]
+class SparseConstrainedConn(BaseSparseConn, HasConstraint):
+    """Sparse linear layer whose weights share learnable magnitudes by
+    constraint group (btorch/models/linear.py:594-867): effective weight of
+    stored nonzero e = initial_weight[e] * magnitude[group[e]], groups given by
+    a constraint matrix of 1-based group ids with the sparsity of `conn`.
+    Runs on the same kernels as SparseConn (the effective weight is formed on
+    the device once per call or run); the gradient of a magnitude is the sum
+    over its group of initial_weight times the per-nonzero weight gradient."""
+
+    def __init__(self, conn, constraint, enforce_dale: bool = True, bias=None, sparse_backend: str | None = None,
+                 sparse_config=None, device=None, dtype=None, persist_initial_weight: bool = False):
+        self.enforce_dale = enforce_dale
+        self.persist_initial_weight = persist_initial_weight
+        self.constraint_info = None
+        c = constraint.T
+        if not isinstance(c, scipy.sparse.coo_array):
+            c = scipy.sparse.coo_array(c)
+        c.eliminate_zeros()
+        self._constraint_matrix = c
+        super().__init__(conn, bias=bias, sparse_backend=sparse_backend, sparse_config=sparse_config,
+                         device=device, dtype=dtype)
+
+    def _init_weights(self, value):
+        self.register_buffer("initial_weight", value, persistent=self.persist_initial_weight)
+        n_groups = int(self._constraint_matrix.data.max()) if self._constraint_matrix.nnz else 0
+        self.magnitude = nn.Parameter(torch.ones(n_groups, dtype=value.dtype, device=value.device))
+        self.register_buffer("_constraint_scatter_indices",
+                             torch.as_tensor(self._group_of_nonzeros(), dtype=torch.long, device=value.device),
+                             persistent=False)
+
+    def _group_of_nonzeros(self) -> np.ndarray:
+        """0-based group id of every stored nonzero (canonical order), looked
+        up in the constraint matrix by (post, src) key."""
+        idx = self.indices.cpu().numpy()
+        n_src = max(self.in_features, 1)
+        key = idx[0].astype(np.int64) * n_src + idx[1]
+        c = self._constraint_matrix
+        ckey = c.row.astype(np.int64) * n_src + c.col
+        order = np.argsort(ckey, kind="stable")
+        ckey, gid = ckey[order], c.data[order].astype(np.int64)
+        pos = np.searchsorted(ckey, key)
+        ok = (pos < ckey.size) & (ckey[np.minimum(pos, max(ckey.size - 1, 0))] == key) if ckey.size else \
+            np.zeros(key.size, bool)
+        if not ok.all():
+            raise AssertionError("Constraint missing for some connections.")
+        return gid[pos] - 1
+
+    def reset_parameters(self) -> None:
+        nn.init.ones_(self.magnitude)
+
+    def _get_effective_weight(self):
+        return self.initial_weight * self.magnitude[self._constraint_scatter_indices]
+
+    def constrain(self, *args, **kwargs):
+        if self.enforce_dale:
+            self.magnitude.data = self.magnitude.relu()
+
+    @classmethod
+    def from_hetersynapse(cls, conn, constraint, receptor_type_index, enforce_dale: bool = True, bias=None,
+                          sparse_backend=None, sparse_config=None, device=None, dtype=None,
+                          persist_initial_weight: bool = False) -> "SparseConstrainedConn":
+        inst = cls(conn=conn, constraint=constraint, enforce_dale=enforce_dale, bias=bias,
+                   sparse_backend=sparse_backend, sparse_config=sparse_config, device=device, dtype=dtype,
+                   persist_initial_weight=persist_initial_weight)
+        inst.constraint_info = {"receptor_type_index": receptor_type_index}
+        return inst
+
+    def get_group_info(self, include_weights: bool = False):
+        import pandas as pd
+
+        gid = self._constraint_scatter_indices
+        n_groups = len(self.magnitude)
+        counts = torch.bincount(gid, minlength=n_groups).cpu().tolist()
+        mags = self.magnitude.detach().cpu().tolist()
+        rows = []
+        for g in range(n_groups):
+            info = {"group_id": g, "num_connections": counts[g], "current_magnitude": mags[g]}
+            if include_weights:
+                w = self.initial_weight[gid == g]
+                info["mean_initial_weight"] = w.mean().item()
+                info["std_initial_weight"] = w.std(unbiased=False).item()
+            rows.append(info)
+        df = pd.DataFrame(rows)
+        if self.constraint_info is not None:
+            ri = self.constraint_info["receptor_type_index"]
+            if len(ri) == n_groups:
+                df = pd.concat([df, ri.reset_index(drop=True)], axis=1)
+        return df
+
+    def set_group_magnitude(self, group_id: int | None = None, receptor_pair=None, value=1.0):
+        if (group_id is None) == (receptor_pair is None):
+            raise ValueError("Exactly one of group_id or receptor_pair must be specified")
+        if receptor_pair is not None:
+            if self.constraint_info is None:
+                raise ValueError("receptor_pair can only be used if created via from_hetersynapse")
+            ri = self.constraint_info["receptor_type_index"]
+            if "pre_receptor_type" not in ri.columns:
+                raise ValueError("receptor_pair requires neuron mode (pre_receptor_type, post_receptor_type)")
+            group_id = ri.set_index(["pre_receptor_type", "post_receptor_type"]).loc[tuple(receptor_pair),
+                                                                                    "receptor_index"]
+        if isinstance(value, (int, float)):
+            value = torch.tensor(value, dtype=self.magnitude.dtype, device=self.magnitude.device)
+        self.magnitude.data[group_id] = value
+
+    def get_weights_by_group(self) -> dict:
+        gid = self._constraint_scatter_indices
+        return {g: self.initial_weight[gid == g] * self.magnitude[g] for g in range(len(self.magnitude))}
+
+
+__all__ = ["DenseConn", "BaseSparseConn", "SparseConn", "SparseConstrainedConn", "available_sparse_backends"]

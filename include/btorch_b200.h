@@ -388,6 +388,18 @@ BT_API int bt_masks_to_float(int64_t batch, int64_t n, const uint32_t* masks,
                              float* out, void* stream);
 
 /* Pack fp32 rows [rows][n] into bitmaps (bit set where the value != 0). */
+/* Spike rasters as sparse coordinates (replaces the dense np.nonzero of the
+ * reference's to_sparse_repr, btorch/io/serialization.py:80-141, for spike
+ * stacks).  bits: [rows = T * batch][ceil(n/32)] bitmask raster.
+ * bt_raster_count: counts[r] = spikes in row r.  bt_raster_coords: with
+ * offsets = exclusive scan of counts, writes the (time, batch, neuron)
+ * coordinates of every spike, row-major (time, then batch, then ascending
+ * neuron), as int32. */
+BT_API int bt_raster_count(int64_t rows, int64_t n, const uint32_t* bits, int64_t* counts, void* stream);
+BT_API int bt_raster_coords(int64_t rows, int64_t batch, int64_t n, const uint32_t* bits,
+                            const int64_t* offsets, int32_t* idx_time, int32_t* idx_batch,
+                            int32_t* idx_neuron, void* stream);
+
 BT_API int bt_float_to_bits(int64_t rows, int64_t n, const float* in,
                      uint32_t* bits, void* stream);
 

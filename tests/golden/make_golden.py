@@ -350,6 +350,58 @@ def case_fp64(rng, *, n, p, steps, c_in, rate, scale, in_gain):
     return out
 
 
+def case_constrained(rng):
+    """SparseConstrainedConn (3 groups) forward and backward on graded inputs,
+    with non-unit group magnitudes."""
+    import scipy.sparse as sp
+    import torch
+    from btorch.models.linear import SparseConstrainedConn
+
+    n_in, n_out, B, G = 120, 90, 4, 3
+    W = ((rng.random((n_in, n_out)) < 0.15) * rng.standard_normal((n_in, n_out))).astype(np.float32)
+    Wc = sp.coo_array(W)
+    C = sp.coo_array((rng.integers(1, G + 1, size=Wc.nnz).astype(np.float32), (Wc.row, Wc.col)), shape=W.shape)
+    m = SparseConstrainedConn(Wc, C, sparse_backend="native")
+    mag = np.array([0.5, 1.25, 2.0], np.float32)
+    with torch.no_grad():
+        m.magnitude.copy_(torch.tensor(mag))
+    x = torch.tensor(((rng.random((B, n_in)) < 0.3) * rng.standard_normal((B, n_in))).astype(np.float32),
+                     requires_grad=True)
+    out = m(x)
+    g = torch.tensor(rng.standard_normal((B, n_out)).astype(np.float32))
+    (out * g).sum().backward()
+    return dict(n_in=n_in, n_out=n_out, W=W, C_row=C.row.astype(np.int64), C_col=C.col.astype(np.int64),
+                C_data=C.data, magnitude=mag, x=x.detach().numpy(), out=out.detach().numpy(), g=g.numpy(),
+                grad_x=x.grad.numpy(), grad_mag=m.magnitude.grad.numpy(),
+                group=m._constraint_scatter_indices.numpy())
+
+
+def case_receptors(rng, *, n, p, batch, steps, n_rec):
+    """LIF + HeterSynapsePSC with n_rec receptors (ExponentialPSC base, a time
+    constant per receptor), no delays: the connection maps presynaptic
+    neurons to (post, receptor) pairs, flat index post * n_rec + receptor."""
+    import pandas as pd
+    import scipy.sparse as sp
+    import torch
+    from btorch.models.linear import SparseConn
+    from btorch.models.neurons import LIF
+    from btorch.models.synapse import ExponentialPSC, HeterSynapsePSC
+
+    Wd = make_conn(rng, n, n * n_rec, p, dyadic=True, dy_exp=-6)
+    conn = SparseConn(sp.coo_array(Wd), sparse_backend="native")
+    taus = np.array([5.0, 20.0, 2.0, 10.0][:n_rec], np.float32)
+    rti = pd.DataFrame({"receptor_type": [f"r{r}" for r in range(n_rec)], "receptor_index": list(range(n_rec))})
+    syn = HeterSynapsePSC(n, n_rec, rti, conn, base_psc=ExponentialPSC,
+                          tau_syn=torch.tensor(np.tile(taus, n)))
+    neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=2.0, hard_reset=True)
+    x = (np.round(rng.poisson(0.06, size=(steps, batch, n)) * 0.75 * 64) / 64).astype(np.float32)
+    _, z, st, _ = _run_rnn(neuron, syn, None, x, batch, ("neuron.v", "synapse.psc", "synapse.base_psc.psc"))
+    post, src, w = canonical(Wd)
+    return dict(n=n, batch=batch, n_rec=n_rec, taus=taus, post=post, src=src, w=w, x=x,
+                z=np.packbits(z.astype(np.uint8), axis=-1, bitorder="little"), v=st["neuron.v"],
+                psc=st["synapse.psc"], psc_rec=st["synapse.base_psc.psc"])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -377,6 +429,8 @@ def main():
                                              spiking=False, chunk=10, unroll=5),
         "fp64_c1": lambda r: case_fp64(r, n=1024, p=0.08, steps=200, c_in=250, rate=0.04, scale=0.01,
                                        in_gain=GAIN["c1"]),
+        "constrained_spmm": lambda r: case_constrained(r),
+        "receptors2": lambda r: case_receptors(r, n=200, p=0.03, batch=3, steps=100, n_rec=2),
     }
     only = set(args.only.split(",")) if args.only else None
     for i, (name, fn) in enumerate(cases.items()):
@@ -386,7 +440,7 @@ def main():
         d = fn(rng)
         # Full spike rasters (bit-packed) are kept; float traces only for the
         # first TRACE_STEPS steps, plus the state after the last step.
-        for key in ("v", "psc", "g_k"):
+        for key in ("v", "psc", "g_k", "psc_rec"):
             if key in d and "z" in d and d[key].ndim == 3:
                 d[key + "_final"] = d[key][-1]
                 d[key] = d[key][:TRACE_STEPS]
