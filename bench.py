@@ -507,6 +507,14 @@ def _traffic(name, live_sample_steps):
     return t["dram_bytes_per_step"] * live_sample_steps / t["window_batch"]
 
 
+def job_totals(elapsed_ms: float, events: int, dev) -> tuple[float, int]:
+    """Whole-job time and work of a replica run: the slowest rank's device time
+    and the sum of every rank's events (one all-reduce each, every rank)."""
+    import torch.distributed as dist
+
+    return _allreduce(elapsed_ms, dev, dist.ReduceOp.MAX), int(_allreduce(events, dev, dist.ReduceOp.SUM))
+
+
 def _allreduce(v, dev, op):
     import torch.distributed as dist
 
@@ -576,8 +584,7 @@ def measure(name, cfg, args, dev, world, rank, local):
     if world > 1:
         import torch.distributed as dist
 
-        elapsed_ms = _allreduce(elapsed_ms, dev, dist.ReduceOp.MAX)
-        events_total = int(_allreduce(events_total, dev, dist.ReduceOp.SUM))
+        elapsed_ms, events_total = job_totals(elapsed_ms, events_total, dev)
     value = events_total / (elapsed_ms * 1e-3)
     line = None
     if rank == 0:
@@ -678,8 +685,7 @@ def main():
         if world > 1:
             import torch.distributed as dist
 
-            e2e_ms = _allreduce(e2e_ms, dev, dist.ReduceOp.MAX)
-            ev = int(_allreduce(ev, dev, dist.ReduceOp.SUM))
+            e2e_ms, ev = job_totals(e2e_ms, ev, dev)
         if rank == 0:
             line["e2e"] = {"value": ev / (e2e_ms * 1e-3), "unit": "events/s",
                            "h2d_bytes_per_step": int(x_host.numel() * 4),
