@@ -59,6 +59,9 @@ CONFIGS = {
                           rate=(2.0, 40.0), dur=(512, 512), w_scale=0.0030, in_gain=1.0, s_state=36),
     "connectome_short": dict(model="lif_hetero_delay", n=140000, indeg=350, indeg_sigma=1.0, n_bins=20, exc=0.7,
                              batch=8, t_max=256, dur=(256, 256), c_m=64.0, drive=(0.25, 8.0), s_state=36),
+    # plain forward simulation: the reference's own CPU-runnable case, batch 1
+    "plain": dict(model="lif_plain", n=4096, p=0.02, batch=1, c_in=1000, t_max=1000, in_rate=0.01, in_std=0.05,
+                  w_scale=0.1, dur=(1000, 1000), s_state=36),
     # serving: Poisson request stream over a pool of connectome-shaped networks
     "serving": dict(model="serving", sizes=(16384, 32768, 65536, 140000), indeg=350, indeg_sigma=1.0, n_bins=20,
                     exc=0.7, c_m=64.0, c_in=4000, in_std=0.05, rate_hz=200.0, n_requests=200,
@@ -77,7 +80,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="batched", choices=sorted(CONFIGS))
-    ap.add_argument("--extra", default="connectome,training,serving",
+    ap.add_argument("--extra", default="plain,connectome,training,serving",
                     help="comma-separated workloads measured after the headline one ('' for none)")
     ap.add_argument("--direction", default="scatter", choices=["scatter", "gather", "auto"])
     ap.add_argument("--no-cudagraph", action="store_true", help="launch every chunk eagerly")
@@ -126,6 +129,17 @@ def make_network(cfg, seed=0):
         w = np.where(exc, w, np.float32(-0.4) * w).astype(np.float32)
         w_in = (rng.normal(0.0, 0.05, size=(cfg["c_in"], n)) * cfg["in_gain"]).astype(np.float32)
         return dict(post=post, src=src, pre=src, w=w, n_bins=1, w_in=w_in)
+    if cfg["model"] == "lif_plain":
+        # fixed connection probability (binomial in-degree), lognormal weights,
+        # inhibitory presynaptic neurons (last 20 %) scaled by -0.4
+        k = rng.binomial(n, cfg["p"], size=n)
+        post = np.repeat(np.arange(n, dtype=np.int64), k)
+        pre = rng.integers(0, n, size=post.size, dtype=np.int64)
+        post, pre = _dedupe_sorted(post, pre, n)
+        w = rng.lognormal(-1.0, 1.0, size=pre.size).astype(np.float32) * np.float32(cfg["w_scale"])
+        w = np.where(pre < int(0.8 * n), w, np.float32(-0.4) * w).astype(np.float32)
+        w_in = rng.normal(0.0, cfg["in_std"], size=(cfg["c_in"], n)).astype(np.float32)
+        return dict(post=post, src=pre, pre=pre, w=w, n_bins=1, w_in=w_in)
     # connectome-shaped: lognormal in-degree, presynaptic type sets the sign,
     # per-synapse delay d in 1..R lands in delay bin d - 1
     R = cfg["n_bins"]
@@ -304,6 +318,10 @@ def build_model(cfg, net, device, direction, batch=None):
                       tau_adapt=200.0, dg_k=0.07, tau_ref=2.0, hard_reset=True)
         syn = ExponentialPSC(n, tau_syn=5.0, linear=conn)
         inp = DenseConn(cfg["c_in"], n, weight=torch.from_numpy(net["w_in"]))
+    elif cfg["model"] == "lif_plain":
+        neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=2.0, hard_reset=True)
+        syn = ExponentialPSC(n, tau_syn=5.0, linear=conn)
+        inp = DenseConn(cfg["c_in"], n, weight=torch.from_numpy(net["w_in"]))
     else:
         neuron = LIF(n, v_threshold=1.0, v_reset=0.0, c_m=cfg["c_m"], tau=20.0, tau_ref=2.0, hard_reset=True)
         rti = pd.DataFrame({"receptor_type": ["syn"], "receptor_index": [0]})
@@ -324,6 +342,8 @@ def make_inputs(cfg, seed, device):
         rates = lo + (hi - lo) * torch.rand(B, generator=g, device=device)
         p = (rates * 1e-3).view(1, B, 1).expand(T, B, C)
         x = torch.poisson(p.contiguous(), generator=g)
+    elif cfg["model"] == "lif_plain":
+        x = torch.poisson(torch.full((T, B, cfg["c_in"]), cfg["in_rate"], device=device), generator=g)
     else:
         lam, amp = cfg["drive"]
         x = torch.empty((T, B, cfg["n"]), device=device, dtype=torch.float32)
@@ -336,6 +356,9 @@ def make_inputs(cfg, seed, device):
 
 
 def describe(name, cfg):
+    if cfg["model"] == "lif_plain":
+        return (f"{name}: LIF+ExpPSC N={cfg['n']} p={cfg['p']} lognormal(-1,1)x{cfg['w_scale']} E/I 80/20 "
+                f"batch {cfg['batch']} T {cfg['t_max']} c_in {cfg['c_in']} at {cfg['in_rate'] * 1e3:.0f} Hz")
     if cfg["model"] == "alif_dense_input":
         return (f"{name}: ALIF+ExpPSC N={cfg['n']} fixed in-degree {cfg['indeg']} batch {cfg['batch']} "
                 f"durations {cfg['dur']} T_max {cfg['t_max']} c_in {cfg['c_in']}")
@@ -410,6 +433,11 @@ def oracle_spec(cfg, net):
                   "dg_k": 0.07, "tau_adapt": 200.0, "coef_gk": coef_gk, "tau_ref": 2.0, "psc_coef": coef_syn,
                   "psc_tau": 5.0}
         return O.NetSpec(n=n, kind=1, hard_reset=True, use_ref=True, dt=1.0, params=params, ptr=ptr,
+                         pre=net["pre"].astype(np.int32), delay=np.zeros(net["pre"].size, np.int32), w=net["w"])
+    if cfg["model"] == "lif_plain":
+        params = {"v_threshold": 1.0, "v_reset": 0.0, "c_m": 1.0, "tau": 20.0, "tau_ref": 2.0,
+                  "psc_coef": coef_syn, "psc_tau": 5.0}
+        return O.NetSpec(n=n, kind=0, hard_reset=True, use_ref=True, dt=1.0, params=params, ptr=ptr,
                          pre=net["pre"].astype(np.int32), delay=np.zeros(net["pre"].size, np.int32), w=net["w"])
     params = {"v_threshold": 1.0, "v_reset": 0.0, "c_m": cfg["c_m"], "tau": 20.0, "tau_ref": 2.0,
               "psc_coef": coef_syn, "psc_tau": 5.0}
@@ -724,9 +752,14 @@ def main():
             torch.cuda.empty_cache()
             continue
         sub, m, xe, le, ne, _ = measure(extra, ecfg, args, dev, world, rank, local)
-        if rank == 0 and world == 1:
+        if rank == 0 and world == 1 and ecfg["batch"] > 1:
             sub["plain_step"] = plain_step(ecfg, ne, xe, le, args, dev)
             sub["vs_plain_step"] = sub["value"] / sub["plain_step"]["value"]
+        if rank == 0 and world == 1 and ecfg["model"] == "lif_plain" and not args.no_cpu_baseline:
+            # the reference's CPU case at full length
+            e, t, thr = cpu_sample(ecfg, ne, xe.cpu().numpy(), ecfg["t_max"])
+            sub["cpu_baseline"] = {"value": e / t, "unit": "events/s", "cores": thr, "kind": "port",
+                                   "sample": f"all {ecfg['t_max']} steps ({t:.2f} s)", "ms_per_step": 1e3 * t / ecfg["t_max"]}
         if rank == 0:
             for k in ("metric", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline",
                       "dtype", "data"):
