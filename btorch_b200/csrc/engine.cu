@@ -33,6 +33,7 @@
 //   ascending canonical order of w * z_{t-1-bin}[pre] (fmaf chain, exactly the
 //   reference's CPU rounding), then runs the neuron update of step t.  The
 //   last synapse update of a run is k_eng_gather_final.
+#include <algorithm>
 #include <type_traits>
 
 #include "neuron.cuh"
@@ -1173,7 +1174,12 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const unsigned planes = unsigned(d.bin_hi - d.bin_lo + 1);
-    const dim3 sgrid(unsigned(ceil_div(int64_t(sms) * 8, planes)), planes);
+    // a plane lists at most n rows: no more blocks than n rows need (small
+    // networks would otherwise launch mostly idle blocks every step)
+    const int64_t rows_per_block = d.scatter_lanes == 1 ? kEngThreads : d.scatter_lanes == 8 ? kEngThreads / 8
+                                                                                            : kEngThreads / 32;
+    const int64_t xblocks = std::min(ceil_div(int64_t(sms) * 8, planes), ceil_div(n, rows_per_block));
+    const dim3 sgrid(unsigned(std::max<int64_t>(xblocks, 1)), planes);
     const int ms = mask_stride(d.batch);
     auto neuron = S == 1 ? k_eng_neuron<KIND, HARD, USE_REF, 1>
                 : S == 2 ? k_eng_neuron<KIND, HARD, USE_REF, 2> : k_eng_neuron<KIND, HARD, USE_REF, 4>;
