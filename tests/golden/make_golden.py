@@ -402,6 +402,127 @@ def case_receptors(rng, *, n, p, batch, steps, n_rec):
                 psc=st["synapse.psc"], psc_rec=st["synapse.base_psc.psc"])
 
 
+
+def connectome_tables(rng, n, n_conn, nan_ids=(), dup=True):
+    """Seeded neuron and connection tables in the reference's column layout
+    (simple_id, EI; pre/post_simple_id, syn_count, delay_steps, nt)."""
+    import pandas as pd
+
+    ei = rng.choice(np.array(["E", "I"], dtype=object), size=n, p=[0.7, 0.3])
+    ei[list(nan_ids)] = np.nan
+    neurons = pd.DataFrame({"simple_id": np.arange(n), "root_id": 1000 + np.arange(n), "EI": ei})
+    pre = rng.integers(0, n, n_conn)
+    post = rng.integers(0, n, n_conn)
+    if not dup:
+        key = np.unique(pre * n + post)
+        key = rng.permutation(key)
+        pre, post = key // n, key % n
+    conns = pd.DataFrame({"pre_simple_id": pre, "post_simple_id": post,
+                          "syn_count": rng.integers(1, 10, len(pre)),
+                          "delay_steps": rng.integers(0, 8, len(pre)),
+                          "nt": rng.choice(np.array(["ach", "gaba", "glut"], dtype=object), size=len(pre))})
+    return neurons, conns
+
+
+def _save_coo(out, name, m):
+    m = m.tocoo()
+    out[f"{name}.row"] = np.asarray(m.row, np.int64)
+    out[f"{name}.col"] = np.asarray(m.col, np.int64)
+    out[f"{name}.data"] = np.asarray(m.data)
+    out[f"{name}.shape"] = np.asarray(m.shape, np.int64)
+
+
+def case_connectome_format(rng):
+    """make_hetersynapse_conn / stack_hetersynapse outputs (entries in the
+    reference's own order) on seeded tables, every mode the reference has."""
+    import json
+    import warnings
+
+    from btorch.connectome.connection import make_hetersynapse_conn, stack_hetersynapse
+
+    out = {}
+    tables = {"dup": connectome_tables(rng, 60, 500, nan_ids=(3, 17, 41)),
+              "uniq": connectome_tables(rng, 50, 400, dup=False)}
+    for t, (neu, con) in tables.items():
+        for c in neu.columns:
+            out[f"in.{t}.neurons.{c}"] = neu[c].to_numpy().astype(str if c == "EI" else np.int64)
+        for c in con.columns:
+            out[f"in.{t}.conns.{c}"] = con[c].to_numpy().astype(str if c == "nt" else np.int64)
+    neu_nan, con_dup = tables["dup"]
+    neu_ok = neu_nan.copy()
+    neu_ok.loc[neu_ok.EI.isna(), "EI"] = "E"
+    neu_u, con_u = tables["uniq"]
+    runs = {
+        "neuron": (neu_ok, con_dup, dict()),
+        "neuron_ignore_post": (neu_ok, con_dup, dict(ignore_post_type=True)),
+        "neuron_delay": (neu_ok, con_dup, dict(delay_col="delay_steps", n_delay_bins=5)),
+        "neuron_filter": (neu_nan, con_dup, dict(dropna="filter")),
+        "neuron_unknown": (neu_nan, con_dup, dict(dropna="unknown")),
+        "neuron_filter_ignore_post": (neu_nan, con_dup, dict(dropna="filter", ignore_post_type=True)),
+        "connection": (neu_ok, con_dup, dict(receptor_type_col="nt", receptor_type_mode="connection")),
+        "connection_delay": (neu_u, con_u, dict(receptor_type_col="nt", receptor_type_mode="connection",
+                                                delay_col="delay_steps", n_delay_bins=6)),
+        "delay_only": (neu_ok, con_dup, dict(receptor_type_col=None, delay_col="delay_steps", n_delay_bins=4)),
+    }
+    for name, (neu, con, kw) in runs.items():
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            m, idx = make_hetersynapse_conn(neu, con, **kw)
+        _save_coo(out, name, m)
+        out[f"{name}.index"] = np.array(idx.to_json(orient="split"))
+        out[f"{name}.kwargs"] = np.array(json.dumps(kw))
+    for mode, kw in (("dict_neuron", dict()), ("dict_connection", dict(receptor_type_col="nt",
+                                                                      receptor_type_mode="connection"))):
+        d, idx = make_hetersynapse_conn(neu_ok, con_dup, return_dict=True, **kw)
+        out[f"{mode}.keys"] = np.array(json.dumps([list(k) if isinstance(k, tuple) else k for k in d]))
+        for i, m in enumerate(d.values()):
+            _save_coo(out, f"{mode}.{i}", m)
+        out[f"{mode}.index"] = np.array(idx.to_json(orient="split"))
+        for how in ("pre", "post", "all"):
+            m2, idx2 = stack_hetersynapse(d, idx, ignore_receptor_type=how)
+            _save_coo(out, f"{mode}.collapse_{how}", m2)
+            out[f"{mode}.collapse_{how}.index"] = np.array(idx2.to_json(orient="split"))
+        _save_coo(out, f"{mode}.stacked", stack_hetersynapse(d, idx))
+    return out
+
+
+def case_receptors_delay(rng, *, n, n_conn, batch, steps, D):
+    """LIF + HeterSynapsePSC(n_receptor=4 E/I pairs, ExponentialPSC with a time
+    constant per receptor, max_delay_steps=D) on the matrix
+    make_hetersynapse_conn(..., delay_col, n_delay_bins=D) builds from seeded
+    tables; weights syn_count * 2**-5, negative from inhibitory neurons."""
+    import scipy.sparse as sp
+    import torch
+    from btorch.connectome.connection import make_hetersynapse_conn
+    from btorch.models.linear import SparseConn
+    from btorch.models.neurons import LIF
+    from btorch.models.synapse import ExponentialPSC, HeterSynapsePSC
+
+    neu, con = connectome_tables(rng, n, n_conn)
+    m, idx = make_hetersynapse_conn(neu, con, delay_col="delay_steps", n_delay_bins=D)
+    m = m.tocoo()
+    inh = (neu.EI.to_numpy() == "I")[m.row // D]
+    w = (m.data * 2.0**-5 * np.where(inh, -1.0, 1.0)).astype(np.float32)
+    W = sp.coo_array((w, (m.row, m.col)), shape=m.shape)
+    conn = SparseConn(W, sparse_backend="native")
+    n_rec = len(idx)
+    taus = np.array([5.0, 3.0, 10.0, 2.5][:n_rec], np.float32)
+    syn = HeterSynapsePSC(n, n_rec, idx, conn, base_psc=ExponentialPSC, max_delay_steps=D,
+                          use_circular_buffer=True, tau_syn=torch.tensor(np.tile(taus, n)))
+    neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=2.0, hard_reset=True)
+    x = (np.round(rng.poisson(0.08, size=(steps, batch, n)) * 0.75 * 64) / 64).astype(np.float32)
+    _, z, st, _ = _run_rnn(neuron, syn, None, x, batch, ("neuron.v", "synapse.psc", "synapse.base_psc.psc"))
+    post, src, wc = canonical(W)
+    out = dict(n=n, batch=batch, n_rec=n_rec, n_bins=D, taus=taus, post=post, src=src, w=wc, x=x,
+               z=np.packbits(z.astype(np.uint8), axis=-1, bitorder="little"), v=st["neuron.v"],
+               psc=st["synapse.psc"], psc_rec=st["synapse.base_psc.psc"])
+    for c in neu.columns:
+        out[f"neurons.{c}"] = neu[c].to_numpy().astype(str if c == "EI" else np.int64)
+    for c in con.columns:
+        out[f"conns.{c}"] = con[c].to_numpy().astype(str if c == "nt" else np.int64)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -431,6 +552,8 @@ def main():
                                        in_gain=GAIN["c1"]),
         "constrained_spmm": lambda r: case_constrained(r),
         "receptors2": lambda r: case_receptors(r, n=200, p=0.03, batch=3, steps=100, n_rec=2),
+        "connectome_format": lambda r: case_connectome_format(r),
+        "receptors_delay": lambda r: case_receptors_delay(r, n=300, n_conn=9000, batch=3, steps=120, D=5),
     }
     only = set(args.only.split(",")) if args.only else None
     for i, (name, fn) in enumerate(cases.items()):
