@@ -26,7 +26,7 @@ _i64 = C.c_int64
 _i32 = C.c_int32
 
 
-ABI_VERSION = 6  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
+ABI_VERSION = 7  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
 
 
 class BtParam(C.Structure):
@@ -59,7 +59,7 @@ class BtEngineDesc(C.Structure):
         ("pull_words_per_warp", _i32), ("neuron_spt", _i32),
         ("work", _vp), ("stats", _vp), ("dense_rows", _i64),
         ("psc_uniform", _i32), ("psc_coef_s", C.c_float), ("psc_tau_s", C.c_float), ("psc_fast_div", _i32),
-        ("psc_rcp", C.c_float), ("pad5_", _i32), ("csr_edges", _vp),
+        ("psc_rcp", C.c_float), ("n_rec", _i32), ("csr_edges", _vp),
     ]
 
 

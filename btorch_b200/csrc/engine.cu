@@ -33,6 +33,13 @@
 //   ascending canonical order of w * z_{t-1-bin}[pre] (fmaf chain, exactly the
 //   reference's CPU rounding), then runs the neuron update of step t.  The
 //   last synapse update of a run is k_eng_gather_final.
+//
+// RECEPTOR CHANNELS (HeterSynapsePSC with n_receptor = C > 1,
+// synapse.py:626-847): the matrix has C columns per neuron (post * C + r, the
+// layout make_hetersynapse_conn builds, connection.py:218-587); PSC state,
+// acc and the PSC coefficients are [batch][n * C], and the neuron's input is
+// the receptor sum of its C channels (receptor_sum, the reference's
+// psc.reshape(..., n, C).sum(-1) rounding).  Scatter and gather modes.
 #include <algorithm>
 #include <type_traits>
 
@@ -41,6 +48,61 @@
 namespace bt {
 
 constexpr int kEngThreads = 256;
+constexpr int kMaxRec = 16;  // receptor channels per neuron
+
+// Receptor columns per neuron (0 in the descriptor means 1).
+__host__ __device__ __forceinline__ int n_rec(const bt_engine_desc& d) { return d.n_rec > 1 ? d.n_rec : 1; }
+
+// Sum of one neuron's C receptor PSCs p[0..C) in the order torch's CPU sum
+// reduces a contiguous row of C floats, which the reference runs as
+// psc.reshape(..., n, C).sum(-1) (synapse.py:744-747):
+//   C < 4       left to right;
+//   4 <= C < 8  a_j = p_j (j < 4), p_4 .. p_{C-1} added to a_0 in turn, then
+//               ((a_0 + a_1) + a_2) + a_3;
+//   C >= 8      a_j = p_j + p_{8+j} + ... over the whole groups of 8, the
+//               left-to-right sum of the remaining tail added to a_0, then
+//               a_0 + a_1 + ... + a_7 left to right.
+// (Established against torch.sum for every C up to 39; the host mirror in
+// btorch_b200/models/synapse.py is checked against torch.sum in the CPU
+// tests.)  Indices are compile-time after unrolling.
+__device__ __forceinline__ float receptor_sum(const float (&p)[kMaxRec], int C) {
+  if (C < 4) {
+    float s = p[0];
+#pragma unroll
+    for (int r = 1; r < 4; ++r)
+      if (r < C) s = add(s, p[r]);
+    return s;
+  }
+  if (C < 8) {
+    float a0 = p[0];
+#pragma unroll
+    for (int r = 4; r < 8; ++r)
+      if (r < C) a0 = add(a0, p[r]);
+    return add(add(add(a0, p[1]), p[2]), p[3]);
+  }
+  const int full = C & ~7;
+  float a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = p[j];
+#pragma unroll
+  for (int r = 8; r < kMaxRec; ++r)
+    if (r < full) a[r & 7] = add(a[r & 7], p[r]);
+  if (full < C) {
+    float t = 0.0f;
+    bool first = true;
+#pragma unroll
+    for (int r = 8; r < kMaxRec; ++r)
+      if (r >= full && r < C) {
+        t = first ? p[r] : add(t, p[r]);
+        first = false;
+      }
+    a[0] = add(a[0], t);
+  }
+  float s = a[0];
+#pragma unroll
+  for (int j = 1; j < 8; ++j) s = add(s, a[j]);
+  return s;
+}
 
 __host__ __device__ __forceinline__ int mask_words(int64_t batch) { return int((batch + 31) >> 5); }
 
@@ -125,6 +187,36 @@ __device__ __forceinline__ ScatterScratch scatter_scratch(const bt_engine_desc& 
   w.mask = reinterpret_cast<uint32_t*>(d.work + Q * 2 * kSub + Q * n + Q * kSub * w.cap) + int64_t(q) * n * w.ms;
   w.ctrl = d.work + Q * (2 * kSub + n + kSub * w.cap + n * w.ms);
   return w;
+}
+
+// Publish neuron i's spikes of step t in the step's spike set (bit u of
+// `spiked`: sample b0 + u): the samples' bits in the neuron's mask, and the
+// neuron in the compacted list if this warp's samples are the first to spike
+// (one warp-aggregated atomic on one of kSub counters).  Called by every lane
+// of the warp.
+template <int S>
+__device__ __forceinline__ void publish_spikes(const bt_engine_desc& d, const StepIdx& si, int64_t i, int64_t b0,
+                                               uint32_t spiked) {
+  if (__ballot_sync(0xffffffffu, spiked != 0) == 0) return;  // warp-uniform
+  const unsigned lane = lane_id();
+  const ScatterScratch ws = scatter_scratch(d, si.q_t);
+  bool first = false;
+  if (spiked) {
+    uint32_t* mrow = ws.mask + i * ws.ms;
+#pragma unroll
+    for (int u = 0; u < S; ++u)
+      if (spiked & (1u << u)) atomicOr(mrow + ((b0 + u) >> 5), 1u << ((b0 + u) & 31));
+    first = atomicOr(ws.flag + i, 1) == 0;
+  }
+  const uint32_t fb = __ballot_sync(0xffffffffu, first);
+  const int sub = int((i - lane) >> ws.cap_shift);  // same for the whole warp (cap % 32 == 0)
+  const int nspk = __reduce_add_sync(0xffffffffu, unsigned(__popc(spiked)));
+  if (lane == 0 && nspk) atomicAdd(ws.spk + sub, nspk);
+  if (fb == 0) return;
+  int32_t base = 0;
+  if (lane == 0) base = atomicAdd(ws.count + sub, __popc(fb));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (first) ws.list[sub * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = int32_t(i);
 }
 
 // Grid (ceil(n / 256), ceil(batch / S)): a thread owns neuron i for S
@@ -217,27 +309,68 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
     }
     if (s != 0.0f) spiked |= 1u << u;
   }
-  if (__ballot_sync(0xffffffffu, spiked != 0) == 0) return;  // warp-uniform
-  // Publish the samples' bits in the neuron's mask; the first sample to spike
-  // lists the neuron (one atomic per warp on one of kSub counters).
-  const ScatterScratch ws = scatter_scratch(d, si.q_t);
-  bool first = false;
-  if (spiked) {
-    uint32_t* mrow = ws.mask + i * ws.ms;
-#pragma unroll
-    for (int u = 0; u < S; ++u)
-      if (spiked & (1u << u)) atomicOr(mrow + ((b0 + u) >> 5), 1u << ((b0 + u) & 31));
-    first = atomicOr(ws.flag + i, 1) == 0;
+  publish_spikes<S>(d, si, i, b0, spiked);
+}
+
+// SCATTER neuron step with receptor channels (n_rec = C > 1): for each
+// channel column c = i * C + r, P_r = stored + acc (acc zeroed); the neuron's
+// input is receptor_sum(P) (+ x); stored = decay_r(P_r).  Grid
+// (ceil(n / 256), batch): a thread owns (neuron i, sample b).
+template <int KIND, bool HARD, bool USE_REF>
+__global__ void __launch_bounds__(kEngThreads) k_eng_neuron_rec(bt_engine_desc d, int64_t k, StepIdx si) {
+  const int64_t n = d.n, B = d.batch;
+  const int C = n_rec(d);
+  const int64_t nc = n * C;
+  const int64_t words = (n + 31) >> 5;
+  const int64_t i = int64_t(blockIdx.x) * kEngThreads + threadIdx.x;
+  const int64_t b = blockIdx.y;
+  if ((i & ~int64_t(31)) >= n) return;  // whole warps past the last word
+  float s = 0.0f;
+  if (i < n) {
+    const int64_t idx = b * n + i, c0 = b * nc + i * C;
+    const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
+    float P[kMaxRec];
+    for (int r = 0; r < C; ++r) {
+      const float pend = d.ring[c0 + r];
+      d.ring[c0 + r] = 0.0f;
+      // past a sample's end: the first step completes psc of its last step,
+      // later arrivals are dropped (as k_eng_neuron)
+      P[r] = k <= len ? add(d.psc[c0 + r], pend) : d.psc[c0 + r];
+      if (k == len) d.psc[c0 + r] = P[r];
+    }
+    float v = d.v[idx];
+    float ref = USE_REF ? d.refractory[idx] : 0.0f;
+    float gk = KIND == BT_NEURON_ALIF ? d.g_k[idx] : 0.0f;
+    if (k < len) {
+      float I = receptor_sum(P, C);
+      if (d.x) I = add(I, d.x[(k * B) * n + idx]);
+      const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, i);
+      const NeuronOut out = neuron_update<KIND, HARD, USE_REF, true>(prm, I, v, ref, gk);
+      s = out.spike;
+      d.v[idx] = v;
+      if (USE_REF) d.refractory[idx] = ref;
+      if (KIND == BT_NEURON_ALIF) d.g_k[idx] = gk;
+      for (int r = 0; r < C; ++r) {
+        const int64_t col = i * C + r;
+        const float pc = d.psc_uniform ? d.psc_coef_s : ld(d.psc_coef, col);
+        const float pt = d.psc_uniform ? d.psc_tau_s : ld(d.psc_tau, col);
+        d.psc[c0 + r] = psc_decay(pc, make_div(pt, d.psc_uniform && d.psc_fast_div, d.psc_rcp), P[r]);
+      }
+    }
+    if (d.psc_trace && k > 0)
+      for (int r = 0; r < C; ++r) d.psc_trace[((k - 1) * B) * nc + c0 + r] = P[r];
+    const int64_t tix = (k * B) * n + idx;
+    if (d.v_trace) d.v_trace[tix] = v;
+    if (USE_REF && d.ref_trace) d.ref_trace[tix] = ref;
+    if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[tix] = gk;
+    if (d.spikes) d.spikes[tix] = s;
   }
-  const uint32_t fb = __ballot_sync(0xffffffffu, first);
-  const int sub = int((i - lane) >> ws.cap_shift);  // same for the whole warp (cap % 32 == 0)
-  const int nspk = __reduce_add_sync(0xffffffffu, unsigned(__popc(spiked)));
-  if (lane == 0 && nspk) atomicAdd(ws.spk + sub, nspk);
-  if (fb == 0) return;
-  int32_t base = 0;
-  if (lane == 0) base = atomicAdd(ws.count + sub, __popc(fb));
-  base = __shfl_sync(0xffffffffu, base, 0);
-  if (first) ws.list[sub * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = int32_t(i);
+  const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
+  if (lane_id() == 0) {
+    d.hist[(int64_t(si.h_t) * B + b) * words + (i >> 5)] = word;
+    if (d.raster) d.raster[(k * B + b) * words + (i >> 5)] = word;
+  }
+  publish_spikes<1>(d, si, i, b, s != 0.0f ? 1u : 0u);
 }
 
 // Offsets of the kSub sub-lists of one spike set in shared memory (warp 0
@@ -318,8 +451,9 @@ __device__ void scatter_dense(const bt_engine_desc& d, int64_t k, const ScatterS
   __shared__ float s_acc[W][32][32];
   const int lane = int(lane_id()), wid = int(threadIdx.x >> 5);
   const int64_t n = d.n, B = d.batch;
-  const int n32 = int(n);
-  const int64_t n_slices = (n + 31) >> 5;
+  const int64_t nc = n * n_rec(d);  // acc columns (post * C + r)
+  const int n32 = int(nc);
+  const int64_t n_slices = (nc + 31) >> 5;
   const int64_t nblocks = int64_t(gridDim.x) * gridDim.y;
   const int64_t bid = int64_t(blockIdx.y) * gridDim.x + blockIdx.x;
   float(*acc)[32] = s_acc[wid];
@@ -369,7 +503,7 @@ __device__ void scatter_dense(const bt_engine_desc& d, int64_t k, const ScatterS
 #pragma unroll
         for (int v = 0; v < W; ++v) sum = add(sum, s_acc[v][l][ln]);
         const int64_t b = int64_t(w) * 32 + l, p = sl * 32 + ln;
-        if (b < B && p < n && sum != 0.0f) d.ring[b * n32 + p] = sum;
+        if (b < B && p < nc && sum != 0.0f) d.ring[b * n32 + p] = sum;
       }
       __syncthreads();
     }
@@ -396,8 +530,11 @@ __device__ void scatter_dense(const bt_engine_desc& d, int64_t k, const ScatterS
 // lane loading 4 edges with one 128-bit load of posts and one of weights, then
 // adding them for every sample in the row's mask (MS words; the sample loop is
 // outside the edge loop, so a lane issues 4 reductions per mask bit).
+// Launch bounds: at least 4 (MS <= 4) or 3 resident blocks per SM, which
+// leaves ptxas 64 / 85 registers -- without a bound its occupancy heuristic
+// has settled on 48 registers and spilled the reduction loop.
 template <int G, int MS>
-__global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, int64_t k, StepIdx si) {
+__global__ void __launch_bounds__(kEngThreads, MS <= 4 ? 4 : 3) k_eng_scatter(bt_engine_desc d, int64_t k, StepIdx si) {
   const int64_t n = d.n;
   const int R = d.n_bins, Q = R + 1;
   const int bin = d.bin_lo + int(blockIdx.y);
@@ -429,7 +566,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, i
   const int grp = int(lane) / G, lig = int(lane) % G;
   constexpr int kPerWarp = 32 / G;
   const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  const int n32 = int(n);  // batch * n < 2^31 (checked on the host)
+  const int n32 = int(n * n_rec(d));  // acc row stride; batch * n * C < 2^31 (checked on the host)
   const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
   long long ev = 0, ed = 0;
   for (int64_t base = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kPerWarp; base < count;
@@ -519,7 +656,8 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter(bt_engine_desc d, i
 // lanes' exclusive offsets (shuffles), so no lane idles on a short row and
 // consecutive lanes load consecutive edges.  Grid as k_eng_scatter.
 template <int MS>
-__global__ void __launch_bounds__(kEngThreads) k_eng_scatter_flat(bt_engine_desc d, int64_t k, StepIdx si) {
+__global__ void __launch_bounds__(kEngThreads, MS <= 4 ? 4 : 3) k_eng_scatter_flat(bt_engine_desc d, int64_t k,
+                                                                              StepIdx si) {
   const int R = d.n_bins, Q = R + 1;
   const int bin = d.bin_lo + int(blockIdx.y);
   int q = si.q_t - bin;
@@ -546,7 +684,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter_flat(bt_engine_desc
   const bool last_use = bin == d.bin_hi;
   const int lane = int(lane_id());
   const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  const int n32 = int(d.n);  // batch * n < 2^31 (checked on the host)
+  const int n32 = int(d.n * n_rec(d));  // acc row stride; batch * n * C < 2^31 (checked on the host)
   const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
   long long ev = 0, ed = 0;
   for (int64_t base = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * 32; base < count;
@@ -641,18 +779,18 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_scatter_flat(bt_engine_desc
 // psc_{t_end-1} = stored + acc; clears acc.
 __global__ void k_eng_scatter_final(bt_engine_desc d) {
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int64_t n = d.n, B = d.batch;
-  if (idx >= B * n) return;
+  const int64_t nc = d.n * n_rec(d), B = d.batch;  // one thread per PSC column
+  if (idx >= B * nc) return;
   const float pending = d.ring[idx];
   d.ring[idx] = 0.0f;
-  const int64_t b = idx / n;
+  const int64_t b = idx / nc;
   const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
   if (d.n_steps - 1 < len) {
     const float P = add(d.psc[idx], pending);
     d.psc[idx] = P;
-    if (d.psc_trace) d.psc_trace[((d.n_steps - 1) * B) * n + idx] = P;
+    if (d.psc_trace) d.psc_trace[((d.n_steps - 1) * B) * nc + idx] = P;
   } else if (d.psc_trace) {
-    d.psc_trace[((d.n_steps - 1) * B) * n + idx] = d.psc[idx];
+    d.psc_trace[((d.n_steps - 1) * B) * nc + idx] = d.psc[idx];
   }
 }
 
@@ -690,7 +828,8 @@ __device__ __forceinline__ float gather_in(const bt_engine_desc& d, int64_t i, i
 
 // One launch per step.  Block = 32 warps = 32 consecutive neurons, so each
 // (sample, 32-neuron word) of the spike bitmap is written by one thread.
-template <int KIND, bool HARD, bool USE_REF>
+// REC: receptor channels, the warp gathers the C columns i * C + r in turn.
+template <int KIND, bool HARD, bool USE_REF, bool REC>
 __global__ void __launch_bounds__(1024) k_eng_gather(bt_engine_desc d, int64_t k, StepIdx si) {
   extern __shared__ uint32_t sbits[];  // [batch]
   const int64_t n = d.n, B = d.batch;
@@ -707,10 +846,21 @@ __global__ void __launch_bounds__(1024) k_eng_gather(bt_engine_desc d, int64_t k
       const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
       // synapse update of step t-1 (skipped on the first step of a call: the
       // stored psc already is psc_{t0-1}; skipped after a sample's last step)
-      float P = d.psc[idx];
-      if (k > 0 && k - 1 < len) {
-        const float wz = gather_in(d, i, b, si.h_prev, words);
-        P = add(psc_decay(d.psc_coef, d.psc_tau, i, P), wz);
+      const bool syn = k > 0 && k - 1 < len;
+      float P;
+      float Pr[REC ? kMaxRec : 1];
+      const int C = REC ? d.n_rec : 1;
+      const int64_t c0 = (b * n + i) * C;  // first PSC column of (b, i)
+      if constexpr (!REC) {
+        P = d.psc[idx];
+        if (syn) P = add(psc_decay(d.psc_coef, d.psc_tau, i, P), gather_in(d, i, b, si.h_prev, words));
+      } else {
+        for (int r = 0; r < C; ++r) {
+          float q = d.psc[c0 + r];
+          if (syn) q = add(psc_decay(d.psc_coef, d.psc_tau, i * C + r, q), gather_in(d, i * C + r, b, si.h_prev, words));
+          Pr[r] = q;
+        }
+        P = receptor_sum(Pr, C);
       }
       float s = 0.0f;
       if (lane == 0) {
@@ -726,11 +876,18 @@ __global__ void __launch_bounds__(1024) k_eng_gather(bt_engine_desc d, int64_t k
           if (USE_REF) d.refractory[idx] = ref;
           if (KIND == BT_NEURON_ALIF) d.g_k[idx] = gk;
         }
-        d.psc[idx] = P;
+        if constexpr (!REC) {
+          d.psc[idx] = P;
+          if (d.psc_trace && k > 0) d.psc_trace[((k - 1) * B) * n + idx] = P;
+        } else {
+          for (int r = 0; r < C; ++r) {
+            d.psc[c0 + r] = Pr[r];
+            if (d.psc_trace && k > 0) d.psc_trace[((k - 1) * B) * n * C + c0 + r] = Pr[r];
+          }
+        }
         if (d.v_trace) d.v_trace[(k * B) * n + idx] = d.v[idx];
         if (USE_REF && d.ref_trace) d.ref_trace[(k * B) * n + idx] = d.refractory[idx];
         if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[(k * B) * n + idx] = d.g_k[idx];
-        if (d.psc_trace && k > 0) d.psc_trace[((k - 1) * B) * n + idx] = P;
         if (d.spikes) d.spikes[(k * B) * n + idx] = s;
         if (s != 0.0f) {
           atomicOr(&sbits[b], 1u << (i & 31));
@@ -767,18 +924,22 @@ __global__ void __launch_bounds__(1024) k_eng_gather_final(bt_engine_desc d, Ste
   const int64_t k = d.n_steps - 1;
   const int64_t i = int64_t(blockIdx.x) * 32 + (threadIdx.x >> 5);
   if (i >= n) return;
+  const int C = n_rec(d);
+  const int64_t nc = n * C;
   for (int64_t b = 0; b < B; ++b) {
-    const int64_t idx = b * n + i;
     const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
-    if (k >= len) {
-      if (lane_id() == 0 && d.psc_trace) d.psc_trace[(k * B) * n + idx] = d.psc[idx];
-      continue;
-    }
-    const float wz = gather_in(d, i, b, si.h_t, words);
-    if (lane_id() == 0) {
-      const float P = add(psc_decay(d.psc_coef, d.psc_tau, i, d.psc[idx]), wz);
-      d.psc[idx] = P;
-      if (d.psc_trace) d.psc_trace[(k * B) * n + idx] = P;
+    for (int r = 0; r < C; ++r) {
+      const int64_t col = i * C + r, idx = b * nc + col;  // PSC column
+      if (k >= len) {
+        if (lane_id() == 0 && d.psc_trace) d.psc_trace[(k * B) * nc + idx] = d.psc[idx];
+        continue;
+      }
+      const float wz = gather_in(d, col, b, si.h_t, words);
+      if (lane_id() == 0) {
+        const float P = add(psc_decay(d.psc_coef, d.psc_tau, col, d.psc[idx]), wz);
+        d.psc[idx] = P;
+        if (d.psc_trace) d.psc_trace[(k * B) * nc + idx] = P;
+      }
     }
   }
 }
@@ -1143,6 +1304,9 @@ int engine_check(const bt_engine_desc* d) {
   BT_CHECK_ARG(d->neuron.kind != BT_NEURON_ALIF || d->g_k, "g_k state missing");
   BT_CHECK_ARG(d->psc_coef.ptr && d->psc_tau.ptr, "PSC coefficients missing");
   BT_CHECK_ARG(d->neuron.spiking, "the fused engine needs a spiking (Heaviside) forward");
+  BT_CHECK_ARG(d->n_rec >= 0 && d->n_rec <= kMaxRec, "n_rec=%d outside [0, %d]", d->n_rec, kMaxRec);
+  BT_CHECK_ARG(d->n * n_rec(*d) < BT_MAX_NEURONS, "n * n_rec must be < 2^25");
+  BT_CHECK_ARG(n_rec(*d) == 1 || d->mode != BT_MODE_PULL, "pull mode has no receptor channels");
   if (d->mode == BT_MODE_SCATTER) {
     BT_CHECK_ARG(d->csr_ptr && d->csr_edges && d->ring && d->work, "scatter needs CSR, ring and work");
     BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->csr_edges) & 15) == 0, "csr_edges must be 16-byte aligned");
@@ -1151,7 +1315,7 @@ int engine_check(const bt_engine_desc* d) {
     BT_CHECK_ARG(d->scatter_lanes == 0 || d->scatter_lanes == 1 || d->scatter_lanes == 8 || d->scatter_lanes == 32,
                  "scatter_lanes=%d (0, 1, 8 or 32)", d->scatter_lanes);
     BT_CHECK_ARG(mask_stride(d->batch) <= 8, "scatter mode supports up to 256 samples");
-    BT_CHECK_ARG(d->batch * d->n < (int64_t(1) << 31), "scatter mode needs batch * n < 2^31");
+    BT_CHECK_ARG(d->batch * d->n * n_rec(*d) < (int64_t(1) << 31), "scatter mode needs batch * n * n_rec < 2^31");
     BT_CHECK_ARG(d->dense_rows == 0 || (d->bin_lo == d->bin_hi && d->sl_ptr && d->sl_src && d->sl_w),
                  "dense delivery needs a single delay bin and the sliced in-edge view");
     BT_CHECK_ARG(d->neuron_spt == 0 || d->neuron_spt == 1 || d->neuron_spt == 2 || d->neuron_spt == 4,
@@ -1193,14 +1357,17 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
                                              : ms <= 4 ? k_eng_scatter_flat<4> : k_eng_scatter_flat<8>)
                    : d.scatter_lanes == 8 ? pick(std::integral_constant<int, 8>())
                                           : pick(std::integral_constant<int, 32>());
+    const int C = n_rec(d);
+    const dim3 rgrid(unsigned(ceil_div(n, kEngThreads)), unsigned(d.batch));
     for (int64_t k = 0; k < d.n_steps; ++k) {
       const StepIdx si = step_idx(d.t0 + k, d.n_bins, d.hist_len);
-      neuron<<<grid, kEngThreads, 0, s>>>(d, k, si);
+      if (C > 1) k_eng_neuron_rec<KIND, HARD, USE_REF><<<rgrid, kEngThreads, 0, s>>>(d, k, si);
+      else neuron<<<grid, kEngThreads, 0, s>>>(d, k, si);
       scatter<<<sgrid, kEngThreads, 0, s>>>(d, k, si);
     }
     BT_CHECK_LAUNCH("k_eng_neuron/k_eng_scatter");
     if (d.n_steps > 0) {
-      k_eng_scatter_final<<<int(ceil_div(d.batch * n, 256)), 256, 0, s>>>(d);
+      k_eng_scatter_final<<<int(ceil_div(d.batch * n * C, 256)), 256, 0, s>>>(d);
       BT_CHECK_LAUNCH("k_eng_scatter_final");
     }
   } else if (d.mode == BT_MODE_PULL) {
@@ -1239,8 +1406,9 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
     const int grid = int(ceil_div(n, 32));
     const size_t smem = sizeof(uint32_t) * size_t(d.batch);
     BT_CHECK_ARG(smem <= 48 * 1024, "batch too large for the gather engine");
+    auto gather = n_rec(d) > 1 ? k_eng_gather<KIND, HARD, USE_REF, true> : k_eng_gather<KIND, HARD, USE_REF, false>;
     for (int64_t k = 0; k < d.n_steps; ++k)
-      k_eng_gather<KIND, HARD, USE_REF><<<grid, 1024, smem, s>>>(d, k, step_idx(d.t0 + k, d.n_bins, d.hist_len));
+      gather<<<grid, 1024, smem, s>>>(d, k, step_idx(d.t0 + k, d.n_bins, d.hist_len));
     BT_CHECK_LAUNCH("k_eng_gather");
     if (d.n_steps > 0) {
       k_eng_gather_final<<<grid, 1024, 0, s>>>(d, step_idx(d.t0 + d.n_steps - 1, d.n_bins, d.hist_len));
@@ -1279,7 +1447,7 @@ extern "C" int bt_engine_prime(const bt_engine_desc* d, void* stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const size_t words = size_t(scatter_work_words(d->n, d->batch, d->n_bins));
   if (cudaMemsetAsync(d->work, 0, sizeof(int32_t) * words, s) != cudaSuccess ||
-      cudaMemsetAsync(d->ring, 0, sizeof(float) * size_t(d->batch * d->n), s) != cudaSuccess)
+      cudaMemsetAsync(d->ring, 0, sizeof(float) * size_t(d->batch * d->n * n_rec(*d)), s) != cudaSuccess)
     return bt_set_error(BT_ERR_CUDA, "memset failed");
   if (d->bin_hi > 0) {
     const int64_t npad = ((d->n + 31) >> 5) * 32;

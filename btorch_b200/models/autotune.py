@@ -48,30 +48,37 @@ class EngineChoice:
                 "pull_words": self.pull_words, "dense_rows": self.dense_rows}
 
 
-def allowed_modes(conn, batch: int) -> list[int]:
+def allowed_modes(conn, batch: int, receptors: int = 1) -> list[int]:
+    """Delivery modes the sparse config admits (the sliced pull has no
+    receptor channels: with receptors > 1 it is left out)."""
     cfg = conn.sparse_config
     if cfg.deterministic or cfg.direction == "gather":
-        return [L.BT_MODE_GATHER, L.BT_MODE_PULL]
-    if cfg.direction == "scatter":
-        return [L.BT_MODE_SCATTER]
-    return [L.BT_MODE_SCATTER, L.BT_MODE_PULL, L.BT_MODE_GATHER]
+        modes = [L.BT_MODE_GATHER, L.BT_MODE_PULL]
+    elif cfg.direction == "scatter":
+        modes = [L.BT_MODE_SCATTER]
+    else:
+        modes = [L.BT_MODE_SCATTER, L.BT_MODE_PULL, L.BT_MODE_GATHER]
+    return [m for m in modes if receptors == 1 or m != L.BT_MODE_PULL]
 
 
-def heuristic(conn, batch: int) -> EngineChoice:
+def heuristic(conn, batch: int, receptors: int = 1) -> EngineChoice:
     """The untuned choice: the configured direction (gather -> warp per neuron
-    below `pull_min_batch` samples, sliced pull above), default tiles."""
+    below `pull_min_batch` samples, sliced pull above; always warp per neuron
+    with receptor channels), default tiles."""
     direction = conn.direction(batch)
     if direction == "gather":
-        mode = L.BT_MODE_PULL if batch >= conn.sparse_config.pull_min_batch else L.BT_MODE_GATHER
+        pull = batch >= conn.sparse_config.pull_min_batch and receptors == 1
+        mode = L.BT_MODE_PULL if pull else L.BT_MODE_GATHER
     else:
         mode = L.BT_MODE_SCATTER
     return EngineChoice(mode)
 
 
-def candidates(conn, batch: int) -> list[EngineChoice]:
+def candidates(conn, batch: int, receptors: int = 1) -> list[EngineChoice]:
     out = []
     mw = L.lib().bt_mask_stride(batch)
-    for mode in allowed_modes(conn, batch):
+    modes = allowed_modes(conn, batch, receptors)
+    for mode in modes:
         if mode == L.BT_MODE_SCATTER:
             for spt in (1, 2, 4):
                 if spt > 1 and spt > batch:
@@ -81,7 +88,7 @@ def candidates(conn, batch: int) -> list[EngineChoice]:
         elif mode == L.BT_MODE_PULL:
             for words in sorted({1, mw} if mw in (2, 4) else {1}):
                 out.append(EngineChoice(mode, pull_words=words))
-        elif batch <= 32:  # a warp per neuron walks the samples serially
+        elif batch <= 32 or modes == [L.BT_MODE_GATHER]:  # a warp per neuron walks the samples serially
             out.append(EngineChoice(mode))
     return out
 
@@ -89,8 +96,8 @@ def candidates(conn, batch: int) -> list[EngineChoice]:
 def _key(plan, batch: int, c_in: int) -> tuple:
     conn = plan.conn
     return (torch.cuda.get_device_name(plan.neuron.v.device), plan.neuron.size, batch, plan.n_bins,
-            plan.uniform_delay, int(conn.indices.shape[1]), c_in, type(plan.neuron).__name__,
-            tuple(allowed_modes(conn, batch)))
+            plan.uniform_delay, int(conn.indices.shape[1]), c_in, type(plan.neuron).__name__, plan.n_rec,
+            tuple(allowed_modes(conn, batch, plan.n_rec)))
 
 
 def tuned(rnn) -> dict:
@@ -108,8 +115,8 @@ def choose(plan, rnn, x: torch.Tensor, sample_len, run) -> EngineChoice:
     if key in cache:
         return cache[key][0]
     if not plan.conn.sparse_config.autotune or T < TUNE_MIN_STEPS:
-        return heuristic(plan.conn, B)
-    cands = candidates(plan.conn, B)
+        return heuristic(plan.conn, B, plan.n_rec)
+    cands = candidates(plan.conn, B, plan.n_rec)
     if len(cands) == 1:
         cache[key] = (cands[0], {})
         return cands[0]

@@ -1,8 +1,9 @@
 """Fused multi-step engine behind RecurrentNN.multi_step_forward.
 
 A RecurrentNN whose neuron is LIF/ALIF, whose synapse is ExponentialPSC,
-DelayedPSC(ExponentialPSC) or HeterSynapsePSC(n_receptor=1, ExponentialPSC)
-over a SparseConn, and whose input module is absent or a DenseConn/nn.Linear
+DelayedPSC(ExponentialPSC) or HeterSynapsePSC(ExponentialPSC, up to
+MAX_RECEPTORS receptor channels) over a SparseConn, and whose input module is
+absent or a DenseConn/nn.Linear
 runs through ``bt_engine_run``: the whole time loop on the device, one or two
 kernel launches per step (btorch_b200/csrc/engine.cu), with the reference's
 outputs (spike stack and requested state stacks) and final state.
@@ -28,11 +29,12 @@ from .history import SpikeHistory
 from .linear import BaseSparseConn
 from .neurons.alif import ALIF
 from .neurons.lif import LIF
-from .synapse import DelayedPSC, ExponentialPSC, HeterSynapsePSC
+from .synapse import DelayedPSC, ExponentialPSC, HeterSynapsePSC, receptor_sum
 
 DEFAULT_CHUNK = 512
 DENSE_FRACTION = 4  # scatter steps with at least n / DENSE_FRACTION spiking neurons are pulled densely
 DEFAULT_GRAPH_CHUNK = 128  # steps per captured chunk (rounded to a multiple of the slot period)
+MAX_RECEPTORS = 16  # receptor channels per neuron the kernels take (bt_engine_desc.n_rec)
 
 
 @dataclass
@@ -47,6 +49,7 @@ class EnginePlan:
     top_syn: nn.Module             # RecurrentNN.synapse
     hetero: bool
     paths: dict                    # state key -> trace kind
+    n_rec: int = 1                 # receptor channels (HeterSynapsePSC.n_receptor)
 
 
 def _module_path(root: nn.Module, target: nn.Module) -> str | None:
@@ -71,6 +74,7 @@ def match(rnn) -> tuple[EnginePlan | None, str]:
     history = None
     uniform = 0
     n_bins = 1
+    n_rec = 1
     if type(syn) is ExponentialPSC:
         psc_mod = syn
     elif type(syn) is DelayedPSC and type(syn.psc_module) is ExponentialPSC:
@@ -79,9 +83,12 @@ def match(rnn) -> tuple[EnginePlan | None, str]:
             uniform = syn.max_delay_steps
             n_bins = uniform + 1
             history = syn.history
-    elif type(syn) is HeterSynapsePSC and type(syn.base_psc) is ExponentialPSC and syn.n_receptor == 1:
+    elif type(syn) is HeterSynapsePSC and type(syn.base_psc) is ExponentialPSC:
+        if syn.n_receptor > MAX_RECEPTORS:
+            return None, f"more than {MAX_RECEPTORS} receptor channels"
         psc_mod = syn.base_psc
         hetero = True
+        n_rec = syn.n_receptor
         if syn.max_delay_steps > 1:
             n_bins = syn.max_delay_steps
             history = syn.history
@@ -93,7 +100,7 @@ def match(rnn) -> tuple[EnginePlan | None, str]:
     if conn.bias is not None:
         return None, "SparseConn bias"
     n = neuron.size
-    if conn.out_features != n or conn.in_features != n * (n_bins if hetero else 1):
+    if conn.out_features != n * n_rec or conn.in_features != n * (n_bins if hetero else 1):
         return None, "connectivity shape does not match the neuron count"
     if n_bins > L.BT_MAX_BINS:
         return None, "too many delay bins"
@@ -114,14 +121,16 @@ def match(rnn) -> tuple[EnginePlan | None, str]:
             paths[key] = "ref"
         elif key == f"{npath}.g_k":
             paths[key] = "gk"
-        elif key in (f"{ppath}.psc", f"{spath}.psc"):
+        elif key == f"{ppath}.psc" or (key == f"{spath}.psc" and n_rec == 1):
             paths[key] = "psc"
+        elif key == f"{spath}.psc":
+            paths[key] = "psc_sum"  # receptor sum of the base PSC trace
         elif hpath is not None and key == f"{hpath}.history":
             paths[key] = "history"
         else:
             return None, f"state '{key}' is not traced by the fused engine"
     plan = EnginePlan(neuron=neuron, psc_mod=psc_mod, conn=conn, inp=inp, n_bins=n_bins, uniform_delay=uniform,
-                      history=history, top_syn=syn, hetero=hetero, paths=paths)
+                      history=history, top_syn=syn, hetero=hetero, paths=paths, n_rec=n_rec)
     return plan, ""
 
 
@@ -219,13 +228,15 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     batch_shape = neuron.v.shape[:-1] if neuron.v.ndim > 1 else ()
     ref_mod = _state2d(neuron.refractory, n) if neuron._use_refractory else None
     gk_mod = _state2d(neuron.g_k, n) if isinstance(neuron, ALIF) else None
-    psc_mod_t = _state2d(psc_mod.psc, n)
+    n_rec = plan.n_rec
+    nc = n * n_rec  # PSC columns (post * n_rec + receptor)
+    psc_mod_t = _state2d(psc_mod.psc, nc)
     T = int(x.shape[0])
     words = (n + 31) // 32
     R = plan.n_bins
     inp = plan.inp
     c_in = int(x.shape[-1]) if inp is not None else n
-    trace_kinds = sorted(k for k in set(plan.paths.values()) if k != "history")
+    trace_kinds = sorted({"psc" if k == "psc_sum" else k for k in plan.paths.values()} - {"history"})
 
     if choice is None:
         choice = _autotune.choose(plan, rnn, x, sample_len, run)
@@ -277,7 +288,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     lay = conn.engine_layout(R, plan.uniform_delay, dev)
     w = static("w", conn._get_effective_weight().detach().float().contiguous())
     keep.append(w)
-    desc.n, desc.batch, desc.n_bins = n, B, R
+    desc.n, desc.batch, desc.n_bins, desc.n_rec = n, B, R, n_rec
     desc.hist_len = H
     desc.csc_ptr, desc.csc_src, desc.csc_w = lay.csc_ptr.data_ptr(), lay.csc_src.data_ptr(), w.data_ptr()
     if mode == L.BT_MODE_SCATTER:
@@ -302,7 +313,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             keep.append(sl_w_d)
             desc.sl_ptr, desc.sl_src, desc.sl_w = sl.sl_ptr.data_ptr(), sl.sl_src.data_ptr(), sl_w_d.data_ptr()
             desc.dense_rows = dense
-        ring = alloc("ring", (B, n), torch.float32)  # W z of the step (bt_engine_prime clears it)
+        ring = alloc("ring", (B, nc), torch.float32)  # W z of the step (bt_engine_prime clears it)
         work = alloc("work", (L.lib().bt_engine_work_words(n, B, R),), torch.int32)
         keep += [ring, work]
         desc.ring, desc.work = ring.data_ptr(), work.data_ptr()
@@ -354,14 +365,15 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     # outputs (graph: chunk-sized static buffers, copied out after each chunk)
     z = torch.empty((T, B, n), device=dev, dtype=torch.float32) if spikes_out == "dense" else None
     raster = torch.empty((T, B, words), device=dev, dtype=torch.int32)
-    traces = {kind: torch.empty((T, B, n), device=dev, dtype=torch.float32) for kind in trace_kinds}
+    traces = {kind: torch.empty((T, B, nc if kind == "psc" else n), device=dev, dtype=torch.float32)
+              for kind in trace_kinds}
     stat_t = torch.zeros((T, 4), device=dev, dtype=torch.int64) if stats else None
     if use_graph:
         out_c = {"raster": alloc("raster", (K, B, words), torch.int32)}
         if z is not None:
             out_c["z"] = alloc("z", (K, B, n), torch.float32)
         for kind in trace_kinds:
-            out_c[kind] = alloc("trace_" + kind, (K, B, n), torch.float32)
+            out_c[kind] = alloc("trace_" + kind, (K, B, nc if kind == "psc" else n), torch.float32)
         if stats:
             out_c["stats"] = alloc("stats", (K, 4), torch.int64)
         out_full = {"raster": raster, "z": z, "stats": stat_t, **traces}
@@ -502,7 +514,11 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         init_block = plan.history.recent_block(hist_depth).clone() if want_hist_trace else None
         plan.history.store_recent_block(block, T)
     if plan.hetero:
-        plan.top_syn.psc = psc_mod.psc.view(*psc_mod.psc.shape[:-1], *plan.top_syn.n_neuron)
+        lead = psc_mod.psc.shape[:-1]
+        if n_rec == 1:
+            plan.top_syn.psc = psc_mod.psc.view(*lead, *plan.top_syn.n_neuron)
+        else:
+            plan.top_syn.psc = receptor_sum(psc_mod.psc.view(*lead, n, n_rec)).view(*lead, *plan.top_syn.n_neuron)
     if "ref" in traces and ref is None:
         traces.pop("ref")
 
@@ -511,6 +527,8 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         if kind == "history":
             states[key] = _history_trace(plan.history, z if z is not None else _expand(raster, n), init_block,
                                          batch_shape, None)
+        elif kind == "psc_sum":
+            states[key] = receptor_sum(traces["psc"].view(T, B, n, n_rec)).view(T, *batch_shape, *plan.neuron.n_neuron)
         else:
             states[key] = traces[kind].view(T, *batch_shape, *_nshape(plan, key))
     rnn.last_engine_stats = stat_t
@@ -538,7 +556,7 @@ def _graph_signature(desc, *tensors):
 
 def _nshape(plan: EnginePlan, key: str):
     if plan.hetero and key.endswith("base_psc.psc"):
-        return (plan.neuron.size,)
+        return (plan.neuron.size * plan.n_rec,)
     return plan.neuron.n_neuron
 
 

@@ -44,7 +44,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 6
+#define BT_ABI_VERSION 7
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -279,7 +279,7 @@ typedef struct bt_engine_desc {
                              (short rows); 0 = 32 */
 
   bt_neuron_desc neuron;
-  bt_param psc_coef, psc_tau;  /* ExponentialPSC decay */
+  bt_param psc_coef, psc_tau;  /* ExponentialPSC decay, per PSC column (n * n_rec) */
 
   /* connectivity (n_pre == n).  Scatter: CSR over the rows pre * n_bins + bin
      of the delay-expanded matrix, csr_dst = post, both edge arrays 16-byte
@@ -288,10 +288,11 @@ typedef struct bt_engine_desc {
   const int32_t* csr_ptr; const uint32_t* csr_dst; const float* csr_w;
   const int32_t* csc_ptr; const uint32_t* csc_src; const float* csc_w;
 
-  /* state [batch, n], updated in place */
+  /* state [batch, n], updated in place; psc is [batch, n * n_rec] (column
+     post * n_rec + r: the base PSC of HeterSynapsePSC) */
   float* v; float* refractory; float* g_k; float* psc;
-  float* ring;            /* [batch][n] scatter: synaptic input W z accumulated for the
-                             next neuron step (zero between runs) */
+  float* ring;            /* [batch][n * n_rec] scatter: synaptic input W z accumulated
+                             for the next neuron step (zero between runs) */
   uint32_t* hist;         /* [hist_len][batch][words] spike bitmaps, slot = step mod H */
 
   /* inputs */
@@ -302,7 +303,7 @@ typedef struct bt_engine_desc {
   uint32_t* raster;       /* [n_steps][batch][words] spike bitmaps */
   float* spikes;          /* [n_steps][batch][n] spikes as fp32 (reference output layout) */
   float* v_trace;         /* [n_steps][batch][n] v after each step */
-  float* psc_trace;       /* [n_steps][batch][n] psc after each step */
+  float* psc_trace;       /* [n_steps][batch][n * n_rec] psc after each step */
   float* ref_trace;       /* [n_steps][batch][n] refractory after each step */
   float* gk_trace;        /* [n_steps][batch][n] g_k after each step (ALIF) */
 
@@ -337,7 +338,11 @@ typedef struct bt_engine_desc {
   float psc_coef_s, psc_tau_s;
   int32_t psc_fast_div;   /* 1: psc_tau verified as above, reciprocal psc_rcp */
   float psc_rcp;
-  int32_t pad5_;
+  int32_t n_rec;          /* receptor channels per neuron, C (0 or 1: none; at most 16;
+                             scatter and gather modes): the matrix has n * C columns,
+                             post * C + r, and the neuron's input is the sum of its C
+                             PSCs in torch's CPU row-sum order (HeterSynapsePSC with
+                             n_receptor = C, btorch/models/synapse.py:626-847) */
   /* scatter: the expanded CSR's edges interleaved, [2 * len(csr_dst)] words:
      post, weight bits, post, weight bits, ... (one 8-byte record per edge, so
      a short row occupies the fewest memory sectors); 16-byte aligned */

@@ -1,0 +1,90 @@
+"""Receptor channels end to end: a connectome table -> make_hetersynapse_conn
+(E/I neuron mode, 4 receptor pairs, per-synapse delays over 5 bins) ->
+HeterSynapsePSC(n_receptor=4, ExponentialPSC with a time constant per
+receptor) -> RecurrentNN, against the reference's own run of the same tables
+(tests/golden/receptors_delay.npz): spike raster, v, receptor-summed psc and
+the per-channel base psc bit for bit, through the fused engine (gather and
+scatter, eager and CUDA graph) and the per-module path."""
+
+import numpy as np
+import pandas as pd
+import pytest
+import scipy.sparse as sp
+import torch
+
+from btorch_b200.connectome import make_hetersynapse_conn
+from btorch_b200.models import LIF, ExponentialPSC, HeterSynapsePSC, RecurrentNN, SparseConn, environ
+from btorch_b200.models.functional import init_net_state
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+
+
+def build(d, direction):
+    n, D = int(d["n"]), int(d["n_bins"])
+    neu = pd.DataFrame({k.split(".", 1)[1]: v for k, v in d.items() if k.startswith("neurons.")})
+    con = pd.DataFrame({k.split(".", 1)[1]: v for k, v in d.items() if k.startswith("conns.")})
+    neu["EI"] = neu["EI"].astype(object)
+    m, idx = make_hetersynapse_conn(neu, con, delay_col="delay_steps", n_delay_bins=D)
+    m = m.tocoo()
+    inh = (neu.EI.to_numpy() == "I")[m.row // D]
+    w = (m.data * 2.0**-5 * np.where(inh, -1.0, 1.0)).astype(np.float32)
+    conn = SparseConn(sp.coo_array((w, (m.row, m.col)), shape=m.shape), sparse_config={"direction": direction})
+    # the connection is the reference's, entry for entry (canonical order)
+    np.testing.assert_array_equal(conn.indices[0].numpy(), d["post"])
+    np.testing.assert_array_equal(conn.indices[1].numpy(), d["src"])
+    C = len(idx)
+    syn = HeterSynapsePSC(n, C, idx, conn, base_psc=ExponentialPSC, max_delay_steps=D, use_circular_buffer=True,
+                          tau_syn=torch.tensor(np.tile(d["taus"], n)))
+    rnn = RecurrentNN(LIF(n, tau_ref=2.0, hard_reset=True), syn,
+                      update_state_names=("neuron.v", "synapse.psc", "synapse.base_psc.psc")).to(DEV)
+    init_net_state(rnn, batch_size=int(d["batch"]), dtype=torch.float32, device=DEV)
+    return rnn
+
+
+@pytest.mark.parametrize("path", ["gather", "scatter", "gather-graph", "scatter-graph", "modular"])
+def test_receptors_with_delays_match_reference(path):
+    d = cases.load("receptors_delay")
+    n = int(d["n"])
+    direction = path.split("-")[0] if path != "modular" else "gather"
+    rnn = build(d, direction)
+    rnn.fused = path != "modular"
+    rnn.cudagraph = path.endswith("graph")
+    x = torch.tensor(d["x"], device=DEV)
+    with torch.no_grad(), environ.context(dt=1.0):
+        if rnn.cudagraph:
+            z1, st1 = rnn(x[:48], engine_chunk=12)
+            z2, st2 = rnn(x[48:], engine_chunk=12)
+            z = torch.cat([z1, z2])
+            st = {k: torch.cat([st1[k], st2[k]]) for k in st1}
+        else:
+            z, st = rnn(x)
+    assert rnn.last_path == ("modular" if path == "modular" else "fused")
+    if path != "modular":
+        assert rnn.last_engine_direction == direction
+    np.testing.assert_array_equal(z.cpu().numpy().astype(np.uint8), cases.spikes(d))
+    K = d["v"].shape[0]
+    np.testing.assert_array_equal(st["neuron.v"].cpu().numpy()[:K], d["v"])
+    np.testing.assert_array_equal(st["synapse.psc"].cpu().numpy()[:K], d["psc"])
+    np.testing.assert_array_equal(st["synapse.base_psc.psc"].cpu().numpy()[:K], d["psc_rec"])
+    np.testing.assert_array_equal(rnn.neuron.v.cpu().numpy(), d["v_final"])
+    np.testing.assert_array_equal(rnn.synapse.psc.cpu().numpy(), d["psc_final"])
+    np.testing.assert_array_equal(rnn.synapse.base_psc.psc.cpu().numpy(), d["psc_rec_final"])
+    # receptor channel lookup (synapse.py:763-830)
+    ee = rnn.synapse.get_psc(("E", "E"))
+    assert ee.shape == (int(d["batch"]), n)
+    np.testing.assert_array_equal(ee.cpu().numpy(), d["psc_rec_final"].reshape(-1, n, 4)[..., 0])
+
+
+def test_receptor_sum_order_on_gpu():
+    """The GPU receptor sum replays torch's CPU order: equal to torch.sum on
+    the CPU for 1..16 channels on values whose sums round differently in
+    other orders."""
+    from btorch_b200.models.synapse import receptor_sum
+
+    rng = np.random.default_rng(5)
+    for C in range(1, 17):
+        a = (rng.standard_normal((64, 300, C)) * np.exp(rng.standard_normal((64, 300, C)) * 3)).astype(np.float32)
+        t = torch.tensor(a)
+        np.testing.assert_array_equal(receptor_sum(t.to(DEV)).cpu().numpy(), t.sum(-1).numpy(), err_msg=str(C))

@@ -55,6 +55,7 @@ def test_two_receptor_hetersynapse_matches_reference(direction):
     init_net_state(rnn, batch_size=int(d["batch"]), dtype=torch.float32, device=DEV)
     with torch.no_grad(), environ.context(dt=1.0):
         z, st = rnn(torch.tensor(d["x"], device=DEV))
+    assert rnn.last_path == "fused" and rnn.last_engine_direction == direction
     ref_z = np.unpackbits(d["z"], axis=-1, bitorder="little")[..., :n]
     np.testing.assert_array_equal(z.cpu().numpy().astype(np.uint8), ref_z)
     K = d["v"].shape[0]
