@@ -54,11 +54,20 @@ CONFIGS = {
     # s_state: v, psc, refractory r/w (24) + drive read (4) + delay-ring slot read and clear (8)
     "connectome": dict(model="lif_hetero_delay", n=140000, indeg=350, indeg_sigma=1.0, n_bins=20, exc=0.7,
                        batch=8, t_max=2000, dur=(2000, 2000), c_m=64.0, drive=(0.25, 8.0), s_state=36),
+    # the connectome workload with receptor channels: HeterSynapsePSC(n_receptor=4), the (pre type, post
+    # type) E/I pairs of make_hetersynapse_conn's neuron mode, a synaptic time constant per channel;
+    # s_state: v, refractory r/w (16) + drive read (4) + per channel psc r/w and acc read/clear (16 C)
+    "connectome_receptors": dict(model="lif_hetero_receptors", n=140000, indeg=350, indeg_sigma=1.0, n_bins=20,
+                                 exc=0.7, batch=8, t_max=2000, dur=(2000, 2000), c_m=64.0, drive=(0.25, 8.0),
+                                 receptors=4, taus=(5.0, 3.0, 10.0, 2.5), s_state=84),
     # shorter runs of the same workloads, for profiler captures (a few GB on the device)
     "batched_short": dict(model="alif_dense_input", n=65536, indeg=500, batch=64, c_in=2000, t_max=512,
                           rate=(2.0, 40.0), dur=(512, 512), w_scale=0.0030, in_gain=1.0, s_state=36),
     "connectome_short": dict(model="lif_hetero_delay", n=140000, indeg=350, indeg_sigma=1.0, n_bins=20, exc=0.7,
                              batch=8, t_max=256, dur=(256, 256), c_m=64.0, drive=(0.25, 8.0), s_state=36),
+    "connectome_receptors_short": dict(model="lif_hetero_receptors", n=140000, indeg=350, indeg_sigma=1.0,
+                                       n_bins=20, exc=0.7, batch=8, t_max=192, dur=(192, 192), c_m=64.0,
+                                       drive=(0.25, 8.0), receptors=4, taus=(5.0, 3.0, 10.0, 2.5), s_state=84),
     # plain forward simulation: the reference's own CPU-runnable case, batch 1
     "plain": dict(model="lif_plain", n=4096, p=0.02, batch=1, c_in=1000, t_max=1000, in_rate=0.01, in_std=0.05,
                   w_scale=0.1, dur=(1000, 1000), s_state=36),
@@ -80,7 +89,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="batched", choices=sorted(CONFIGS))
-    ap.add_argument("--extra", default="plain,connectome,training,serving",
+    ap.add_argument("--extra", default="plain,connectome,connectome_receptors,training,serving",
                     help="comma-separated workloads measured after the headline one ('' for none)")
     ap.add_argument("--direction", default="scatter", choices=["scatter", "gather", "auto"])
     ap.add_argument("--no-cudagraph", action="store_true", help="launch every chunk eagerly")
@@ -152,7 +161,16 @@ def make_network(cfg, seed=0):
     delay = rng.integers(1, R + 1, size=post.size)
     count = rng.geometric(0.25, size=post.size)
     w = (count * np.where(pre < int(cfg["exc"] * n), 1.0, -1.0) * 2.0 ** -6).astype(np.float32)
-    return dict(post=post, src=pre * R + (delay - 1), pre=pre, delay_bin=delay - 1, w=w, n_bins=R, w_in=None)
+    src = pre * R + (delay - 1)
+    C = cfg.get("receptors", 1)
+    if C > 1:
+        # column post * 4 + pair, pair = 2 type(pre) + type(post), type 0 = E (the first exc * n ids), 1 = I:
+        # the stacked layout of make_hetersynapse_conn's neuron mode; re-sorted into (column, src) order
+        inh = np.arange(n) >= int(cfg["exc"] * n)
+        col = post * C + 2 * inh[pre] + inh[post]
+        order = np.lexsort((src, col))
+        post, src, pre, delay, w = col[order], src[order], pre[order], delay[order], w[order]
+    return dict(post=post, src=src, pre=pre, delay_bin=delay - 1, w=w, n_bins=R, w_in=None, n_rec=C)
 
 
 def make_training_network(cfg, seed=0):
@@ -310,8 +328,8 @@ def build_model(cfg, net, device, direction, batch=None):
                                     SparseConn)
     from btorch_b200.models.functional import init_net_state
 
-    n, R = cfg["n"], net["n_bins"]
-    conn = SparseConn.from_canonical(net["post"], net["src"], net["w"], (n * R, n), enforce_dale=False,
+    n, R, C = cfg["n"], net["n_bins"], net.get("n_rec", 1)
+    conn = SparseConn.from_canonical(net["post"], net["src"], net["w"], (n * R, n * C), enforce_dale=False,
                                      sparse_config={"direction": direction})
     if cfg["model"] == "alif_dense_input":
         neuron = ALIF(n, v_threshold=1.0, v_reset=0.0, c_m=1.0, g_leak=0.05, E_leak=0.0, E_k=-1.0,
@@ -322,6 +340,14 @@ def build_model(cfg, net, device, direction, batch=None):
         neuron = LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=2.0, hard_reset=True)
         syn = ExponentialPSC(n, tau_syn=5.0, linear=conn)
         inp = DenseConn(cfg["c_in"], n, weight=torch.from_numpy(net["w_in"]))
+    elif C > 1:
+        neuron = LIF(n, v_threshold=1.0, v_reset=0.0, c_m=cfg["c_m"], tau=20.0, tau_ref=2.0, hard_reset=True)
+        rti = pd.DataFrame([(0, "E", "E"), (1, "E", "I"), (2, "I", "E"), (3, "I", "I")],
+                           columns=["receptor_index", "pre_receptor_type", "post_receptor_type"])
+        taus = torch.tensor(cfg["taus"], dtype=torch.float32).repeat(n)
+        syn = HeterSynapsePSC(n, C, rti, conn, base_psc=ExponentialPSC, max_delay_steps=R,
+                              use_circular_buffer=True, tau_syn=taus)
+        inp = None
     else:
         neuron = LIF(n, v_threshold=1.0, v_reset=0.0, c_m=cfg["c_m"], tau=20.0, tau_ref=2.0, hard_reset=True)
         rti = pd.DataFrame({"receptor_type": ["syn"], "receptor_index": [0]})
@@ -362,8 +388,10 @@ def describe(name, cfg):
     if cfg["model"] == "alif_dense_input":
         return (f"{name}: ALIF+ExpPSC N={cfg['n']} fixed in-degree {cfg['indeg']} batch {cfg['batch']} "
                 f"durations {cfg['dur']} T_max {cfg['t_max']} c_in {cfg['c_in']}")
+    rec = (f" {cfg['receptors']} receptor channels (E/I pairs, tau_syn {'/'.join(map(str, cfg['taus']))})"
+           if cfg.get("receptors", 1) > 1 else "")
     return (f"{name}: LIF+HeterSynapsePSC(ExpPSC) N={cfg['n']} lognormal in-degree mean {cfg['indeg']} "
-            f"sigma {cfg['indeg_sigma']} delays 1..{cfg['n_bins']} batch {cfg['batch']} T {cfg['t_max']} "
+            f"sigma {cfg['indeg_sigma']} delays 1..{cfg['n_bins']}{rec} batch {cfg['batch']} T {cfg['t_max']} "
             f"drive {cfg['drive'][1]} x Poisson({cfg['drive'][0]})")
 
 
@@ -752,7 +780,7 @@ def main():
             torch.cuda.empty_cache()
             continue
         sub, m, xe, le, ne, _ = measure(extra, ecfg, args, dev, world, rank, local)
-        if rank == 0 and world == 1 and ecfg["batch"] > 1:
+        if rank == 0 and world == 1 and ecfg["batch"] > 1 and ecfg.get("receptors", 1) == 1:
             sub["plain_step"] = plain_step(ecfg, ne, xe, le, args, dev)
             sub["vs_plain_step"] = sub["value"] / sub["plain_step"]["value"]
         if rank == 0 and world == 1 and ecfg["model"] == "lif_plain" and not args.no_cpu_baseline:

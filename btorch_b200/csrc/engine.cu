@@ -64,44 +64,50 @@ __host__ __device__ __forceinline__ int n_rec(const bt_engine_desc& d) { return 
 //               a_0 + a_1 + ... + a_7 left to right.
 // (Established against torch.sum for every C up to 39; the host mirror in
 // btorch_b200/models/synapse.py is checked against torch.sum in the CPU
-// tests.)  Indices are compile-time after unrolling.
-__device__ __forceinline__ float receptor_sum(const float (&p)[kMaxRec], int C) {
-  if (C < 4) {
+// tests.)  p holds M >= C values; indices are compile-time after unrolling.
+template <int M>
+__device__ __forceinline__ float receptor_sum(const float (&p)[M], int C) {
+  if (C < 4 || M < 4) {
     float s = p[0];
 #pragma unroll
-    for (int r = 1; r < 4; ++r)
+    for (int r = 1; r < 4 && r < M; ++r)
       if (r < C) s = add(s, p[r]);
     return s;
   }
-  if (C < 8) {
-    float a0 = p[0];
+  if constexpr (M >= 4) {
+    if (C < 8 || M < 8) {
+      float a0 = p[0];
 #pragma unroll
-    for (int r = 4; r < 8; ++r)
-      if (r < C) a0 = add(a0, p[r]);
-    return add(add(add(a0, p[1]), p[2]), p[3]);
+      for (int r = 4; r < 8 && r < M; ++r)
+        if (r < C) a0 = add(a0, p[r]);
+      return add(add(add(a0, p[1]), p[2]), p[3]);
+    }
   }
-  const int full = C & ~7;
-  float a[8];
+  if constexpr (M >= 8) {
+    const int full = C & ~7;
+    float a[8];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) a[j] = p[j];
+    for (int j = 0; j < 8; ++j) a[j] = p[j];
 #pragma unroll
-  for (int r = 8; r < kMaxRec; ++r)
-    if (r < full) a[r & 7] = add(a[r & 7], p[r]);
-  if (full < C) {
-    float t = 0.0f;
-    bool first = true;
+    for (int r = 8; r < M; ++r)
+      if (r < full) a[r & 7] = add(a[r & 7], p[r]);
+    if (full < C) {
+      float t = 0.0f;
+      bool first = true;
 #pragma unroll
-    for (int r = 8; r < kMaxRec; ++r)
-      if (r >= full && r < C) {
-        t = first ? p[r] : add(t, p[r]);
-        first = false;
-      }
-    a[0] = add(a[0], t);
+      for (int r = 8; r < M; ++r)
+        if (r >= full && r < C) {
+          t = first ? p[r] : add(t, p[r]);
+          first = false;
+        }
+      a[0] = add(a[0], t);
+    }
+    float s = a[0];
+#pragma unroll
+    for (int j = 1; j < 8; ++j) s = add(s, a[j]);
+    return s;
   }
-  float s = a[0];
-#pragma unroll
-  for (int j = 1; j < 8; ++j) s = add(s, a[j]);
-  return s;
+  return p[0];  // not reached: C <= M
 }
 
 __host__ __device__ __forceinline__ int mask_words(int64_t batch) { return int((batch + 31) >> 5); }
@@ -241,12 +247,16 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   float* __restrict__ gk_p = KIND == BT_NEURON_ALIF ? d.g_k + off0 : nullptr;
   const float* __restrict__ x_p = d.x ? d.x + k * B * n + off0 : nullptr;
   float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
+  int64_t lenv[S];
   const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
   const int n32 = int(n);  // batch * n < 2^31 in scatter mode (checked on the host)
+  // every load before the first store: a load behind a store through a
+  // pointer that may alias it waits for the store
 #pragma unroll
   for (int u = 0; u < S; ++u) {
     const bool in = valid && u < nb;
     const int o = u * n32;
+    lenv[u] = (in && d.sample_len) ? d.sample_len[b0 + u] : INT64_MAX;
     pend[u] = in ? ld_f32(ring_p + o, pol_keep) : 0.0f;
     pv[u] = in ? psc_p[o] : 0.0f;
     xv[u] = (in && x_p) ? ld_nc_f32(x_p + o, pol_stream) : 0.0f;
@@ -271,7 +281,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
     float s = 0.0f;
     if (valid) {
       st_f32(ring_p + o, 0.0f, pol_keep);
-      const int64_t len = d.sample_len ? d.sample_len[b0 + u] : INT64_MAX;
+      const int64_t len = lenv[u];
       float v = vv[u], ref = rv[u], gk = gv[u];
       float P;
       if (k < len) {
@@ -315,11 +325,16 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
 // SCATTER neuron step with receptor channels (n_rec = C > 1): for each
 // channel column c = i * C + r, P_r = stored + acc (acc zeroed); the neuron's
 // input is receptor_sum(P) (+ x); stored = decay_r(P_r).  Grid
-// (ceil(n / 256), batch): a thread owns (neuron i, sample b).
-template <int KIND, bool HARD, bool USE_REF>
+// (ceil(n / 256), batch): a thread owns (neuron i, sample b).  CT = C known
+// at compile time (2 or 4: the channels of (b, i) are one 8- or 16-byte
+// vector) or 0 (any C up to kMaxRec).  Every load of the thread is issued
+// before its first store: a load behind a store through a pointer that may
+// alias it waits for the store, which made this step latency bound.
+template <int KIND, bool HARD, bool USE_REF, int CT>
 __global__ void __launch_bounds__(kEngThreads) k_eng_neuron_rec(bt_engine_desc d, int64_t k, StepIdx si) {
+  constexpr int M = CT > 0 ? CT : kMaxRec;
   const int64_t n = d.n, B = d.batch;
-  const int C = n_rec(d);
+  const int C = CT > 0 ? CT : n_rec(d);
   const int64_t nc = n * C;
   const int64_t words = (n + 31) >> 5;
   const int64_t i = int64_t(blockIdx.x) * kEngThreads + threadIdx.x;
@@ -328,37 +343,91 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron_rec(bt_engine_desc d
   float s = 0.0f;
   if (i < n) {
     const int64_t idx = b * n + i, c0 = b * nc + i * C;
-    const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
-    float P[kMaxRec];
-    for (int r = 0; r < C; ++r) {
-      const float pend = d.ring[c0 + r];
-      d.ring[c0 + r] = 0.0f;
-      // past a sample's end: the first step completes psc of its last step,
-      // later arrivals are dropped (as k_eng_neuron)
-      P[r] = k <= len ? add(d.psc[c0 + r], pend) : d.psc[c0 + r];
-      if (k == len) d.psc[c0 + r] = P[r];
+    float* __restrict__ ring = d.ring + c0;
+    float* __restrict__ psc = d.psc + c0;
+    // loads
+    float pend[M], stv[M], pc[M], pt[M];
+    if constexpr (CT == 4) {
+      const float4 a = *reinterpret_cast<const float4*>(ring), q = *reinterpret_cast<const float4*>(psc);
+      pend[0] = a.x, pend[1] = a.y, pend[2] = a.z, pend[3] = a.w;
+      stv[0] = q.x, stv[1] = q.y, stv[2] = q.z, stv[3] = q.w;
+    } else if constexpr (CT == 2) {
+      const float2 a = *reinterpret_cast<const float2*>(ring), q = *reinterpret_cast<const float2*>(psc);
+      pend[0] = a.x, pend[1] = a.y;
+      stv[0] = q.x, stv[1] = q.y;
+    } else {
+      for (int r = 0; r < C; ++r) {
+        pend[r] = ring[r];
+        stv[r] = psc[r];
+      }
     }
+#pragma unroll
+    for (int r = 0; r < M; ++r) {
+      if (r >= C) break;
+      pc[r] = d.psc_uniform ? d.psc_coef_s : ld(d.psc_coef, i * C + r);
+      pt[r] = d.psc_uniform ? d.psc_tau_s : ld(d.psc_tau, i * C + r);
+    }
+    const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
     float v = d.v[idx];
     float ref = USE_REF ? d.refractory[idx] : 0.0f;
     float gk = KIND == BT_NEURON_ALIF ? d.g_k[idx] : 0.0f;
+    const float xv = d.x ? d.x[(k * B) * n + idx] : 0.0f;
+    const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, i);
+    // past a sample's end: the first step completes psc of its last step,
+    // later arrivals are dropped (as k_eng_neuron)
+    float P[M];
+#pragma unroll
+    for (int r = 0; r < M; ++r) {
+      if (r >= C) break;
+      P[r] = k <= len ? add(stv[r], pend[r]) : stv[r];
+    }
+    // stores
+    if constexpr (CT == 4) {
+      *reinterpret_cast<float4*>(ring) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    } else if constexpr (CT == 2) {
+      *reinterpret_cast<float2*>(ring) = make_float2(0.0f, 0.0f);
+    } else {
+      for (int r = 0; r < C; ++r) ring[r] = 0.0f;
+    }
+    float out[M];
+    bool write = k <= len;
     if (k < len) {
-      float I = receptor_sum(P, C);
-      if (d.x) I = add(I, d.x[(k * B) * n + idx]);
-      const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, i);
-      const NeuronOut out = neuron_update<KIND, HARD, USE_REF, true>(prm, I, v, ref, gk);
-      s = out.spike;
+      const float I0 = receptor_sum(P, C);
+      const float I = d.x ? add(I0, xv) : I0;
+      const NeuronOut o = neuron_update<KIND, HARD, USE_REF, true>(prm, I, v, ref, gk);
+      s = o.spike;
       d.v[idx] = v;
       if (USE_REF) d.refractory[idx] = ref;
       if (KIND == BT_NEURON_ALIF) d.g_k[idx] = gk;
-      for (int r = 0; r < C; ++r) {
-        const int64_t col = i * C + r;
-        const float pc = d.psc_uniform ? d.psc_coef_s : ld(d.psc_coef, col);
-        const float pt = d.psc_uniform ? d.psc_tau_s : ld(d.psc_tau, col);
-        d.psc[c0 + r] = psc_decay(pc, make_div(pt, d.psc_uniform && d.psc_fast_div, d.psc_rcp), P[r]);
+#pragma unroll
+      for (int r = 0; r < M; ++r) {
+        if (r >= C) break;
+        out[r] = psc_decay(pc[r], make_div(pt[r], d.psc_uniform && d.psc_fast_div, d.psc_rcp), P[r]);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < M; ++r) {
+        if (r >= C) break;
+        out[r] = P[r];
       }
     }
-    if (d.psc_trace && k > 0)
-      for (int r = 0; r < C; ++r) d.psc_trace[((k - 1) * B) * nc + c0 + r] = P[r];
+    if (write) {
+      if constexpr (CT == 4) {
+        *reinterpret_cast<float4*>(psc) = make_float4(out[0], out[1], out[2], out[3]);
+      } else if constexpr (CT == 2) {
+        *reinterpret_cast<float2*>(psc) = make_float2(out[0], out[1]);
+      } else {
+        for (int r = 0; r < C; ++r) psc[r] = out[r];
+      }
+    }
+    if (d.psc_trace && k > 0) {
+      float* tr = d.psc_trace + ((k - 1) * B) * nc + c0;
+#pragma unroll
+      for (int r = 0; r < M; ++r) {
+        if (r >= C) break;
+        tr[r] = P[r];
+      }
+    }
     const int64_t tix = (k * B) * n + idx;
     if (d.v_trace) d.v_trace[tix] = v;
     if (USE_REF && d.ref_trace) d.ref_trace[tix] = ref;
@@ -781,17 +850,17 @@ __global__ void k_eng_scatter_final(bt_engine_desc d) {
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t nc = d.n * n_rec(d), B = d.batch;  // one thread per PSC column
   if (idx >= B * nc) return;
-  const float pending = d.ring[idx];
-  d.ring[idx] = 0.0f;
+  // all loads before the first store (see k_eng_neuron_rec)
+  float* __restrict__ ring = d.ring;
+  float* __restrict__ psc = d.psc;
+  const float pending = ring[idx];
+  const float stored = psc[idx];
   const int64_t b = idx / nc;
   const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
-  if (d.n_steps - 1 < len) {
-    const float P = add(d.psc[idx], pending);
-    d.psc[idx] = P;
-    if (d.psc_trace) d.psc_trace[((d.n_steps - 1) * B) * nc + idx] = P;
-  } else if (d.psc_trace) {
-    d.psc_trace[((d.n_steps - 1) * B) * nc + idx] = d.psc[idx];
-  }
+  ring[idx] = 0.0f;
+  const float P = d.n_steps - 1 < len ? add(stored, pending) : stored;
+  if (d.n_steps - 1 < len) psc[idx] = P;
+  if (d.psc_trace) d.psc_trace[((d.n_steps - 1) * B) * nc + idx] = P;
 }
 
 // ----------------------------------------------------------------- gather --
@@ -1359,9 +1428,13 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
                                           : pick(std::integral_constant<int, 32>());
     const int C = n_rec(d);
     const dim3 rgrid(unsigned(ceil_div(n, kEngThreads)), unsigned(d.batch));
+    // vector access to the C channels of (b, i) needs 8 / 16-byte aligned state and acc
+    const bool aligned = ((reinterpret_cast<uintptr_t>(d.psc) | reinterpret_cast<uintptr_t>(d.ring)) & 15) == 0;
+    auto rec = C == 4 && aligned ? k_eng_neuron_rec<KIND, HARD, USE_REF, 4>
+             : C == 2 && aligned ? k_eng_neuron_rec<KIND, HARD, USE_REF, 2> : k_eng_neuron_rec<KIND, HARD, USE_REF, 0>;
     for (int64_t k = 0; k < d.n_steps; ++k) {
       const StepIdx si = step_idx(d.t0 + k, d.n_bins, d.hist_len);
-      if (C > 1) k_eng_neuron_rec<KIND, HARD, USE_REF><<<rgrid, kEngThreads, 0, s>>>(d, k, si);
+      if (C > 1) rec<<<rgrid, kEngThreads, 0, s>>>(d, k, si);
       else neuron<<<grid, kEngThreads, 0, s>>>(d, k, si);
       scatter<<<sgrid, kEngThreads, 0, s>>>(d, k, si);
     }

@@ -518,7 +518,13 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         if n_rec == 1:
             plan.top_syn.psc = psc_mod.psc.view(*lead, *plan.top_syn.n_neuron)
         else:
-            plan.top_syn.psc = receptor_sum(psc_mod.psc.view(*lead, n, n_rec)).view(*lead, *plan.top_syn.n_neuron)
+            ps = receptor_sum(psc_mod.psc.view(*lead, n, n_rec)).view(*lead, *plan.top_syn.n_neuron)
+            cur = plan.top_syn.psc
+            if torch.is_tensor(cur) and cur.shape == ps.shape and cur.dtype == ps.dtype and cur.device == ps.device \
+                    and not cur.is_inference():
+                cur.copy_(ps)  # keep the module's own (non-inference) tensor: in-place resets stay legal
+            else:
+                plan.top_syn.psc = ps
     if "ref" in traces and ref is None:
         traces.pop("ref")
 

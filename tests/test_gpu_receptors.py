@@ -88,3 +88,19 @@ def test_receptor_sum_order_on_gpu():
         a = (rng.standard_normal((64, 300, C)) * np.exp(rng.standard_normal((64, 300, C)) * 3)).astype(np.float32)
         t = torch.tensor(a)
         np.testing.assert_array_equal(receptor_sum(t.to(DEV)).cpu().numpy(), t.sum(-1).numpy(), err_msg=str(C))
+
+
+def test_inplace_reset_after_inference_run():
+    """A fused run under inference_mode leaves the modules' state tensors
+    usable by an in-place reset outside it (the serving / benchmark loop)."""
+    from btorch_b200.models.functional import reset_net
+
+    d = cases.load("receptors_delay")
+    rnn = build(d, "scatter")
+    rnn.update_state_names = ()
+    x = torch.tensor(d["x"], device=DEV)
+    for _ in range(2):
+        reset_net(rnn, inplace=True)
+        with torch.inference_mode(), environ.context(dt=1.0):
+            z, _ = rnn(x)
+        np.testing.assert_array_equal(z.cpu().numpy().astype(np.uint8), cases.spikes(d))
