@@ -718,25 +718,31 @@ def main():
     line, rnn, x, lens, net, one_step = measure(args.config, cfg, args, dev, world, rank, local)
     stream = torch.cuda.current_stream(dev)
     T, B, n = cfg["t_max"], cfg["batch"], cfg["n"]
-    # e2e: host buffers through the public API (H2D of the input, D2H of the raster)
+    # e2e: host buffers through the public API -- the input in pinned host
+    # memory, the model on the device: the engine streams the input to the
+    # device chunk by chunk and the spike raster back to pinned host memory,
+    # on a copy stream overlapped with the compute
     if not args.no_e2e:
         x_host = x.cpu().pin_memory()
-        raster_host = torch.empty((T, B, (n + 31) // 32), dtype=torch.int32).pin_memory()
+        r = None
+        for _ in range(3):
+            # the loop below holds one result while the next call runs: warm the
+            # host allocator's cache of pinned output blocks the same way
+            r = one_step(x_host)
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        ev_parts = []
+        ev = 0
+        d2h = 0
         for _ in range(args.steps):
-            xd = x_host.to(dev, non_blocking=True)
-            r = one_step(xd)
-            raster_host.copy_(r, non_blocking=True)
-            ev_parts.append(rnn.last_engine_stats[:, 1].sum())
+            r = one_step(x_host)  # returns the raster in host memory (the previous one held meanwhile)
+            ev += int(rnn.last_engine_stats[:, 1].sum())
+            d2h = r.numel() * r.element_size()
         e1.record(stream)
         torch.cuda.synchronize()
-        ev = int(sum(int(p.item()) for p in ev_parts))
         e2e_ms = e0.elapsed_time(e1)
         if world > 1:
             import torch.distributed as dist
@@ -744,9 +750,9 @@ def main():
             e2e_ms, ev = job_totals(e2e_ms, ev, dev)
         if rank == 0:
             line["e2e"] = {"value": ev / (e2e_ms * 1e-3), "unit": "events/s",
-                           "h2d_bytes_per_step": int(x_host.numel() * 4),
-                           "d2h_bytes_per_step": int(raster_host.numel() * 4)}
-        del x_host, raster_host
+                           "h2d_bytes_per_step": int(x_host.numel() * 4), "d2h_bytes_per_step": int(d2h),
+                           "path": "host input and raster streamed in chunks on a copy stream"}
+        del x_host, r
     if args.ncu_window is not None:
         w0 = args.ncu_window
 

@@ -221,7 +221,17 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     neuron, psc_mod, conn = plan.neuron, plan.psc_mod, plan.conn
     n = neuron.size
     dev = neuron.v.device
-    L.require_cuda(x, neuron.v, what="RecurrentNN")
+    # host-resident input: streamed to the device chunk by chunk and the
+    # outputs streamed back, on a copy stream overlapped with the compute
+    host_io = not x.is_cuda
+    if host_io:
+        L.require_cuda(neuron.v, what="RecurrentNN")
+        if x.dtype != torch.float32:
+            raise TypeError("RecurrentNN input must be float32 for the fused engine.")
+        if not x.is_pinned():
+            x = x.pin_memory()
+    else:
+        L.require_cuda(x, neuron.v, what="RecurrentNN")
     dt = float(environ.get("dt"))
     v_mod = _state2d(neuron.v, n)
     B = v_mod.shape[0]
@@ -362,12 +372,20 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         L.check(L.lib().bt_engine_prime(C.byref(desc), s), "bt_engine_prime")
         launches += 1 if desc.bin_hi > 0 else 0
 
-    # outputs (graph: chunk-sized static buffers, copied out after each chunk)
-    z = torch.empty((T, B, n), device=dev, dtype=torch.float32) if spikes_out == "dense" else None
-    raster = torch.empty((T, B, words), device=dev, dtype=torch.int32)
-    traces = {kind: torch.empty((T, B, nc if kind == "psc" else n), device=dev, dtype=torch.float32)
-              for kind in trace_kinds}
-    stat_t = torch.zeros((T, 4), device=dev, dtype=torch.int64) if stats else None
+    # outputs (graph: chunk-sized static buffers, copied out after each chunk;
+    # host input: pinned host tensors filled by the copy stream)
+    odev = torch.device("cpu") if host_io else dev
+
+    def out_tensor(shape, dtype, zero=False):
+        if host_io:
+            t = torch.empty(shape, dtype=dtype, pin_memory=True)
+            return t.zero_() if zero else t
+        return (torch.zeros if zero else torch.empty)(shape, device=dev, dtype=dtype)
+
+    z = out_tensor((T, B, n), torch.float32) if spikes_out == "dense" else None
+    raster = out_tensor((T, B, words), torch.int32)
+    traces = {kind: out_tensor((T, B, nc if kind == "psc" else n), torch.float32) for kind in trace_kinds}
+    stat_t = out_tensor((T, 4), torch.int64, zero=True) if stats else None
     if use_graph:
         out_c = {"raster": alloc("raster", (K, B, words), torch.int32)}
         if z is not None:
@@ -389,22 +407,26 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         if x3.dtype != torch.float32:
             raise TypeError("RecurrentNN input must be float32 for the fused engine.")
         x3 = x3.contiguous()
+        if host_io and not x3.is_pinned():
+            x3 = x3.pin_memory()
     if sample_len is not None:
         sl_full = torch.as_tensor(sample_len, device=dev, dtype=torch.int64).reshape(B)
+    io = _HostStreams(dev, x3, K, T, (z, raster, stat_t, traces)) if host_io else None
 
     def chunk_inputs(k0, kc):
         """Device inputs of the chunk at k0: (projection input or None, step input, sample lengths)."""
+        src = io.take(k0) if host_io else x3[k0:k0 + kc]  # host input: the prefetched device copy
         if use_graph:
             xin = alloc("x", (K, B, c_in), torch.float32)
-            xin[:kc].copy_(x3[k0:k0 + kc])
+            xin[:kc].copy_(src[:kc])
             xp = alloc("xp", (K, B, n), torch.float32) if inp is not None else xin
             if inp is None:
                 xin = None
         elif inp is not None:
-            xin = x3[k0:k0 + kc].float().contiguous()
+            xin = src[:kc].float().contiguous()
             xp = torch.empty((kc, B, n), device=dev, dtype=torch.float32)
         else:
-            xin, xp = None, x3[k0:k0 + kc]
+            xin, xp = None, src[:kc]
         slc = None
         if sample_len is not None:
             slv = (sl_full - k0).clamp(0, kc).to(torch.int32)
@@ -448,16 +470,26 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             profile.append(("step", e0, _ev()))
         return nl
 
+    if host_io:
+        io.prefetch(0)
     for k0 in range(0, T, K):
         kc = min(K, T - k0)
         if chunk_hook is not None:
             chunk_hook(k0)
+        if host_io and k0 + K < T:
+            io.prefetch(k0 + K)
         xin, xp, slc = chunk_inputs(k0, kc)
         if not use_graph:
-            outs = {"raster": raster[k0], "z": z[k0] if z is not None else None,
-                    "stats": stat_t[k0] if stat_t is not None else None,
-                    **{kind: traces[kind][k0] for kind in trace_kinds}}
+            if host_io:
+                outs = io.device_outs(k0)
+            else:
+                outs = {"raster": raster[k0], "z": z[k0] if z is not None else None,
+                        "stats": stat_t[k0] if stat_t is not None else None,
+                        **{kind: traces[kind][k0] for kind in trace_kinds}}
             launches += launch(k0, kc, xin, xp, slc, outs, s)
+            if host_io:
+                io.consumed(k0)
+                io.drain(k0, kc)
             continue
         if "stats" in out_c:
             out_c["stats"].zero_()
@@ -487,9 +519,19 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             launches += nl
         else:
             launches += launch(k0, kc, xin, xp, slc, out_c, s)
+        if host_io:
+            io.consumed(k0)
+            dev_outs = io.device_outs(k0)
+            for kind, t in out_c.items():
+                if dev_outs.get(kind) is not None:
+                    dev_outs[kind][:kc].copy_(t[:kc])
+            io.drain(k0, kc)
+            continue
         for kind, t in out_c.items():
             if out_full.get(kind) is not None:
                 out_full[kind][k0:k0 + kc].copy_(t[:kc])
+    if host_io:
+        io.finish()
 
     if use_graph:
         v_mod.copy_(v)
@@ -531,8 +573,8 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     states = {}
     for key, kind in plan.paths.items():
         if kind == "history":
-            states[key] = _history_trace(plan.history, z if z is not None else _expand(raster, n), init_block,
-                                         batch_shape, None)
+            zz = z.to(dev) if z is not None else _expand(raster.to(dev), n)
+            states[key] = _history_trace(plan.history, zz, init_block, batch_shape, None).to(odev)
         elif kind == "psc_sum":
             states[key] = receptor_sum(traces["psc"].view(T, B, n, n_rec)).view(T, *batch_shape, *plan.neuron.n_neuron)
         else:
@@ -546,6 +588,79 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         z = z.view(T, *batch_shape, *neuron.n_neuron)
         return z, states
     return raster, states
+
+
+_COPY_STREAMS: dict = {}
+
+
+class _HostStreams:
+    """Chunked host <-> device streaming of one call with host-resident input.
+
+    Input chunk c (steps k0 .. k0 + K) goes host -> device on a copy stream
+    into one of two device staging buffers while the previous chunk computes;
+    the compute stream waits for it (take) and frees the buffer once the
+    chunk's launches are enqueued (consumed).  Each chunk's outputs land in one
+    of two chunk-sized device buffers and go device -> host on the copy stream
+    (drain), the compute stream waiting before it reuses a buffer.  Device
+    memory is two chunks' worth whatever T."""
+
+    def __init__(self, dev, x3, K, T, outs):
+        self.dev, self.x3, self.K, self.T = dev, x3, K, T
+        z, raster, stat_t, traces = outs
+        self.host = {"raster": raster, "z": z, "stats": stat_t, **traces}
+        self.cs = _COPY_STREAMS.get(dev)
+        if self.cs is None:
+            self.cs = _COPY_STREAMS[dev] = torch.cuda.Stream(dev)
+        shape = (K,) + tuple(x3.shape[1:])
+        self.stg = [torch.empty(shape, device=dev, dtype=x3.dtype) for _ in range(2)]
+        self.dout = [{k: torch.empty((K,) + tuple(h.shape[1:]), device=dev, dtype=h.dtype)
+                      for k, h in self.host.items() if h is not None} for _ in range(2)]
+        self.ev_in, self.ev_free, self.ev_out_free = [None, None], [None, None], [None, None]
+
+    def _par(self, k0):
+        return (k0 // self.K) & 1
+
+    def prefetch(self, k0):
+        p = self._par(k0)
+        kc = min(self.K, self.T - k0)
+        with torch.cuda.stream(self.cs):
+            if self.ev_free[p] is not None:
+                self.cs.wait_event(self.ev_free[p])
+            self.stg[p][:kc].copy_(self.x3[k0:k0 + kc], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(self.cs)
+            self.ev_in[p] = ev
+
+    def take(self, k0):
+        p = self._par(k0)
+        torch.cuda.current_stream(self.dev).wait_event(self.ev_in[p])
+        return self.stg[p]
+
+    def consumed(self, k0):
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(self.dev))
+        self.ev_free[self._par(k0)] = ev
+
+    def device_outs(self, k0):
+        p = self._par(k0)
+        if self.ev_out_free[p] is not None:
+            torch.cuda.current_stream(self.dev).wait_event(self.ev_out_free[p])
+        return self.dout[p]
+
+    def drain(self, k0, kc):
+        p = self._par(k0)
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(self.dev))
+        with torch.cuda.stream(self.cs):
+            self.cs.wait_event(ev)
+            for k, d in self.dout[p].items():
+                self.host[k][k0:k0 + kc].copy_(d[:kc], non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(self.cs)
+        self.ev_out_free[p] = done
+
+    def finish(self):
+        self.cs.synchronize()  # host outputs complete; staging buffers idle
 
 
 def _graph_signature(desc, *tensors):

@@ -192,10 +192,11 @@ class RecurrentNN(RecurrentNNAbstract):
             or any(torch.is_tensor(a) and a.requires_grad for a in args))
         extra = len(args) > 1 and any(a is not None for a in args[1:])
         plan, reason = (None, "disabled")
-        if self.cudagraph:
-            CudaGraphRunner.check_supported(self, args)
         if self.fused and not needs_grad and not extra and not kwargs and loop_args in (None, (0,)):
             plan, reason = _engine.match(self)
+        if self.cudagraph and plan is None:
+            # (the fused engine also takes host-resident input, streamed in chunks)
+            CudaGraphRunner.check_supported(self, args)
         if plan is not None:
             self.last_path = "fused"
             return _engine.run(plan, self, args[0], sample_len=sample_len, chunk=engine_chunk,

@@ -98,3 +98,30 @@ def test_graph_refuses_gradients():
     x = torch.tensor(d["x"], device=DEV, requires_grad=True)
     with pytest.raises(RuntimeError, match="inference-only"):
         rnn(x)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("name", ["lif_dyadic_input", "hetero_delay"])
+def test_host_input_streams_equal_device_input(name, graph):
+    """Host-resident input (pinned or not): chunks stream to the device on a
+    copy stream and the outputs stream back; results equal the device-input
+    run bit for bit, outputs on the host."""
+    d = cases.load(name)
+    outs = {}
+    for where in ("cuda", "cpu", "pinned"):
+        rnn, _ = cases.build_model(d, DEV, "scatter")
+        rnn.cudagraph = graph
+        x = torch.tensor(d["x"])
+        x = x.to(DEV) if where == "cuda" else (x.pin_memory() if where == "pinned" else x)
+        with torch.no_grad(), environ.context(dt=float(d["dt"])):
+            z, st = rnn(x, engine_chunk=24, engine_stats=True)
+            stats = rnn.last_engine_stats.cpu().numpy()
+            r, _ = rnn(x[:50], spikes_out="bitmask", engine_chunk=24)
+        assert z.device.type == ("cuda" if where == "cuda" else "cpu")
+        assert r.device.type == z.device.type
+        outs[where] = (z.cpu().numpy(), st["neuron.v"].cpu().numpy(), stats, r.cpu().numpy(),
+                       rnn.neuron.v.cpu().numpy())
+    for where in ("cpu", "pinned"):
+        for a, b in zip(outs["cuda"], outs[where]):
+            np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(outs["cuda"][0].astype(np.uint8), cases.spikes(d))
