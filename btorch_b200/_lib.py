@@ -81,6 +81,7 @@ _PROTOS = {
     "bt_engine_run": (C.c_int, [C.POINTER(BtEngineDesc), _vp]),
     "bt_engine_prime": (C.c_int, [C.POINTER(BtEngineDesc), _vp]),
     "bt_input_project": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "bt_input_project_live": (C.c_int, [_i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_bits_to_float": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
     "bt_float_to_bits": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
     "bt_raster_count": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),

@@ -250,19 +250,24 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   int64_t lenv[S];
   const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
   const int n32 = int(n);  // batch * n < 2^31 in scatter mode (checked on the host)
-  // every load before the first store: a load behind a store through a
-  // pointer that may alias it waits for the store
+  // Every load before the first store: a load behind a store through a
+  // pointer that may alias it waits for the store.  A sample past its length
+  // (k > len) reads and writes no state unless state traces are requested:
+  // its state is frozen and its accumulator is not read again in this call.
+  const bool st_traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace;
+#pragma unroll
+  for (int u = 0; u < S; ++u) lenv[u] = (valid && u < nb && d.sample_len) ? d.sample_len[b0 + u] : INT64_MAX;
 #pragma unroll
   for (int u = 0; u < S; ++u) {
     const bool in = valid && u < nb;
+    const bool live = in && k < lenv[u], edge = in && k <= lenv[u], frozen = in && st_traces;
     const int o = u * n32;
-    lenv[u] = (in && d.sample_len) ? d.sample_len[b0 + u] : INT64_MAX;
-    pend[u] = in ? ld_f32(ring_p + o, pol_keep) : 0.0f;
-    pv[u] = in ? psc_p[o] : 0.0f;
-    xv[u] = (in && x_p) ? ld_nc_f32(x_p + o, pol_stream) : 0.0f;
-    vv[u] = in ? v_p[o] : 0.0f;
-    rv[u] = (in && USE_REF) ? ref_p[o] : 0.0f;
-    gv[u] = (in && KIND == BT_NEURON_ALIF) ? gk_p[o] : 0.0f;
+    pend[u] = edge ? ld_f32(ring_p + o, pol_keep) : 0.0f;
+    pv[u] = (edge || frozen) ? psc_p[o] : 0.0f;
+    xv[u] = (live && x_p) ? ld_nc_f32(x_p + o, pol_stream) : 0.0f;
+    vv[u] = (live || frozen) ? v_p[o] : 0.0f;
+    rv[u] = ((live || frozen) && USE_REF) ? ref_p[o] : 0.0f;
+    gv[u] = ((live || frozen) && KIND == BT_NEURON_ALIF) ? gk_p[o] : 0.0f;
   }
   const int64_t ip = valid ? i : 0;
   const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, ip);
@@ -280,8 +285,8 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
     const int o = u * n32;
     float s = 0.0f;
     if (valid) {
-      st_f32(ring_p + o, 0.0f, pol_keep);
       const int64_t len = lenv[u];
+      if (k <= len) st_f32(ring_p + o, 0.0f, pol_keep);
       float v = vv[u], ref = rv[u], gk = gv[u];
       float P;
       if (k < len) {
@@ -341,7 +346,9 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron_rec(bt_engine_desc d
   const int64_t b = blockIdx.y;
   if ((i & ~int64_t(31)) >= n) return;  // whole warps past the last word
   float s = 0.0f;
-  if (i < n) {
+  const int64_t len = (i < n && d.sample_len) ? d.sample_len[b] : INT64_MAX;
+  const bool st_traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace;
+  if (i < n && (k <= len || st_traces)) {  // else: past its length, nothing to read or write
     const int64_t idx = b * n + i, c0 = b * nc + i * C;
     float* __restrict__ ring = d.ring + c0;
     float* __restrict__ psc = d.psc + c0;
@@ -367,7 +374,6 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron_rec(bt_engine_desc d
       pc[r] = d.psc_uniform ? d.psc_coef_s : ld(d.psc_coef, i * C + r);
       pt[r] = d.psc_uniform ? d.psc_tau_s : ld(d.psc_tau, i * C + r);
     }
-    const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
     float v = d.v[idx];
     float ref = USE_REF ? d.refractory[idx] : 0.0f;
     float gk = KIND == BT_NEURON_ALIF ? d.g_k[idx] : 0.0f;
@@ -432,8 +438,8 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron_rec(bt_engine_desc d
     if (d.v_trace) d.v_trace[tix] = v;
     if (USE_REF && d.ref_trace) d.ref_trace[tix] = ref;
     if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[tix] = gk;
-    if (d.spikes) d.spikes[tix] = s;
   }
+  if (i < n && d.spikes) d.spikes[(k * B + b) * n + i] = s;
   const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
   if (lane_id() == 0) {
     d.hist[(int64_t(si.h_t) * B + b) * words + (i >> 5)] = word;
@@ -1272,12 +1278,18 @@ __global__ void k_prime_history(bt_engine_desc d) {
 // ------------------------------------------------------- input projection --
 
 // Per row r: its nonzero inputs as (channel, value) pairs in ascending channel
-// order (warp ballot + prefix), and their count.
+// order (warp ballot + prefix), and their count.  With live_len, row
+// r = t * batch + b of a sample past its length (t >= live_len[b]) gets
+// count -1 and no pairs: nothing reads its projection.
 __global__ void k_row_pairs(int64_t rows, int64_t c_in, const float* __restrict__ xin, int32_t* __restrict__ cnt,
-                            int2* __restrict__ pairs) {
+                            int2* __restrict__ pairs, const int32_t* __restrict__ live_len, int64_t batch) {
   const int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   if (r >= rows) return;
   const unsigned lane = lane_id();
+  if (live_len && r / batch >= __ldg(live_len + r % batch)) {  // warp-uniform
+    if (lane == 0) cnt[r] = -1;
+    return;
+  }
   int32_t total = 0;
   for (int64_t c0 = 0; c0 < c_in; c0 += 32) {
     const int64_t c = c0 + lane;
@@ -1313,6 +1325,7 @@ __global__ void __launch_bounds__(256) k_input_project(int64_t rows, int64_t c_i
   }
   for (int64_t r = r0; r < r0 + kProjRows && r < rows; ++r) {
     const int32_t c_n = cnt[r];
+    if (c_n < 0) continue;  // a finished sample's step: left unwritten
     const int2* rp = pairs + r * c_in;
     float acc[kProjNPT];
 #pragma unroll
@@ -1530,8 +1543,9 @@ extern "C" int bt_engine_prime(const bt_engine_desc* d, void* stream) {
   return BT_OK;
 }
 
-extern "C" int bt_input_project(int64_t rows, int64_t c_in, int64_t n, const float* xin, const float* w_t,
-                                const float* bias, float* out, int32_t* work, void* stream) {
+namespace {
+int input_project(int64_t rows, int64_t c_in, int64_t n, const float* xin, const float* w_t, const float* bias,
+                  float* out, int32_t* work, const int32_t* live_len, int64_t batch, void* stream) {
   BT_CHECK_ARG(rows >= 0 && c_in >= 0 && n >= 0, "negative size");
   if (rows == 0 || n == 0) return BT_OK;
   BT_CHECK_ARG(xin && w_t && out && work, "null pointer");
@@ -1540,13 +1554,26 @@ extern "C" int bt_input_project(int64_t rows, int64_t c_in, int64_t n, const flo
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int2* pairs = reinterpret_cast<int2*>(work);
   int32_t* cnt = work + 2 * rows * c_in;
-  k_row_pairs<<<int(ceil_div(rows * 32, 256)), 256, 0, s>>>(rows, c_in, xin, cnt, pairs);
+  k_row_pairs<<<int(ceil_div(rows * 32, 256)), 256, 0, s>>>(rows, c_in, xin, cnt, pairs, live_len, batch);
   BT_CHECK_LAUNCH("k_row_pairs");
   dim3 grid(unsigned(ceil_div(rows, kProjRows)), unsigned(ceil_div(n, 256 * kProjNPT)));
   BT_CHECK_ARG(grid.y < 65536 && grid.x < (1u << 31), "projection grid too large");
   k_input_project<<<grid, 256, 0, s>>>(rows, c_in, n, w_t, bias, cnt, pairs, out);
   BT_CHECK_LAUNCH("k_input_project");
   return BT_OK;
+}
+}  // namespace
+
+extern "C" int bt_input_project(int64_t rows, int64_t c_in, int64_t n, const float* xin, const float* w_t,
+                                const float* bias, float* out, int32_t* work, void* stream) {
+  return input_project(rows, c_in, n, xin, w_t, bias, out, work, nullptr, 1, stream);
+}
+
+extern "C" int bt_input_project_live(int64_t steps, int64_t batch, int64_t c_in, int64_t n, const float* xin,
+                                     const float* w_t, const float* bias, const int32_t* sample_len, float* out,
+                                     int32_t* work, void* stream) {
+  BT_CHECK_ARG(steps >= 0 && batch > 0, "bad steps / batch");
+  return input_project(steps * batch, c_in, n, xin, w_t, bias, out, work, sample_len, batch, stream);
 }
 
 extern "C" int bt_bits_to_float(int64_t rows, int64_t n, const uint32_t* bits, float* out, void* stream) {

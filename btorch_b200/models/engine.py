@@ -457,8 +457,13 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
                 torch.empty(kc * B * (2 * c_in + 1), device=dev, dtype=torch.int32)
             keep.append(pw)
             e0 = _ev() if profile is not None else None
-            L.check(L.lib().bt_input_project(kc * B, c_in, n, xin.data_ptr(), w_t.data_ptr(), L.ptr(bias),
-                                             xp.data_ptr(), pw.data_ptr(), stream), "bt_input_project")
+            if slc is not None:  # finished samples' steps are not projected
+                L.check(L.lib().bt_input_project_live(kc, B, c_in, n, xin.data_ptr(), w_t.data_ptr(), L.ptr(bias),
+                                                      slc.data_ptr(), xp.data_ptr(), pw.data_ptr(), stream),
+                        "bt_input_project_live")
+            else:
+                L.check(L.lib().bt_input_project(kc * B, c_in, n, xin.data_ptr(), w_t.data_ptr(), L.ptr(bias),
+                                                 xp.data_ptr(), pw.data_ptr(), stream), "bt_input_project")
             nl += 2
             if profile is not None:
                 profile.append(("project", e0, _ev()))

@@ -376,6 +376,14 @@ BT_API int bt_input_project(int64_t rows, int64_t c_in, int64_t n,
                      const float* xin, const float* w_t, const float* bias,
                      float* out, int32_t* work, void* stream);
 
+/* bt_input_project over steps * batch rows (row t * batch + b) that skips the
+ * steps of finished samples: rows with t >= sample_len[b] (this call's steps,
+ * as bt_engine_desc.sample_len) are neither scanned nor written -- the engine
+ * does not read them.  Same work scratch. */
+BT_API int bt_input_project_live(int64_t steps, int64_t batch, int64_t c_in, int64_t n,
+                     const float* xin, const float* w_t, const float* bias,
+                     const int32_t* sample_len, float* out, int32_t* work, void* stream);
+
 /* Expand spike bitmaps [rows][words] to fp32 [rows][n] (words = ceil(n/32),
  * bit i%32 of word i/32 is neuron i). */
 BT_API int bt_bits_to_float(int64_t rows, int64_t n, const uint32_t* bits,

@@ -1,6 +1,7 @@
 """GPU parity: the sm_100a kernels against the reference's golden vectors and
 the CPU oracle, through the module API (which calls the C ABI)."""
 
+import operator
 import numpy as np
 import pytest
 import torch
@@ -234,3 +235,33 @@ def test_engine_state_names_default_all_memories(direction):
     assert sorted(st_f) == sorted(st_m)
     for k in st_f:
         torch.testing.assert_close(st_f[k], st_m[k], rtol=0, atol=0, msg=k)
+
+
+@pytest.mark.parametrize("direction", MODES)
+@pytest.mark.parametrize("name", ["lif_dyadic_input", "hetero_delay"])
+def test_uneven_lengths_without_traces(name, direction):
+    """Per-sample lengths with no state traces requested (finished samples are
+    then neither read nor written, and their projected input rows are not
+    computed): every sample's raster and final state (v, psc) equal the same
+    sample run alone for its length, and spikes after its end are zero."""
+    d = cases.load(name)
+    B = int(d["batch"])
+    T = d["x"].shape[0]
+    lens = [T, 31, 1, 77][:B]
+    rnn, psc_name = cases.build_model(d, DEV, direction)
+    rnn.update_state_names = ()
+    x = torch.tensor(d["x"], device=DEV)
+    with torch.no_grad(), environ.context(dt=float(d["dt"])):
+        z, _ = rnn(x, sample_len=torch.tensor(lens))
+    z = z.cpu().numpy()
+    v = rnn.neuron.v.cpu().numpy()
+    psc = operator.attrgetter(psc_name)(rnn).cpu().numpy()
+    for b, L in enumerate(lens):
+        alone, _ = cases.build_model(dict(d, batch=np.int64(1)), DEV, direction)
+        alone.update_state_names = ()
+        with torch.no_grad(), environ.context(dt=float(d["dt"])):
+            za, _ = alone(x[:L, b:b + 1])
+        np.testing.assert_array_equal(z[:L, b], za.cpu().numpy()[:, 0], err_msg=f"sample {b}")
+        assert z[L:, b].sum() == 0
+        np.testing.assert_array_equal(v[b], alone.neuron.v.cpu().numpy()[0])
+        np.testing.assert_array_equal(psc[b], operator.attrgetter(psc_name)(alone).cpu().numpy()[0])
