@@ -41,6 +41,7 @@
 // the receptor sum of its C channels (receptor_sum, the reference's
 // psc.reshape(..., n, C).sum(-1) rounding).  Scatter and gather modes.
 #include <algorithm>
+#include <cstring>
 #include <type_traits>
 
 #include "neuron.cuh"
@@ -229,7 +230,7 @@ __device__ __forceinline__ void publish_spikes(const bt_engine_desc& d, const St
 // consecutive samples; a warp covers one 32-neuron bitmap word of each of
 // them.  All S samples' state is loaded before any is updated (memory-level
 // parallelism), and the neuron's parameters are read once for the S samples.
-template <int KIND, bool HARD, bool USE_REF, int S>
+template <int KIND, bool HARD, bool USE_REF, int S, bool FAST>
 __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, int64_t k, StepIdx si) {
   const int64_t n = d.n, B = d.batch;
   const int64_t words = (n + 31) >> 5;
@@ -292,12 +293,12 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
       if (k < len) {
         P = add(pv[u], pend[u]);
         const float I = x_p ? add(P, xv[u]) : P;
-        const NeuronOut out = neuron_update<KIND, HARD, USE_REF, true>(prm, I, v, ref, gk);
+        const NeuronOut out = neuron_update<KIND, HARD, USE_REF, true, FAST>(prm, I, v, ref, gk);
         s = out.spike;
         v_p[o] = v;
         if (USE_REF) ref_p[o] = ref;
         if (KIND == BT_NEURON_ALIF) gk_p[o] = gk;
-        psc_p[o] = psc_decay(pc, dpt, P);
+        psc_p[o] = psc_decay_k<FAST>(pc, dpt, P);
       } else {
         // Finished sample: its state freezes at its last step.  On the first
         // step past the end the pending sum completes psc of that last step;
@@ -1410,6 +1411,25 @@ int engine_check(const bt_engine_desc* d) {
   return BT_OK;
 }
 
+// The device's Div kind of divisor c (neuron.cuh make_div) is 1 or 2.
+bool fast_divisor(float c, bool verified) {
+  uint32_t u;
+  std::memcpy(&u, &c, sizeof(u));
+  const uint32_t e = u >> 23;
+  return ((u & 0x7fffffu) == 0u && e >= 1u && e <= 253u) || verified;
+}
+
+// Uniform scalar parameters whose divisions all avoid the IEEE path.
+bool fast_divisors(const bt_engine_desc& d, int kind) {
+  const bt_neuron_desc& nd = d.neuron;
+  if (!nd.uniform || !d.psc_uniform) return false;
+  const float den = nd.sv[0] - nd.sv[1];  // v_threshold - v_reset, as the device computes it
+  bool ok = fast_divisor(nd.sv[2], nd.fast_div & 1) && fast_divisor(den, nd.fast_div & 2) &&
+            fast_divisor(d.psc_tau_s, d.psc_fast_div != 0);
+  ok = ok && (kind == BT_NEURON_LIF ? fast_divisor(nd.sv[3], nd.fast_div & 4) : fast_divisor(nd.sv[9], nd.fast_div & 8));
+  return ok;
+}
+
 template <int KIND, bool HARD, bool USE_REF>
 int run_typed(const bt_engine_desc& d, cudaStream_t s) {
   const int64_t n = d.n;
@@ -1427,8 +1447,12 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
     const int64_t xblocks = std::min(ceil_div(int64_t(sms) * 8, planes), ceil_div(n, rows_per_block));
     const dim3 sgrid(unsigned(std::max<int64_t>(xblocks, 1)), planes);
     const int ms = mask_stride(d.batch);
-    auto neuron = S == 1 ? k_eng_neuron<KIND, HARD, USE_REF, 1>
-                : S == 2 ? k_eng_neuron<KIND, HARD, USE_REF, 2> : k_eng_neuron<KIND, HARD, USE_REF, 4>;
+    // every divisor a power of two or a verified reciprocal: no IEEE division compiled in
+    const bool fast = fast_divisors(d, KIND);
+    auto neuron = fast ? (S == 1 ? k_eng_neuron<KIND, HARD, USE_REF, 1, true>
+                          : S == 2 ? k_eng_neuron<KIND, HARD, USE_REF, 2, true> : k_eng_neuron<KIND, HARD, USE_REF, 4, true>)
+                       : (S == 1 ? k_eng_neuron<KIND, HARD, USE_REF, 1, false>
+                          : S == 2 ? k_eng_neuron<KIND, HARD, USE_REF, 2, false> : k_eng_neuron<KIND, HARD, USE_REF, 4, false>);
     auto pick = [&](auto g) {
       constexpr int G = decltype(g)::value;
       // MS >= ms: mask_stride gives 1, 2, 4, or 5..8 words (MS = 8)

@@ -80,6 +80,17 @@ __device__ __forceinline__ float divc(float x, const Div& d) {
   return d.kind == 1 ? mul(x, d.r) : d.kind == 2 ? div_recip(x, d.c, d.r) : div(x, d.c);
 }
 
+// divc for a launch whose divisors are all of kind 1 or 2 (FAST, decided on
+// the host from the parameter values): the IEEE-division branch is compiled
+// out, which shortens the per-sample update of the issue-bound neuron steps.
+template <bool FAST>
+__device__ __forceinline__ float divk(float x, const Div& d) {
+  if constexpr (FAST)
+    return d.kind == 1 ? mul(x, d.r) : div_recip(x, d.c, d.r);
+  else
+    return divc(x, d);
+}
+
 // The parameters of one neuron, read once into registers (the kernels update
 // many samples of the same neuron with them).
 struct NeuronParams {
@@ -150,29 +161,29 @@ __device__ __forceinline__ NeuronParams load_params(const bt_neuron_desc& d, int
 // One BaseNode.single_step_forward with input current I.  v, ref, gk are
 // updated in place.  SPIKING selects the Heaviside forward at compile time
 // (the fused engine); otherwise pr.spiking decides at run time.
-template <int KIND, bool HARD, bool USE_REF, bool SPIKING = false>
+template <int KIND, bool HARD, bool USE_REF, bool SPIKING = false, bool FAST = false>
 __device__ __forceinline__ NeuronOut neuron_update(const NeuronParams& pr, float I, float& v, float& ref, float& gk) {
   const float dt = pr.dt;
   float v1;
   if (KIND == BT_NEURON_LIF) {
     // euler_step(dV): v + dt * ((-(v - v_reset)) / tau + x / c_m)
-    v1 = add(v, mul(dt, add(divc(-sub(v, pr.vr), pr.d_tau), divc(I, pr.d_cm))));
+    v1 = add(v, mul(dt, add(divk<FAST>(-sub(v, pr.vr), pr.d_tau), divk<FAST>(I, pr.d_cm))));
   } else {
     // exp_euler_step(dV): derivative = ((-g_leak)(v - E_leak) + (-g_k)(v - E_k) + x) / c_m
     //                     linear     = ((-g_leak) - g_k) / c_m
     const float leak = mul(pr.ngl, sub(v, pr.El));
     const float adapt = mul(-gk, sub(v, pr.Ek));
-    const float deriv = divc(add(add(leak, adapt), I), pr.d_cm);
-    const float lin = divc(sub(pr.ngl, gk), pr.d_cm);
+    const float deriv = divk<FAST>(add(add(leak, adapt), I), pr.d_cm);
+    const float lin = divk<FAST>(sub(pr.ngl, gk), pr.d_cm);
     const float coef = div(expm1f(mul(dt, lin)), lin);
     v1 = add(v, mul(coef, deriv));
     // neuronal_adaptation: g_k + coef_gk * ((-g_k) / tau_adapt)
-    gk = add(gk, mul(pr.cgk, divc(-gk, pr.d_tau_a)));
+    gk = add(gk, mul(pr.cgk, divk<FAST>(-gk, pr.d_tau_a)));
   }
   NeuronOut o;
   o.v_charged = v1;
   // neuronal_fire: surrogate((v - v_th) / (v_th - v_reset)) * (refractory == 0)
-  o.u = divc(sub(v1, pr.vth), pr.d_den);
+  o.u = divk<FAST>(sub(v1, pr.vth), pr.d_den);
   float s;
   if (SPIKING || pr.spiking)
     s = o.u >= 0.0f ? 1.0f : 0.0f;
@@ -208,6 +219,10 @@ __device__ __forceinline__ float psc_decay(float coef, float tau, float rtau, fl
 }
 __device__ __forceinline__ float psc_decay(float coef, const Div& tau, float p) {
   return add(p, mul(coef, divc(-p, tau)));
+}
+template <bool FAST>
+__device__ __forceinline__ float psc_decay_k(float coef, const Div& tau, float p) {
+  return add(p, mul(coef, divk<FAST>(-p, tau)));
 }
 __device__ __forceinline__ float psc_decay(float coef, float tau, float p) {
   return psc_decay(coef, tau, pow2_recip(tau), p);
