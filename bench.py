@@ -100,7 +100,24 @@ def parse():
     ap.add_argument("--ncu-window", type=int, default=None,
                     help="profile only time steps [S, S+64) (S a multiple of 64) of one extra batch after "
                          "the timed ones (cudaProfilerStart/Stop; use with ncu --profile-from-start off)")
+    ap.add_argument("--engine-choice", default=None,
+                    help="run the headline workload with this engine choice instead of the tuner's, e.g. "
+                         "'scatter,spt=2,lanes=1' (profiling: the tuner's timings differ under a profiler)")
     return ap.parse_args()
+
+
+def parse_choice(text):
+    """'scatter,spt=2,lanes=1' / 'gather' / 'pull,words=2' -> autotune.EngineChoice."""
+    if not text:
+        return None
+    from btorch_b200 import _lib as L
+    from btorch_b200.models.autotune import EngineChoice
+
+    mode, *kv = text.split(",")
+    f = dict(item.split("=") for item in kv)
+    modes = {"scatter": L.BT_MODE_SCATTER, "gather": L.BT_MODE_GATHER, "pull": L.BT_MODE_PULL}
+    return EngineChoice(modes[mode], neuron_spt=int(f.get("spt", 0)), scatter_lanes=int(f.get("lanes", 0)),
+                        pull_words=int(f.get("words", 0)), dense_rows=int(f.get("dense", -1)))
 
 
 # ------------------------------------------------------------- workload --
@@ -586,6 +603,7 @@ def measure(name, cfg, args, dev, world, rank, local):
     from btorch_b200.models.functional import reset_net
 
     net = make_network(cfg, args.seed)
+    forced = parse_choice(args.engine_choice) if name == args.config else None
     rnn = build_model(cfg, net, dev, args.direction)
     rnn.cudagraph = not args.no_cudagraph
     x, lens = make_inputs(cfg, args.seed + rank, dev)
@@ -594,7 +612,8 @@ def measure(name, cfg, args, dev, world, rank, local):
     def one_step(xx, profile=None):
         reset_net(rnn, inplace=True)
         with torch.inference_mode(), environ.context(dt=1.0):
-            raster, _ = rnn(xx, sample_len=lens, spikes_out="bitmask", engine_stats=True, engine_profile=profile)
+            raster, _ = rnn(xx, sample_len=lens, spikes_out="bitmask", engine_stats=True, engine_profile=profile,
+                            engine_choice=forced)
         return raster
 
     for _ in range(max(3, args.warmup)):
@@ -767,7 +786,8 @@ def main():
         reset_net(rnn, inplace=True)
         rnn.cudagraph = False
         with torch.inference_mode(), environ.context(dt=1.0):
-            rnn(x, sample_len=lens, spikes_out="bitmask", engine_chunk=64, engine_chunk_hook=hook)
+            rnn(x, sample_len=lens, spikes_out="bitmask", engine_chunk=64, engine_chunk_hook=hook,
+                engine_choice=parse_choice(args.engine_choice))
         torch.cuda.synchronize()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         S = args.cpu_sample_steps

@@ -181,12 +181,14 @@ class RecurrentNN(RecurrentNNAbstract):
 
     def multi_step_forward(self, *args, loop_args=None, sample_len=None, spikes_out: str = "dense",
                            engine_chunk: int | None = None, engine_stats: bool = False,
-                           engine_profile: list | None = None, engine_chunk_hook=None, **kwargs):
+                           engine_profile: list | None = None, engine_chunk_hook=None, engine_choice=None,
+                           **kwargs):
         """Run T = args[0].shape[0] steps.  Extensions over the reference:
         sample_len ([batch] steps per sample; later steps of a sample freeze its
         state and emit no spikes), spikes_out="bitmask" (return the spike raster
         as [T, batch, ceil(n/32)] int32 words), engine_stats (record per-step
-        active counts in self.last_engine_stats)."""
+        active counts in self.last_engine_stats), engine_choice (an
+        autotune.EngineChoice to run instead of the tuner's)."""
         needs_grad = torch.is_grad_enabled() and (
             any(p.requires_grad for p in self.parameters())
             or any(torch.is_tensor(a) and a.requires_grad for a in args))
@@ -201,7 +203,7 @@ class RecurrentNN(RecurrentNNAbstract):
             self.last_path = "fused"
             return _engine.run(plan, self, args[0], sample_len=sample_len, chunk=engine_chunk,
                                spikes_out=spikes_out, stats=engine_stats, profile=engine_profile,
-                               chunk_hook=engine_chunk_hook)
+                               chunk_hook=engine_chunk_hook, choice=engine_choice)
         if sample_len is not None or spikes_out != "dense":
             raise NotImplementedError(f"sample_len / spikes_out need the fused engine ({reason})")
         self.last_fused_reason = reason

@@ -47,3 +47,20 @@ def test_tuned_run_equals_untuned(name, direction):
             assert best.mode in autotune.allowed_modes(conn, int(d["batch"]))
     for a, b in zip(outs[False], outs[True]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_explicit_engine_choice_is_used():
+    """engine_choice= bypasses the tuner: the run uses it and equals the tuned run."""
+    from btorch_b200 import _lib as L
+
+    d = cases.load("lif_dyadic_input")
+    x = torch.tensor(d["x"], device=DEV)
+    outs = []
+    for choice in (None, autotune.EngineChoice(L.BT_MODE_SCATTER, neuron_spt=1, scatter_lanes=8)):
+        rnn, _ = cases.build_model(d, DEV, "scatter")
+        with torch.no_grad(), environ.context(dt=float(d["dt"])):
+            z, _ = rnn(x, engine_choice=choice)
+        if choice is not None:
+            assert rnn.last_engine_choice == choice
+        outs.append(z.cpu().numpy())
+    np.testing.assert_array_equal(outs[0], outs[1])
