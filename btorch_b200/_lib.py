@@ -72,6 +72,7 @@ _PROTOS = {
     "bt_spmv_scatter": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_spmv_gather_noalloc": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_spmv_grad_input": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "bt_spmv_grad_input_t": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_spmv_grad_weight": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_check_neuron_desc": (C.c_int, [C.POINTER(BtNeuronDesc)]),
     "bt_fast_div_check": (C.c_int, [C.c_float, C.c_float, _vp, _vp]),

@@ -133,15 +133,87 @@ __global__ void k_spmv_grad_input(int64_t batch, int64_t n_in, int64_t n_out,
   }
 }
 
-// masks[j][q] bit l <=> x[32 q + l][j] != 0.  One thread per source.
+// out[c][r] = in[r][c] for an rows x cols fp32 matrix, through 32 x 32
+// shared-memory tiles (block 32 x 8: coalesced reads and writes).
+__global__ void k_transpose(int64_t rows, int64_t cols, const float* __restrict__ in, float* __restrict__ out) {
+  __shared__ float tile[32][33];
+  const int64_t c0 = int64_t(blockIdx.x) * 32, r0 = int64_t(blockIdx.y) * 32;
+#pragma unroll
+  for (int k = 0; k < 32; k += 8) {
+    const int64_t r = r0 + threadIdx.y + k, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) tile[threadIdx.y + k][threadIdx.x] = in[r * cols + c];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 32; k += 8) {
+    const int64_t c = c0 + threadIdx.y + k, r = r0 + threadIdx.x;
+    if (r < rows && c < cols) out[c * rows + r] = tile[threadIdx.x][threadIdx.y + k];
+  }
+}
+
+// grad_x[b][j] = sum over j's out-edges e in CSR order of w_e * g[b][dst_e],
+// read from gT = g transposed ([n_out][batch]): one warp per source j, lane =
+// V consecutive samples, so every edge reads one contiguous run of gT (a
+// 512-byte row for 128 samples) instead of one scattered word per sample.
+// The warp loads 32 edges at a time and broadcasts them in order; each
+// (b, j) is an fmaf chain in ascending edge order (deterministic).
+template <int V>
+__global__ void k_spmv_grad_input_t(int64_t batch, int64_t n_in, const int32_t* __restrict__ csr_ptr,
+                                    const uint32_t* __restrict__ csr_dst, const float* __restrict__ csr_w,
+                                    const float* __restrict__ gT, float* __restrict__ gx) {
+  const int64_t j = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (j >= n_in) return;
+  const unsigned lane = lane_id();
+  const int32_t beg = csr_ptr[j], end = csr_ptr[j + 1];
+  for (int64_t b0 = 0; b0 < batch; b0 += 32 * V) {
+    const int64_t bl = b0 + int64_t(lane) * V;  // this lane's first sample
+    float acc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = 0.0f;
+    for (int32_t base = beg; base < end; base += 32) {
+      const int32_t e = base + int32_t(lane);
+      const uint32_t dst = e < end ? (__ldg(csr_dst + e) & kIdMask) : 0u;
+      const float w = e < end ? __ldg(csr_w + e) : 0.0f;
+      const int cnt = end - base < 32 ? end - base : 32;
+#pragma unroll 4
+      for (int q = 0; q < cnt; ++q) {
+        const uint32_t dq = __shfl_sync(0xffffffffu, dst, q);
+        const float wq = __shfl_sync(0xffffffffu, w, q);
+        const float* row = gT + int64_t(dq) * batch + bl;
+        if constexpr (V == 4) {
+          if (bl < batch) {
+            const float4 g4 = __ldg(reinterpret_cast<const float4*>(row));
+            acc[0] = fmaf(wq, g4.x, acc[0]);
+            acc[1] = fmaf(wq, g4.y, acc[1]);
+            acc[2] = fmaf(wq, g4.z, acc[2]);
+            acc[3] = fmaf(wq, g4.w, acc[3]);
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            if (bl + v < batch) acc[v] = fmaf(wq, __ldg(row + v), acc[v]);
+        }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+      if (bl + v < batch) gx[(bl + v) * n_in + j] = acc[v];
+  }
+}
+
+// masks[j][q] bit l <=> x[32 q + l][j] != 0.  One thread per source; the 32
+// samples of a word are loaded before any is tested.
 __global__ void k_source_masks(int64_t batch, int64_t n_in, int64_t mwords, const float* __restrict__ x,
                                uint32_t* __restrict__ masks) {
   const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (j >= n_in) return;
   for (int64_t q = 0; q < mwords; ++q) {
+    float xv[32];
+#pragma unroll
+    for (int l = 0; l < 32; ++l) xv[l] = q * 32 + l < batch ? x[(q * 32 + l) * n_in + j] : 0.0f;
     uint32_t m = 0;
-    for (int64_t l = 0; l < 32 && q * 32 + l < batch; ++l)
-      if (x[(q * 32 + l) * n_in + j] != 0.0f) m |= 1u << l;
+#pragma unroll
+    for (int l = 0; l < 32; ++l) m |= (xv[l] != 0.0f ? 1u : 0u) << l;
     masks[j * mwords + q] = m;
   }
 }
@@ -233,6 +305,29 @@ extern "C" int bt_spmv_grad_input(int64_t batch, int64_t n_in, int64_t n_out, co
   k_spmv_grad_input<<<grid_for_warps(n_in), 256, 0, s>>>(batch, n_in, n_out, csr_ptr, csr_dst, csr_w, grad_out,
                                                           grad_x);
   BT_CHECK_LAUNCH("k_spmv_grad_input");
+  return BT_OK;
+}
+
+extern "C" int bt_spmv_grad_input_t(int64_t batch, int64_t n_in, int64_t n_out, const int32_t* csr_ptr,
+                                    const uint32_t* csr_dst, const float* csr_w, const float* grad_out,
+                                    float* grad_x, float* work, void* stream) {
+  BT_CHECK_ARG(batch >= 0 && n_in >= 0 && n_out >= 0, "negative size");
+  if (batch == 0 || n_in == 0) return BT_OK;
+  BT_CHECK_ARG(csr_ptr && grad_out && grad_x && work, "null pointer");
+  BT_CHECK_ARG(n_out < (int64_t(1) << 31) / 32 * 32 && batch < (int64_t(1) << 31) / 32 * 32, "too large");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n_out > 0) {
+    const dim3 tgrid(unsigned(ceil_div(n_out, 32)), unsigned(ceil_div(batch, 32)));
+    BT_CHECK_ARG(tgrid.y < 65536, "batch too large for the transpose grid");
+    k_transpose<<<tgrid, dim3(32, 8), 0, s>>>(batch, n_out, grad_out, work);
+    BT_CHECK_LAUNCH("k_transpose");
+  }
+  // 16-byte sample runs need batch % 4 == 0 and an aligned transpose buffer
+  if (batch % 4 == 0 && (reinterpret_cast<uintptr_t>(work) & 15) == 0)
+    k_spmv_grad_input_t<4><<<grid_for_warps(n_in), 256, 0, s>>>(batch, n_in, csr_ptr, csr_dst, csr_w, work, grad_x);
+  else
+    k_spmv_grad_input_t<1><<<grid_for_warps(n_in), 256, 0, s>>>(batch, n_in, csr_ptr, csr_dst, csr_w, work, grad_x);
+  BT_CHECK_LAUNCH("k_spmv_grad_input_t");
   return BT_OK;
 }
 

@@ -161,9 +161,10 @@ class SparseMM(torch.autograd.Function):
         if ctx.needs_input_grad[0]:
             w_csr = ctx.w_csr if ctx.w_csr is not None else pack_csr_weights(layout, w_canon)
             gx = torch.empty_like(x)
-            L.check(L.lib().bt_spmv_grad_input(B, n_in, layout.n_out, layout.csr_ptr.data_ptr(),
-                                               layout.csr_dst.data_ptr(), w_csr.data_ptr(), g.data_ptr(),
-                                               gx.data_ptr(), s), "bt_spmv_grad_input")
+            gT = torch.empty(max(1, B * layout.n_out), device=g.device, dtype=torch.float32)
+            L.check(L.lib().bt_spmv_grad_input_t(B, n_in, layout.n_out, layout.csr_ptr.data_ptr(),
+                                                 layout.csr_dst.data_ptr(), w_csr.data_ptr(), g.data_ptr(),
+                                                 gx.data_ptr(), gT.data_ptr(), s), "bt_spmv_grad_input_t")
         if ctx.needs_input_grad[1]:
             gw = torch.empty(layout.nnz, device=g.device, dtype=torch.float32)
             masks = torch.empty(max(1, n_in * ((B + 31) // 32)), device=g.device, dtype=torch.int32)

@@ -146,6 +146,16 @@ BT_API int bt_spmv_grad_input(int64_t batch, int64_t n_in, int64_t n_out,
                        const float* csr_w, const float* grad_out,
                        float* grad_x, void* stream);
 
+/* The same product through grad_out transposed into `work` (batch * n_out
+ * floats, caller scratch): every edge then reads one contiguous run of
+ * samples instead of one scattered word per sample.  Each grad_x[b, j] is
+ * an fmaf chain over j's out-edges in CSR order (deterministic; rounding
+ * differs from bt_spmv_grad_input's lane-split sum). */
+BT_API int bt_spmv_grad_input_t(int64_t batch, int64_t n_in, int64_t n_out,
+                       const int32_t* csr_ptr, const uint32_t* csr_dst,
+                       const float* csr_w, const float* grad_out,
+                       float* grad_x, float* work, void* stream);
+
 /* grad_w[canonical e = (j -> i)] = sum_b x[b, j] * grad_out[b, i], over
  * stored nonzeros only and only over samples whose input x[b, j] is nonzero
  * (ascending b, fmaf); entries whose source is silent in every sample are

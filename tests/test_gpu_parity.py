@@ -265,3 +265,38 @@ def test_uneven_lengths_without_traces(name, direction):
         assert z[L:, b].sum() == 0
         np.testing.assert_array_equal(v[b], alone.neuron.v.cpu().numpy()[0])
         np.testing.assert_array_equal(psc[b], operator.attrgetter(psc_name)(alone).cpu().numpy()[0])
+
+
+@pytest.mark.parametrize("batch", [1, 37, 128, 200])
+def test_grad_input_transposed_matches_lane_split(batch):
+    """bt_spmv_grad_input_t (gradient transposed into scratch, one contiguous
+    sample run per edge) against bt_spmv_grad_input and a float64 product:
+    both fp32 sums within 1e-5, the transposed one deterministic."""
+    import scipy.sparse as sp
+
+    from btorch_b200 import _lib as L
+    from btorch_b200.models import SparseConn
+    from btorch_b200.models._ops import pack_csr_weights
+
+    rng = np.random.default_rng(batch)
+    n_in, n_out = 700, 900
+    W = sp.random(n_in, n_out, density=0.03, random_state=batch, dtype=np.float32)
+    m = SparseConn(sp.coo_array(W), enforce_dale=False).to(DEV)
+    lay = m.layout(DEV)
+    w_csr = pack_csr_weights(lay, m._get_effective_weight().detach())
+    g = torch.tensor(rng.standard_normal((batch, n_out)).astype(np.float32), device=DEV)
+    outs = []
+    s = L.stream_of(torch.device(DEV))
+    for fn in ("bt_spmv_grad_input", "bt_spmv_grad_input_t", "bt_spmv_grad_input_t"):
+        gx = torch.empty((batch, n_in), device=DEV)
+        args = [batch, n_in, n_out, lay.csr_ptr.data_ptr(), lay.csr_dst.data_ptr(), w_csr.data_ptr(), g.data_ptr(),
+                gx.data_ptr()]
+        if fn.endswith("_t"):
+            work = torch.empty(batch * n_out, device=DEV)
+            args.append(work.data_ptr())
+        L.check(getattr(L.lib(), fn)(*args, s), fn)
+        outs.append(gx.cpu().numpy())
+    want = g.cpu().numpy().astype(np.float64) @ W.toarray().astype(np.float64).T
+    np.testing.assert_allclose(outs[0], want, rtol=1e-5, atol=1e-5)
+    np.testing.assert_allclose(outs[1], want, rtol=1e-5, atol=1e-5)
+    np.testing.assert_array_equal(outs[1], outs[2])
