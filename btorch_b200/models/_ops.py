@@ -279,10 +279,39 @@ def fast_division(c: float, device) -> tuple[bool, float]:
     return _FAST_DIV[key], float(r32)
 
 
+_DESC_PARAMS = ("v_threshold", "v_reset", "c_m", "tau_ref", "g_leak", "E_leak", "E_k", "dg_k", "tau_adapt", "tau")
+
+
+def _desc_key(node, dt):
+    """What neuron_desc reads from `node`: parameter tensors by identity,
+    storage and version (no values, so no synchronisation), plus the flags."""
+    sg = node.surrogate_function
+    key = [float(dt), type(node), bool(node.hard_reset), bool(node._use_refractory),
+           getattr(sg, "spiking", True), getattr(sg, "slope", None), getattr(sg, "damping_factor", None)]
+    for name in _DESC_PARAMS:
+        t = getattr(node, name, None)
+        key.append((id(t), t.data_ptr(), _version(t), tuple(t.shape)) if torch.is_tensor(t) else t)
+    return tuple(key)
+
+
 def neuron_desc(node, dt: float):
     """bt_neuron_desc for an LIF/ALIF module; returns (desc, keepalive).  When
     every parameter is a scalar, their values are also passed by value
-    (desc.uniform), so the kernels read no parameter memory."""
+    (desc.uniform), so the kernels read no parameter memory.
+
+    Cached on the module until a parameter tensor is rebound, resized or
+    modified in place (its version counter), or dt or a flag changes: the
+    per-module path asks for it in every step's forward and backward."""
+    key = _desc_key(node, dt)
+    hit = node.__dict__.get("_bt_neuron_desc")
+    if hit is not None and hit[0] == key:
+        return hit[1], hit[2]
+    d, keep = _build_neuron_desc(node, dt)
+    node.__dict__["_bt_neuron_desc"] = (key, d, keep)
+    return d, keep
+
+
+def _build_neuron_desc(node, dt: float):
     from .neurons.alif import ALIF
     from .neurons.lif import LIF
 

@@ -146,3 +146,27 @@ def test_engine_plan_matching_on_cpu_modules():
     rnn2 = RecurrentNN(LIF(n), ExponentialPSC(n, 5.0, torch.nn.Linear(n, n)))
     plan2, why2 = rnn2.fused_plan()
     assert plan2 is None and "SparseConn" in why2
+
+
+def test_neuron_desc_cache_follows_parameter_changes():
+    """The per-module path's neuron descriptor is cached on the module and
+    rebuilt when a parameter is modified in place, rebound, or dt changes."""
+    import torch
+
+    from btorch_b200.models import ALIF, LIF
+    from btorch_b200.models._ops import neuron_desc
+
+    for cls in (LIF, ALIF):
+        m = cls(8, v_threshold=1.0, tau_ref=2.0)
+        d1, _ = neuron_desc(m, 1.0)
+        d2, _ = neuron_desc(m, 1.0)
+        assert d1 is d2
+        assert neuron_desc(m, 0.5)[0] is not d1
+        d3, _ = neuron_desc(m, 1.0)
+        with torch.no_grad():
+            m.v_threshold.fill_(2.0)
+        d4, _ = neuron_desc(m, 1.0)
+        assert d4 is not d3 and d4.sv[0] == 2.0
+        m.v_threshold = torch.tensor(3.0)
+        d5, _ = neuron_desc(m, 1.0)
+        assert d5 is not d4 and d5.sv[0] == 3.0
