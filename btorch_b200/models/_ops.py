@@ -159,7 +159,7 @@ class SparseMM(torch.autograd.Function):
         s = L.stream_of(g.device)
         gx = gw = None
         if ctx.needs_input_grad[0]:
-            w_csr = ctx.w_csr if ctx.w_csr is not None else pack_csr_weights(layout, w_canon)
+            w_csr = ctx.w_csr if ctx.w_csr is not None else _csr_weights_cached(layout, w_canon)
             gx = torch.empty_like(x)
             gT = torch.empty(max(1, B * layout.n_out), device=g.device, dtype=torch.float32)
             L.check(L.lib().bt_spmv_grad_input_t(B, n_in, layout.n_out, layout.csr_ptr.data_ptr(),
@@ -172,6 +172,19 @@ class SparseMM(torch.autograd.Function):
                                                 layout.csc_src.data_ptr(), x.data_ptr(), g.data_ptr(),
                                                 gw.data_ptr(), masks.data_ptr(), s), "bt_spmv_grad_weight")
         return gx, gw, None, None, None
+
+
+def _csr_weights_cached(layout, w):
+    """Weights in CSR order for the transpose gather, packed once per weight
+    tensor object and version: a SparseConn's weight is its magnitude
+    parameter, the same tensor in every step of a window until the optimizer
+    updates it (weak reference, so a new tensor at a reused address misses)."""
+    hit = getattr(layout, "_w_csr_cache", None)
+    if hit is not None and hit[0]() is w and hit[1] == (w.data_ptr(), _version(w)):
+        return hit[2]
+    packed = pack_csr_weights(layout, w.detach())
+    layout._w_csr_cache = (weakref.ref(w), (w.data_ptr(), _version(w)), packed)
+    return packed
 
 
 def sparse_mm(x2d, w_canon, layout, direction, w_csr=None):
