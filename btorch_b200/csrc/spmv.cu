@@ -314,7 +314,7 @@ extern "C" int bt_spmv_grad_input_t(int64_t batch, int64_t n_in, int64_t n_out, 
   BT_CHECK_ARG(batch >= 0 && n_in >= 0 && n_out >= 0, "negative size");
   if (batch == 0 || n_in == 0) return BT_OK;
   BT_CHECK_ARG(csr_ptr && grad_out && grad_x && work, "null pointer");
-  BT_CHECK_ARG(n_out < (int64_t(1) << 31) / 32 * 32 && batch < (int64_t(1) << 31) / 32 * 32, "too large");
+  BT_CHECK_ARG(batch * n_out < (int64_t(1) << 40), "too large");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (n_out > 0) {
     const dim3 tgrid(unsigned(ceil_div(n_out, 32)), unsigned(ceil_div(batch, 32)));
