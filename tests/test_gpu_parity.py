@@ -300,3 +300,29 @@ def test_grad_input_transposed_matches_lane_split(batch):
     np.testing.assert_allclose(outs[0], want, rtol=1e-5, atol=1e-5)
     np.testing.assert_allclose(outs[1], want, rtol=1e-5, atol=1e-5)
     np.testing.assert_array_equal(outs[1], outs[2])
+
+
+def test_input_project_live_rows_equal_full_projection():
+    """bt_input_project_live writes exactly the rows of live steps, equal to
+    bt_input_project's, and leaves the rows of finished samples untouched."""
+    from btorch_b200 import _lib as L
+
+    rng = np.random.default_rng(3)
+    steps, batch, c_in, n = 9, 5, 300, 1100
+    x = torch.tensor((rng.random((steps, batch, c_in)) < 0.05).astype(np.float32) * 1.5, device=DEV)
+    w_t = torch.tensor(rng.standard_normal((c_in, n)).astype(np.float32), device=DEV)
+    bias = torch.tensor(rng.standard_normal(n).astype(np.float32), device=DEV)
+    lens = torch.tensor([9, 0, 4, 1, 7], dtype=torch.int32, device=DEV)
+    work = torch.empty(steps * batch * (2 * c_in + 1), dtype=torch.int32, device=DEV)
+    s = L.stream_of(torch.device(DEV))
+    full = torch.empty((steps, batch, n), device=DEV)
+    L.check(L.lib().bt_input_project(steps * batch, c_in, n, x.data_ptr(), w_t.data_ptr(), bias.data_ptr(),
+                                     full.data_ptr(), work.data_ptr(), s), "bt_input_project")
+    live = torch.full((steps, batch, n), 1234.5, device=DEV)
+    L.check(L.lib().bt_input_project_live(steps, batch, c_in, n, x.data_ptr(), w_t.data_ptr(), bias.data_ptr(),
+                                          lens.data_ptr(), live.data_ptr(), work.data_ptr(), s),
+            "bt_input_project_live")
+    f, lv = full.cpu().numpy(), live.cpu().numpy()
+    for b, L_b in enumerate(lens.tolist()):
+        np.testing.assert_array_equal(lv[:L_b, b], f[:L_b, b])
+        assert (lv[L_b:, b] == 1234.5).all()

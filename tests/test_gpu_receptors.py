@@ -104,3 +104,24 @@ def test_inplace_reset_after_inference_run():
         with torch.inference_mode(), environ.context(dt=1.0):
             z, _ = rnn(x)
         np.testing.assert_array_equal(z.cpu().numpy().astype(np.uint8), cases.spikes(d))
+
+
+@pytest.mark.parametrize("direction", ["gather", "scatter"])
+def test_host_streamed_receptor_run_with_traces(direction):
+    """A host-resident input streamed through the fused receptor engine, with
+    every state trace requested (per-channel psc, summed psc, v) and uneven
+    sample lengths: identical to the device-input run, outputs on the host."""
+    d = cases.load("receptors_delay")
+    x = torch.tensor(d["x"])
+    lens = torch.tensor([120, 33, 80][: int(d["batch"])])
+    outs = []
+    for host in (False, True):
+        rnn = build(d, direction)
+        xin = x.pin_memory() if host else x.to(DEV)
+        with torch.no_grad(), environ.context(dt=1.0):
+            z, st = rnn(xin, sample_len=lens, engine_chunk=40)
+        assert z.device.type == ("cpu" if host else "cuda")
+        outs.append([z.cpu().numpy()] + [st[k].cpu().numpy() for k in sorted(st)] +
+                    [rnn.synapse.base_psc.psc.cpu().numpy(), rnn.neuron.v.cpu().numpy()])
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
