@@ -272,6 +272,7 @@ def measure_training(cfg, args, dev):
             "ms_per_window": ms / steps, "windows": steps, "window_steps": Wn,
             "neuron_steps_per_s": n * B * Wn * steps / (ms * 1e-3),
             "loss_first_last": [float(losses[0]), float(losses[-1])], "direction": conn.direction(B),
+            "path": brain.last_path,
             "config": {"workload": f"training: LIF+ExpPSC N={n} p={cfg['p']} ({len(net['w'])} trainable weights) "
                                    f"batch {B} T {cfg['t_max']} TBPTT windows {Wn} checkpoint chunks "
                                    f"{cfg['chunk']} sigmoid alpha {cfg['alpha']} readout {cfg['n_out']} "

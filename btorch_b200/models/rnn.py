@@ -18,6 +18,7 @@ import torch.nn as nn
 from torch.utils.checkpoint import checkpoint
 
 from . import base, environ
+from . import bptt as _bptt
 from . import engine as _engine
 from .cudagraph import CudaGraphRunner
 from .functional import filter_hidden_states, named_hidden_states, prepare_sparse_modules, set_hidden_states
@@ -207,6 +208,13 @@ class RecurrentNN(RecurrentNNAbstract):
         if sample_len is not None or spikes_out != "dense":
             raise NotImplementedError(f"sample_len / spikes_out need the fused engine ({reason})")
         self.last_fused_reason = reason
+        if self.fused and needs_grad and not extra and not kwargs and loop_args in (None, (0,)):
+            paths, why = _bptt.match(self)
+            if paths is not None:
+                out = _bptt.run(self, args[0], paths)
+                if out is not None:
+                    return out
+            self.last_fused_reason = f"{reason}; fused BPTT: {why or 'buffers too large'}"
         return super().multi_step_forward(*args, loop_args=loop_args, **kwargs)
 
 

@@ -6,6 +6,10 @@
   linear readout, MSE -- loss and every parameter gradient within 1e-4
   relative (norm-wise), spike rasters identical.
 * Against finite differences of the smooth-surrogate forward (sigmoid spikes).
+
+Both training paths are checked: the per-module one (an autograd node per
+module per step) and the fused BPTT (one autograd Function per call,
+btorch_b200/models/bptt.py).
 """
 
 import numpy as np
@@ -21,7 +25,7 @@ pytestmark = pytest.mark.gpu
 DEV = "cuda"
 
 
-def build(d, direction="gather", refractory=True, alpha=None):
+def build(d, direction="gather", refractory=True, alpha=None, fused=True):
     n = int(d["n"])
     W = sp.coo_array((d["w"], (d["src"], d["post"])), shape=(n, n))
     conn = SparseConn(W, sparse_config={"direction": direction})
@@ -32,7 +36,7 @@ def build(d, direction="gather", refractory=True, alpha=None):
     syn = ExponentialPSC(n, tau_syn=float(d["psc_tau"]), linear=conn)
     inp = DenseConn(int(d["c_in"]), n, weight=torch.tensor(d["W_in"]))
     brain = RecurrentNN(neuron, syn, neuron_inp_module=inp, update_state_names=("neuron.v",), grad_checkpoint=True,
-                        chunk_size=int(d["chunk"]), unroll=int(d["unroll"])).to(DEV)
+                        chunk_size=int(d["chunk"]), unroll=int(d["unroll"]), fused=fused).to(DEV)
     readout = torch.nn.Linear(n, int(d["n_out"])).to(DEV)
     with torch.no_grad():
         readout.weight.copy_(torch.tensor(d["W_out"]))
@@ -41,8 +45,8 @@ def build(d, direction="gather", refractory=True, alpha=None):
     return brain, readout, conn, inp
 
 
-def train_windows(d, direction="gather"):
-    brain, readout, conn, inp = build(d, direction)
+def train_windows(d, direction="gather", fused=True):
+    brain, readout, conn, inp = build(d, direction, fused=fused)
     steps, windows = int(d["steps"]), int(d["windows"])
     x = torch.tensor(d["x"], device=DEV)
     target = torch.tensor(d["target"], device=DEV)
@@ -50,8 +54,9 @@ def train_windows(d, direction="gather"):
     with environ.context(dt=1.0):
         for k in range(windows):
             sl = slice(k * steps, (k + 1) * steps)
-            z, _ = brain(x[sl])
-            assert brain.last_path == "modular"
+            z, st = brain(x[sl])
+            assert brain.last_path == ("fused-bptt" if fused else "modular"), brain.last_path
+            assert st["neuron.v"].shape == (steps, int(d["batch"]), int(d["n"]))
             loss = ((readout(z) - target[sl]) ** 2).mean()
             for m in (brain, readout):
                 m.zero_grad(set_to_none=True)
@@ -70,11 +75,12 @@ def rel_err(a, b):
     return float(np.linalg.norm(a.astype(np.float64) - b) / max(np.linalg.norm(b.astype(np.float64)), 1e-30))
 
 
+@pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("direction", ["gather", "scatter"])
 @pytest.mark.parametrize("name", ["train_spiking", "train_smooth"])
-def test_bptt_gradients_match_reference_autograd(name, direction):
+def test_bptt_gradients_match_reference_autograd(name, direction, fused):
     d = cases.load(name)
-    out = train_windows(d, direction)
+    out = train_windows(d, direction, fused)
     n = int(d["n"])
     z = np.concatenate(out["z"])
     if int(d["spiking"]):
@@ -87,7 +93,8 @@ def test_bptt_gradients_match_reference_autograd(name, direction):
             assert rel_err(out[key], d[key]) < 1e-4, (key, rel_err(out[key], d[key]))
 
 
-def test_bptt_matches_finite_differences_smooth():
+@pytest.mark.parametrize("fused", [True, False])
+def test_bptt_matches_finite_differences_smooth(fused):
     """Analytic gradient of the smooth-surrogate forward against central
     differences of the same forward (fp32, the 6 largest-gradient weights of
     the recurrent and input layers).  The surrogate backward is
@@ -98,7 +105,7 @@ def test_bptt_matches_finite_differences_smooth():
     d = cases.load("train_smooth")
     steps = int(d["steps"])
     k = 2.0 * np.log(np.sqrt(2.0) + 1.0)
-    brain, readout, conn, inp = build(d, refractory=False, alpha=4.0 / k)
+    brain, readout, conn, inp = build(d, refractory=False, alpha=4.0 / k, fused=fused)
     x = torch.tensor(d["x"][:steps], device=DEV)
     target = torch.tensor(d["target"][:steps], device=DEV)
 
@@ -125,3 +132,33 @@ def test_bptt_matches_finite_differences_smooth():
                 flat[i] = old
             fd = (lp - lm) / (2 * eps)
             assert abs(fd - float(g[i])) <= 2e-2 * abs(float(g[i])) + 1e-6, (i, fd, float(g[i]))
+
+
+def test_fused_bptt_state_stack_gradients_and_alif():
+    """Gradients that enter through the returned state stacks (v, psc) and the
+    final state, for an ALIF network, equal the per-module path's."""
+    import scipy.sparse as sp
+
+    from btorch_b200.models import ALIF
+
+    rng = np.random.default_rng(11)
+    n, B, T = 64, 3, 25
+    W = sp.random(n, n, density=0.1, random_state=4, dtype=np.float32)
+    W.data = (np.round(W.data * 64) / 64 * np.where(rng.random(W.nnz) < 0.8, 1, -1)).astype(np.float32)
+    x = torch.tensor((rng.random((T, B, n)) < 0.3).astype(np.float32) * 0.5, device=DEV)
+    grads = []
+    for fused in (True, False):
+        conn = SparseConn(sp.coo_array(W), sparse_config={"direction": "gather"})
+        neuron = ALIF(n, v_threshold=1.0, v_reset=0.0, c_m=1.0, g_leak=0.05, E_leak=0.0, E_k=-1.0,
+                      tau_adapt=50.0, dg_k=0.1, tau_ref=None, hard_reset=False, surrogate_function=Sigmoid(alpha=3.0))
+        brain = RecurrentNN(neuron, ExponentialPSC(n, tau_syn=5.0, linear=conn),
+                            update_state_names=("neuron.v", "synapse.psc"), fused=fused).to(DEV)
+        init_net_state(brain, batch_size=B, dtype=torch.float32, device=DEV)
+        with environ.context(dt=1.0):
+            z, st = brain(x)
+        assert brain.last_path == ("fused-bptt" if fused else "modular")
+        loss = (z * torch.linspace(0.5, 1.5, n, device=DEV)).sum() + (st["neuron.v"] ** 2).mean() \
+            + st["synapse.psc"].sum() * 0.1 + brain.neuron.g_k.sum() * 0.3
+        loss.backward()
+        grads.append(conn.magnitude.grad.cpu().numpy())
+    assert rel_err(grads[0], grads[1]) < 1e-5, rel_err(grads[0], grads[1])
