@@ -105,9 +105,13 @@ class _FusedBPTT(torch.autograd.Function):
             wz = _spmv(direction, lay, Z[t], w, w_csr)
             L.check(L.lib().bt_psc_step(B, n, L.param(coef), L.param(tau), Ps[t].data_ptr(), wz.data_ptr(),
                                         Ps[t + 1].data_ptr(), s), "bt_psc_step")
-        ctx.rnn, ctx.d, ctx.keep, ctx.coef, ctx.tau, ctx.lay = rnn, d, keep, coef, tau, lay
-        ctx.bufs = (I, U, M, VCH, Vs, GKs)
-        ctx.save_for_backward(mag, Z)  # Z is also returned: autograd checks it is not modified in place
+        # no reference to the module itself: the module's state will hold this
+        # Function's outputs, and a cycle would keep the step buffers alive
+        ctx.d, ctx.keep, ctx.coef, ctx.tau, ctx.lay = d, keep, coef, tau, lay
+        ctx.detach_reset = int(bool(neuron.detach_reset))
+        # saved through autograd, so they are freed after backward (unless
+        # retain_graph) and Z, also returned, is checked for in-place changes
+        ctx.save_for_backward(mag, Z, I, U, M, VCH, Vs, GKs)
         ctx.has_gk = GKs is not None
         ctx.set_materialize_grads(False)
         stack = lambda A, kind: A[1:].clone() if A is not None and kind in kinds else None  # noqa: E731
@@ -121,8 +125,7 @@ class _FusedBPTT(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, gZ, gV, gP, gGK, _gR, gvT, gpT, ggT, _grT):
-        mag, Z = ctx.saved_tensors
-        I, U, M, VCH, Vs, GKs = ctx.bufs
+        mag, Z, I, U, M, VCH, Vs, GKs = ctx.saved_tensors
         T, B, n = Z.shape
         dev = Z.device
         lay, d = ctx.lay, ctx.d
@@ -136,7 +139,7 @@ class _FusedBPTT(torch.autograd.Function):
         g_psc = torch.zeros((B, n), device=dev) if gpT is None else gpT.reshape(B, n).contiguous().clone()
         cur_v = None if gvT is None else gvT.reshape(B, n).contiguous()
         cur_gk = None if (ggT is None or not ctx.has_gk) else ggT.reshape(B, n).contiguous()
-        detach_reset = int(bool(ctx.rnn.neuron.detach_reset))
+        detach_reset = ctx.detach_reset
         for t in reversed(range(T)):
             gp = G_psc[t]
             torch.add(g_psc, gP[t], out=gp) if gP is not None else gp.copy_(g_psc)
