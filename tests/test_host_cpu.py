@@ -170,3 +170,33 @@ def test_neuron_desc_cache_follows_parameter_changes():
         m.v_threshold = torch.tensor(3.0)
         d5, _ = neuron_desc(m, 1.0)
         assert d5 is not d4 and d5.sv[0] == 3.0
+
+
+def test_fused_bptt_match_rules():
+    """Which models the fused BPTT takes (host logic only): LIF/ALIF +
+    ExponentialPSC over a square SparseConn, optional nn.Linear input, state
+    stacks of v / psc / g_k / refractory; everything else steps module by
+    module."""
+    import numpy as np
+    import scipy.sparse as sp
+
+    from btorch_b200.models import ALIF, LIF, DelayedPSC, DenseConn, ExponentialPSC, RecurrentNN, SparseConn
+    from btorch_b200.models import bptt
+
+    n = 16
+    W = sp.coo_array(sp.random(n, n, density=0.2, random_state=0, dtype=np.float32))
+
+    def net(neuron=None, syn=None, **kw):
+        neuron = neuron or LIF(n, tau_ref=2.0)
+        syn = syn or ExponentialPSC(n, 5.0, SparseConn(W))
+        return RecurrentNN(neuron, syn, **kw)
+
+    paths, why = bptt.match(net())
+    assert why == "" and set(paths.values()) == {"v", "ref", "psc"}
+    paths, _ = bptt.match(net(ALIF(n), update_state_names=("neuron.g_k",)))
+    assert paths == {"neuron.g_k": "gk"}
+    assert bptt.match(net(neuron_inp_module=DenseConn(4, n)))[0] is not None
+    assert bptt.match(net(syn=DelayedPSC(ExponentialPSC(n, 5.0, SparseConn(W)), max_delay_steps=3)))[1] == "synapse"
+    assert bptt.match(net(cpu_offload=True))[0] is None
+    rect = sp.coo_array(sp.random(n, 2 * n, density=0.2, random_state=1, dtype=np.float32))
+    assert bptt.match(net(syn=ExponentialPSC(n, 5.0, SparseConn(rect))))[0] is None
