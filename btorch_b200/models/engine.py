@@ -3,12 +3,14 @@
 A RecurrentNN whose neuron is LIF/ALIF, whose synapse is ExponentialPSC,
 DelayedPSC(ExponentialPSC) or HeterSynapsePSC(ExponentialPSC, up to
 MAX_RECEPTORS receptor channels) over a SparseConn, and whose input module is
-absent or a DenseConn/nn.Linear
-runs through ``bt_engine_run``: the whole time loop on the device, one or two
-kernel launches per step (btorch_b200/csrc/engine.cu), with the reference's
-outputs (spike stack and requested state stacks) and final state.
+absent or a DenseConn/nn.Linear runs through ``bt_engine_run``: the whole
+time loop on the device, one or two kernel launches per step
+(btorch_b200/csrc/engine.cu), with the reference's outputs (spike stack and
+requested state stacks) and final state.  The input may be resident in host
+memory: it is then streamed through the device in chunks (_HostStreams).
 
-Anything else, and any call that needs gradients, runs the per-module path.
+Calls that need gradients run the fused BPTT (bptt.py) or the per-module
+path; anything else the engine does not take runs the per-module path.
 """
 
 from __future__ import annotations
