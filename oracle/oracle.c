@@ -24,7 +24,11 @@
  *     connection.py:973-1027, and SpikeHistory.get_flattened,
  *     history.py:299-345);
  *   - RecurrentNN.single_step_forward (btorch/models/rnn.py:517-528):
- *     I = psc + x; z = neuron(I); psc = decay(psc) + W z_delayed.
+ *     I = psc + x; z = neuron(I); psc = decay(psc) + W z_delayed;
+ *   - receptor channels of HeterSynapsePSC (synapse.py:626-847): C PSC
+ *     columns per neuron (post * C + r, each with its own coefficients), the
+ *     neuron's input the sum of its C columns in the order torch's CPU sum
+ *     reduces a contiguous row (synapse.py:744-747).
  * Every torch op is one correctly rounded fp32 op here; the file must be
  * compiled with -ffp-contract=off so that no multiply-add is fused.
  */
@@ -62,11 +66,42 @@ typedef struct orc_net {
   /* outputs (any may be NULL) */
   uint8_t* spikes;     /* [steps][batch][n] */
   float* v_trace;      /* [steps][batch][n] */
-  float* psc_trace;    /* [steps][batch][n] */
+  float* psc_trace;    /* [steps][batch][n * n_rec] */
   int32_t threads;
+  int32_t n_rec;       /* receptor columns per neuron (0 or 1: none); psc, psc_coef,
+                          psc_tau and the columns of ptr are then n * n_rec wide */
 } orc_net;
 
 static inline float relu_keep_nan(float x) { return (x != x) ? x : (x > 0.0f ? x : 0.0f); }
+
+/* Sum of C floats in torch's CPU order for a contiguous row (C < 4: left to
+ * right; 4 <= C < 8: four accumulators, the rest folded into the first in
+ * turn; C >= 8: eight accumulators over whole groups of 8, the tail's sum
+ * added to the first), as the reference's .sum(-1) over receptors rounds. */
+static float receptor_sum(const float* p, int C) {
+  if (C < 4) {
+    float s = p[0];
+    for (int r = 1; r < C; ++r) s = s + p[r];
+    return s;
+  }
+  if (C < 8) {
+    float a0 = p[0];
+    for (int r = 4; r < C; ++r) a0 = a0 + p[r];
+    return ((a0 + p[1]) + p[2]) + p[3];
+  }
+  const int full = C & ~7;
+  float a[8];
+  for (int j = 0; j < 8; ++j) a[j] = p[j];
+  for (int r = 8; r < full; ++r) a[r & 7] = a[r & 7] + p[r];
+  if (full < C) {
+    float t = p[full];
+    for (int r = full + 1; r < C; ++r) t = t + p[r];
+    a[0] = a[0] + t;
+  }
+  float s = a[0];
+  for (int j = 1; j < 8; ++j) s = s + a[j];
+  return s;
+}
 
 typedef struct {
   const orc_net* net;
@@ -85,7 +120,8 @@ static void neuron_phase(const orc_net* d, int64_t k, int64_t lo, int64_t hi) {
       const int64_t idx = b * n + i;
       float s = 0.0f;
       if (live) {
-        const float P = d->psc[idx];
+        const int C = d->n_rec > 1 ? d->n_rec : 1;
+        const float P = C > 1 ? receptor_sum(d->psc + idx * C, C) : d->psc[idx];
         const float I = d->x ? P + d->x[(k * B) * n + idx] : P;
         float v = d->v[idx];
         const float vth = d->vth[i], vr = d->vr[i], cm = d->cm[i];
@@ -154,24 +190,25 @@ static void neuron_phase(const orc_net* d, int64_t k, int64_t lo, int64_t hi) {
 static void synapse_phase(const orc_net* d, int64_t k, int64_t lo, int64_t hi) {
   const int64_t n = d->n, B = d->batch, H = d->max_delay + 1;
   const int64_t t = d->t0 + k;
+  const int64_t C = d->n_rec > 1 ? d->n_rec : 1, nc = n * C;
   for (int64_t b = 0; b < B; ++b) {
     const int live = !d->sample_len || k < d->sample_len[b];
-    for (int64_t i = lo; i < hi; ++i) {
-      const int64_t idx = b * n + i;
+    for (int64_t col = lo * C; col < hi * C; ++col) {  /* the PSC columns of neurons [lo, hi) */
+      const int64_t idx = b * nc + col;
       if (live) {
         /* W z: fmaf chain over in-edges in canonical order */
         float acc = 0.0f;
-        for (int64_t e = d->ptr[i]; e < d->ptr[i + 1]; ++e) {
+        for (int64_t e = d->ptr[col]; e < d->ptr[col + 1]; ++e) {
           const int64_t s = t - d->delay[e];
           const float z = s >= 0 ? d->hist[((s % H) * B + b) * n + d->pre[e]] : 0.0f;
           acc = fmaf(d->w[e], z, acc);
         }
         const float p = d->psc[idx];
-        const float dec = d->psc_coef[i] * ((-p) / d->psc_tau[i]);
+        const float dec = d->psc_coef[col] * ((-p) / d->psc_tau[col]);
         const float q = p + dec;
         d->psc[idx] = q + acc;
       }
-      if (d->psc_trace) d->psc_trace[(k * B) * n + idx] = d->psc[idx];
+      if (d->psc_trace) d->psc_trace[(k * B) * nc + idx] = d->psc[idx];
     }
   }
 }

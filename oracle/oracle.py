@@ -43,7 +43,7 @@ class _Net(C.Structure):
         ("v", _f), ("ref", _f), ("gk", _f), ("psc", _f), ("hist", _f),
         ("t0", C.c_int64),
         ("spikes", _u8), ("v_trace", _f), ("psc_trace", _f),
-        ("threads", C.c_int32),
+        ("threads", C.c_int32), ("n_rec", C.c_int32),
     ]
 
 
@@ -127,6 +127,7 @@ class NetSpec:
     delay: np.ndarray  # int32 [nnz]
     w: np.ndarray  # float32 [nnz]
     max_delay: int = 0
+    n_rec: int = 1  # receptor columns per neuron: ptr, psc_coef, psc_tau span n * n_rec columns
 
 
 @dataclass
@@ -144,7 +145,7 @@ def init_state(spec: NetSpec, batch: int, v0=None, gk0=0.0) -> NetState:
     n = spec.n
     v = np.empty((batch, n), np.float32)
     v[:] = spec.params["v_reset"] if v0 is None else v0
-    st = NetState(v=v, psc=np.zeros((batch, n), np.float32))
+    st = NetState(v=v, psc=np.zeros((batch, n * max(1, spec.n_rec)), np.float32))
     if spec.use_ref:
         st.ref = np.zeros((batch, n), np.float32)
     if spec.kind == 1:
@@ -162,7 +163,9 @@ def run(spec: NetSpec, state: NetState, x, steps=None, sample_len=None, threads=
         steps = x.shape[0] if steps is None else steps
         assert x.shape[1:] == (B, n)
     threads = threads or os.cpu_count() or 1
-    P = {k: _f32(np.broadcast_to(np.asarray(v, np.float32), (n,))) for k, v in spec.params.items()}
+    nc = n * max(1, spec.n_rec)
+    P = {k: _f32(np.broadcast_to(np.asarray(v, np.float32), (nc if k.startswith("psc_") else n,)))
+         for k, v in spec.params.items()}
     need = ["v_threshold", "v_reset", "c_m", "psc_coef", "psc_tau"]
     need += ["tau"] if spec.kind == 0 else ["g_leak", "E_leak", "E_k", "dg_k", "tau_adapt", "coef_gk"]
     if spec.use_ref:
@@ -171,7 +174,7 @@ def run(spec: NetSpec, state: NetState, x, steps=None, sample_len=None, threads=
         assert k in P, f"missing parameter {k}"
     spikes = np.zeros((steps, B, n), np.uint8)
     v_tr = np.zeros((steps, B, n), np.float32) if want_v else None
-    p_tr = np.zeros((steps, B, n), np.float32) if want_psc else None
+    p_tr = np.zeros((steps, B, nc), np.float32) if want_psc else None
     sl = None if sample_len is None else np.ascontiguousarray(sample_len, np.int32)
     net = _Net(
         n=n, batch=B, steps=steps, kind=spec.kind, hard_reset=int(spec.hard_reset),
@@ -186,6 +189,7 @@ def run(spec: NetSpec, state: NetState, x, steps=None, sample_len=None, threads=
         v=_p(state.v, _f), ref=_p(state.ref, _f), gk=_p(state.gk, _f), psc=_p(state.psc, _f),
         hist=_p(state.hist, _f), t0=state.t,
         spikes=_p(spikes, _u8), v_trace=_p(v_tr, _f), psc_trace=_p(p_tr, _f), threads=threads,
+        n_rec=max(1, spec.n_rec),
     )
     keep = (x, P, spikes, v_tr, p_tr, sl)  # noqa: F841 -- buffers live across the call
     if lib().orc_run(C.byref(net)) != 0:

@@ -72,3 +72,34 @@ def test_oracle_reproduces_training_forward_raster():
     xp = O.linear(x.reshape(T * B, -1), d["W_in"].T.copy()).reshape(T, B, n)
     z = O.run(spec, O.init_state(spec, B), xp)["spikes"]
     np.testing.assert_array_equal(z, np.unpackbits(d["z"], axis=-1, bitorder="little")[..., :n])
+
+
+@pytest.mark.parametrize("name", ["receptors2", "receptors_delay"])
+def test_oracle_receptor_channels_match_reference(name):
+    """The oracle's receptor columns (C PSCs per neuron, per-column time
+    constants, receptor sum in torch's CPU order) against the reference's
+    HeterSynapsePSC runs: rasters, v, per-channel psc and final state bit for
+    bit."""
+    import torch
+
+    d = cases.load(name)
+    n, B, C = int(d["n"]), int(d["batch"]), int(d["n_rec"])
+    D = int(d["n_bins"]) if "n_bins" in d else 1
+    post, src, w = d["post"].astype(np.int64), d["src"].astype(np.int64), d["w"].astype(np.float32)
+    ptr = np.concatenate([[0], np.cumsum(np.bincount(post, minlength=n * C))]).astype(np.int64)
+    taus = np.tile(d["taus"].astype(np.float32), n)
+    lin = -1.0 / torch.tensor(taus)
+    coef = (torch.expm1(1.0 * lin) / lin).numpy()
+    spec = O.NetSpec(n=n, kind=0, hard_reset=True, use_ref=True, dt=1.0,
+                     params={"v_threshold": 1.0, "v_reset": 0.0, "c_m": 1.0, "tau": 20.0, "tau_ref": 2.0,
+                             "psc_coef": coef, "psc_tau": taus},
+                     ptr=ptr, pre=(src // D).astype(np.int32), delay=(src % D).astype(np.int32), w=w,
+                     max_delay=D - 1, n_rec=C)
+    st = O.init_state(spec, B)
+    o = O.run(spec, st, d["x"], want_v=True, want_psc=True, threads=4)
+    np.testing.assert_array_equal(o["spikes"], cases.spikes(d))
+    K = d["v"].shape[0]
+    np.testing.assert_array_equal(o["v"][:K], d["v"])
+    np.testing.assert_array_equal(o["psc"][:K], d["psc_rec"])
+    np.testing.assert_array_equal(st.v, d["v_final"])
+    np.testing.assert_array_equal(st.psc, d["psc_rec_final"])
