@@ -125,3 +125,44 @@ def test_host_streamed_receptor_run_with_traces(direction):
                     [rnn.synapse.base_psc.psc.cpu().numpy(), rnn.neuron.v.cpu().numpy()])
     for a, b in zip(*outs):
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("direction", ["gather", "scatter"])
+@pytest.mark.parametrize("C", [3, 9])
+def test_odd_receptor_counts_match_oracle(C, direction):
+    """Receptor counts without a vector path (3) and with the eight-accumulator
+    sum (9, the E/I/unknown pairs): the fused engine against the oracle, bit
+    for bit (dyadic weights, per-synapse delays over 4 bins)."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(C)
+    n, B, T, D = 200, 3, 90, 4
+    nnz = 3000
+    post = rng.integers(0, n * C, nnz)
+    src = rng.integers(0, n * D, nnz)
+    key = np.unique(post * (n * D) + src)
+    post, src = key // (n * D), key % (n * D)
+    w = (rng.integers(1, 6, key.size) * np.where(rng.random(key.size) < 0.8, 1.0, -1.0) * 2.0 ** -4).astype(np.float32)
+    taus = np.tile((2.0 + rng.integers(0, 8, C)).astype(np.float32), n)
+    x = (np.round(rng.poisson(0.1, (T, B, n)) * 0.75 * 64) / 64).astype(np.float32)
+    conn = SparseConn(sp.coo_array((w, (src, post)), shape=(n * D, n * C)), sparse_config={"direction": direction})
+    rti = pd.DataFrame({"receptor_type": [f"r{r}" for r in range(C)], "receptor_index": list(range(C))})
+    syn = HeterSynapsePSC(n, C, rti, conn, base_psc=ExponentialPSC, max_delay_steps=D, use_circular_buffer=True,
+                          tau_syn=torch.tensor(taus))
+    rnn = RecurrentNN(LIF(n, tau_ref=2.0, hard_reset=True), syn, update_state_names=("neuron.v",)).to(DEV)
+    init_net_state(rnn, batch_size=B, dtype=torch.float32, device=DEV)
+    with torch.no_grad(), environ.context(dt=1.0):
+        z, st = rnn(torch.tensor(x, device=DEV))
+    assert rnn.last_path == "fused" and rnn.last_engine_direction == direction
+    ptr = np.concatenate([[0], np.cumsum(np.bincount(post, minlength=n * C))]).astype(np.int64)
+    coef = syn.base_psc.coefficients(1.0)[0].cpu().numpy()
+    spec = O.NetSpec(n=n, kind=0, hard_reset=True, use_ref=True, dt=1.0,
+                     params={"v_threshold": 1.0, "v_reset": 0.0, "c_m": 1.0, "tau": 20.0, "tau_ref": 2.0,
+                             "psc_coef": coef, "psc_tau": taus},
+                     ptr=ptr, pre=(src // D).astype(np.int32), delay=(src % D).astype(np.int32), w=w,
+                     max_delay=D - 1, n_rec=C)
+    ost = O.init_state(spec, B)
+    o = O.run(spec, ost, x, want_v=True, threads=4)
+    np.testing.assert_array_equal(z.cpu().numpy().astype(np.uint8), o["spikes"])
+    np.testing.assert_array_equal(st["neuron.v"].cpu().numpy(), o["v"])
+    np.testing.assert_array_equal(rnn.synapse.base_psc.psc.cpu().numpy(), ost.psc)
