@@ -286,4 +286,175 @@ def stack_hetersynapse(conn_dict: dict, receptor_type_index: pd.DataFrame,
     return stack(conn_dict.items(), lookup, len(receptor_type_index))
 
 
-__all__ = ["expand_conn_for_delays", "make_hetersynapse_conn", "make_sparse_mat", "stack_hetersynapse"]
+def _cell_type_codes(neurons: pd.DataFrame, cell_type_col: str, nan_in_same_group: bool):
+    """root_id -> integer cell-type code lookup (connection.py:118-130).
+
+    Every neuron whose cell type is missing gets a type of its own
+    ("__none_<i>__", i counting the missing ones in table order) unless
+    nan_in_same_group; the missing types that remain (and root ids absent
+    from the table) share one extra code.  A duplicated root id takes the
+    type of its last row.  Returns (sorted unique root ids, their codes,
+    the code of a missing type)."""
+    ct = neurons[cell_type_col]
+    missing = ct.isna().to_numpy()
+    if not nan_in_same_group and missing.any():
+        ct = ct.astype(object).copy()
+        ct[missing] = [f"__none_{i}__" for i in range(int(missing.sum()))]
+    codes, labels = pd.factorize(ct)  # missing -> -1
+    na_code = len(labels)
+    codes = np.where(codes < 0, na_code, codes).astype(np.int64)
+    roots = neurons["root_id"].to_numpy()
+    last = ~pd.Index(roots).duplicated(keep="last")
+    roots, codes = roots[last], codes[last]
+    order = np.argsort(roots, kind="stable")
+    return roots[order], codes[order], na_code
+
+
+def _lookup(keys, values, query, default):
+    """values[keys == q] for each q (keys sorted and unique), else default."""
+    query = np.asarray(query)
+    if len(keys) == 0:
+        return np.full(len(query), default, np.int64)
+    pos = np.clip(np.searchsorted(keys, query), 0, len(keys) - 1)
+    return np.where(keys[pos] == query, values[pos], default)
+
+
+def _pair_cell_codes(neurons, connections, cell_type_col, nan_in_same_group):
+    """The first row of every distinct (pre, post) simple-id pair
+    (connection.py:132-139) with its pre and post cell-type codes."""
+    first = ~connections.duplicated(subset=["pre_simple_id", "post_simple_id"]).to_numpy()
+    tab = connections.loc[first]
+    roots, codes, na_code = _cell_type_codes(neurons, cell_type_col, nan_in_same_group)
+    pre_ct = _lookup(roots, codes, tab["pre_root_id"].to_numpy(), na_code)
+    post_ct = _lookup(roots, codes, tab["post_root_id"].to_numpy(), na_code)
+    return (tab["pre_simple_id"].to_numpy(dtype=np.int64), tab["post_simple_id"].to_numpy(dtype=np.int64),
+            pre_ct, post_ct, na_code)
+
+
+def _first_seen_ids(*cols):
+    """1-based ids of the distinct rows of the integer columns `cols`,
+    numbered in order of first appearance (pd.factorize order)."""
+    if len(cols[0]) == 0:
+        return np.zeros(0, np.int64)
+    key = np.stack([np.asarray(c, np.int64) for c in cols], axis=1)
+    _, first, inverse = np.unique(key, axis=0, return_index=True, return_inverse=True)
+    rank = np.empty(len(first), np.int64)
+    rank[np.argsort(first, kind="stable")] = np.arange(len(first))
+    return rank[inverse.reshape(-1)] + 1
+
+
+def make_constraint_by_neuron_type(neurons: pd.DataFrame, connections: pd.DataFrame,
+                                   nan_in_same_group: bool = True) -> scipy.sparse.sparray:
+    """(n, n) COO whose value at each connected (pre, post) pair is a 1-based
+    group id, one per distinct (pre cell type, post cell type) pair, numbered
+    in order of first appearance in the connection table
+    (connection.py:96-158).  Duplicate (pre, post) rows count once (first
+    row); entries follow the table's order.  Missing cell types form one
+    group with each other (nan_in_same_group) or one type per neuron."""
+    pre, post, pre_ct, post_ct, _ = _pair_cell_codes(neurons, connections, "cell_type", nan_in_same_group)
+    gid = _first_seen_ids(pre_ct, post_ct)
+    n = neurons.shape[0]
+    return scipy.sparse.coo_array((gid, (pre, post)), shape=(n, n))
+
+
+def make_hetersynapse_constraint(
+    neurons: pd.DataFrame,
+    connections: pd.DataFrame,
+    cell_type_col: str = "cell_type",
+    receptor_type_col: str = "EI",
+    receptor_type_mode: Literal["neuron", "connection"] = "neuron",
+    constraint_mode: Literal["full", "cell_only", "cell_and_receptor"] = "full",
+    nan_in_same_group: bool = True,
+    ignore_post_type: bool = False,
+) -> scipy.sparse.sparray:
+    """Constraint groups in the receptor-expanded space of
+    make_hetersynapse_conn (connection.py:590-787).
+
+    cell_only: the (pre, post) cell-type groups of
+    make_constraint_by_neuron_type, repeated pair-major for every receptor
+    index (column post * n_pairs + pair), whether or not that receptor pair
+    holds the synapse.  full / cell_and_receptor: one group per distinct
+    (pre cell type, post cell type, receptor key) over the entries of the
+    expanded matrix, numbered in the matrix's entry order; the receptor key
+    is the receptor type (connection mode or ignore_post_type), else the
+    (pre, post) receptor-type pair -- for cell_and_receptor as the string
+    "<pre>-<post>", so pairs whose strings coincide share a group.  The cell
+    types of the first table row given `cell_type_col` are used, while
+    make_constraint_by_neuron_type (cell_only) reads the column "cell_type".
+    The expanded matrix is built with the default NaN policy (an error on
+    missing receptor types), and any mode other than full / cell_only means
+    cell_and_receptor, as in the reference (connection.py:745-779)."""
+    def expanded():
+        return make_hetersynapse_conn(neurons, connections, receptor_type_col, receptor_type_mode,
+                                      return_dict=False, ignore_post_type=ignore_post_type)
+
+    # the (pre, post) cell-type groups come first in every mode, as in the
+    # reference (so a table without "cell_type" fails the same way)
+    cell = make_constraint_by_neuron_type(neurons, connections, nan_in_same_group=nan_in_same_group).tocoo()
+    if constraint_mode == "cell_only":
+        _, index = expanded()
+        n_pairs = len(index)
+        k = np.arange(n_pairs).repeat(cell.nnz)
+        return scipy.sparse.coo_array(
+            (np.tile(cell.data, n_pairs), (np.tile(cell.row, n_pairs), np.tile(cell.col, n_pairs) * n_pairs + k)),
+            shape=(cell.shape[0], cell.shape[1] * n_pairs))
+
+    mat, index = expanded()
+    mat = mat.tocoo()
+    n_pairs = len(index)
+    row = np.asarray(mat.row, np.int64)
+    col = np.asarray(mat.col, np.int64)
+    if row.size == 0:
+        return scipy.sparse.coo_array((np.zeros(0, np.int64), (row, col)), shape=mat.shape)
+    pair = col % n_pairs
+    post_of = col // n_pairs
+    # cell types of each entry's (pre, post) neurons, from the first table
+    # row of that pair; both missing if the table has no such row
+    pre, post, pre_ct, post_ct, na = _pair_cell_codes(neurons, connections, cell_type_col, nan_in_same_group)
+    span = max(int(pre.max(initial=0)), int(post.max(initial=0)), int(row.max()), int(post_of.max())) + 1
+    order = np.argsort(pre * span + post, kind="stable")
+    e_pre = _lookup((pre * span + post)[order], pre_ct[order], row * span + post_of, na)
+    e_post = _lookup((pre * span + post)[order], post_ct[order], row * span + post_of, na)
+
+    # receptor key of every receptor index
+    if "receptor_type" in index.columns:
+        labels = index["receptor_type"]
+    elif constraint_mode == "full":
+        labels = pd.Series(list(zip(index["pre_receptor_type"], index["post_receptor_type"])), dtype=object)
+    else:
+        labels = index["pre_receptor_type"].astype(str) + "-" + index["post_receptor_type"].astype(str)
+    rec_code = pd.factorize(labels)[0].astype(np.int64)
+    at = _lookup(index["receptor_index"].to_numpy(dtype=np.int64), rec_code, pair, -1)
+    gid = _first_seen_ids(e_pre, e_post, at)
+    return scipy.sparse.coo_array((gid, (row, col)), shape=mat.shape)
+
+
+def make_hetersynapse_constrained_conn(
+    neurons: pd.DataFrame,
+    connections: pd.DataFrame,
+    cell_type_col: str = "cell_type",
+    receptor_type_col: str = "EI",
+    receptor_type_mode: Literal["neuron", "connection"] = "neuron",
+    constraint_mode: Literal["full", "cell_only", "cell_and_receptor"] = "full",
+    nan_in_same_group: bool = True,
+    dropna: Literal["error", "filter", "unknown"] = "error",
+    ignore_post_type: bool = False,
+):
+    """(matrix, constraint, receptor_type_index) for
+    SparseConstrainedConn.from_hetersynapse (connection.py:790-836): the
+    matrix of make_hetersynapse_conn with `dropna`, the groups of
+    make_hetersynapse_constraint (which builds its expanded matrix with the
+    default NaN policy)."""
+    mat, index = make_hetersynapse_conn(neurons, connections, receptor_type_col=receptor_type_col,
+                                        receptor_type_mode=receptor_type_mode, return_dict=False, dropna=dropna,
+                                        ignore_post_type=ignore_post_type)
+    constraint = make_hetersynapse_constraint(
+        neurons, connections, cell_type_col=cell_type_col, receptor_type_col=receptor_type_col,
+        receptor_type_mode=receptor_type_mode, constraint_mode=constraint_mode,
+        nan_in_same_group=nan_in_same_group, ignore_post_type=ignore_post_type)
+    return mat, constraint, index
+
+
+__all__ = ["expand_conn_for_delays", "make_constraint_by_neuron_type", "make_hetersynapse_conn",
+           "make_hetersynapse_constrained_conn", "make_hetersynapse_constraint", "make_sparse_mat",
+           "stack_hetersynapse"]

@@ -523,6 +523,66 @@ def case_receptors_delay(rng, *, n, n_conn, batch, steps, D):
     return out
 
 
+def constraint_tables(rng, n, n_conn):
+    """Seeded tables with cell types (three missing), two cell-type columns,
+    root ids (every 7th connection names a root id absent from the neuron
+    table) and duplicate (pre, post) rows."""
+    import pandas as pd
+
+    ct = rng.choice(np.array(["a", "b", "c", "d"], dtype=object), size=n)
+    ct[[2, 9, 30]] = np.nan
+    neurons = pd.DataFrame({"root_id": 1000 + np.arange(n), "simple_id": np.arange(n), "cell_type": ct,
+                            "EI": rng.choice(np.array(["E", "I"], dtype=object), size=n, p=[0.7, 0.3]),
+                            "ct2": rng.choice(np.array(["x", "y"], dtype=object), size=n)})
+    pre = rng.integers(0, n, n_conn)
+    post = rng.integers(0, n, n_conn)
+    conns = pd.DataFrame({"pre_simple_id": pre, "post_simple_id": post, "pre_root_id": 1000 + pre,
+                          "post_root_id": 1000 + post, "syn_count": rng.integers(1, 9, n_conn),
+                          "nt": rng.choice(np.array(["ach", "gaba", "glut"], dtype=object), size=n_conn)})
+    conns.loc[::7, "pre_root_id"] = 99999
+    return neurons, conns
+
+
+CONSTRAINT_RUNS = [
+    dict(constraint_mode=m, receptor_type_mode=r, ignore_post_type=i, nan_in_same_group=g, cell_type_col=c)
+    for m in ("full", "cell_only", "cell_and_receptor") for r in ("neuron", "connection")
+    for i in (False, True) for g in (True, False) for c in ("cell_type", "ct2")]
+
+
+def case_connectome_constraint(rng):
+    """make_constraint_by_neuron_type / make_hetersynapse_constraint /
+    make_hetersynapse_constrained_conn outputs on seeded tables, every mode."""
+    import json
+
+    from btorch.connectome.connection import (make_constraint_by_neuron_type,
+                                              make_hetersynapse_constrained_conn,
+                                              make_hetersynapse_constraint)
+
+    neu, con = constraint_tables(rng, 60, 500)
+    out = {}
+    for c in neu.columns:
+        out[f"in.neurons.{c}"] = neu[c].to_numpy().astype(np.int64 if neu[c].dtype.kind == "i" else str)
+    for c in con.columns:
+        out[f"in.conns.{c}"] = con[c].to_numpy().astype(np.int64 if con[c].dtype.kind == "i" else str)
+    for g in (True, False):
+        _save_coo(out, f"by_type.{int(g)}", make_constraint_by_neuron_type(neu, con, nan_in_same_group=g))
+    for i, kw in enumerate(CONSTRAINT_RUNS):
+        kw = dict(kw, receptor_type_col="EI" if kw["receptor_type_mode"] == "neuron" else "nt")
+        _save_coo(out, f"hetero.{i}", make_hetersynapse_constraint(neu, con, **kw))
+        out[f"hetero.{i}.kwargs"] = np.array(json.dumps(kw))
+    from btorch.models.linear import SparseConstrainedConn
+
+    for mode in ("cell_only", "cell_and_receptor"):
+        m, c, idx = make_hetersynapse_constrained_conn(neu, con, constraint_mode=mode)
+        _save_coo(out, f"combined.{mode}.conn", m)
+        _save_coo(out, f"combined.{mode}.constraint", c)
+        out[f"combined.{mode}.index"] = np.array(idx.to_json(orient="split"))
+        lin = SparseConstrainedConn.from_hetersynapse(m.astype(np.float32), c, idx, enforce_dale=True)
+        out[f"combined.{mode}.group"] = lin._constraint_scatter_indices.numpy().astype(np.int64)
+        out[f"combined.{mode}.n_groups"] = np.int64(lin.magnitude.numel())
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -554,6 +614,7 @@ def main():
         "receptors2": lambda r: case_receptors(r, n=200, p=0.03, batch=3, steps=100, n_rec=2),
         "connectome_format": lambda r: case_connectome_format(r),
         "receptors_delay": lambda r: case_receptors_delay(r, n=300, n_conn=9000, batch=3, steps=120, D=5),
+        "connectome_constraint": lambda r: case_connectome_constraint(r),
     }
     only = set(args.only.split(",")) if args.only else None
     for i, (name, fn) in enumerate(cases.items()):
