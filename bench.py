@@ -726,10 +726,12 @@ def plain_step(cfg, net, x, lens, args, dev):
 def main():
     args = parse()
     cfg = CONFIGS[args.config]
-    world, rank, local = dist_setup(args)
     if args.impl == "reference":
-        reference_arm(args, cfg, world, rank)
+        # host cores only: rank 0 times the CPU algorithm and the other ranks
+        # exit, so no process group (and no GPU) is set up
+        reference_arm(args, cfg, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
         return
+    world, rank, local = dist_setup(args)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     from btorch_b200.models import environ
