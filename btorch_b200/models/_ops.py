@@ -165,7 +165,9 @@ class SparseMM(torch.autograd.Function):
             L.check(L.lib().bt_spmv_grad_input_t(B, n_in, layout.n_out, layout.csr_ptr.data_ptr(),
                                                  layout.csr_dst.data_ptr(), w_csr.data_ptr(), g.data_ptr(),
                                                  gx.data_ptr(), gT.data_ptr(), s), "bt_spmv_grad_input_t")
-        if ctx.needs_input_grad[1]:
+        if ctx.needs_input_grad[1] and layout.nnz == 0:
+            gw = torch.zeros(0, device=g.device, dtype=torch.float32)
+        elif ctx.needs_input_grad[1]:
             gw = torch.empty(layout.nnz, device=g.device, dtype=torch.float32)
             masks = torch.empty(max(1, n_in * ((B + 31) // 32)), device=g.device, dtype=torch.int32)
             L.check(L.lib().bt_spmv_grad_weight(B, n_in, layout.n_out, layout.csc_ptr.data_ptr(),

@@ -60,6 +60,8 @@ def match(rnn) -> tuple[dict | None, str]:
         return None, "offload / graphs / grad history"
     if syn.linear.in_features != neuron.size or syn.linear.out_features != neuron.size:
         return None, "connectivity shape"
+    if syn.linear.indices.shape[1] == 0:
+        return None, "no synapses"
     paths = {}
     npath = next(name for name, m in rnn.named_modules() if m is neuron)
     spath = next(name for name, m in rnn.named_modules() if m is syn)

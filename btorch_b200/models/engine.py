@@ -101,6 +101,9 @@ def match(rnn) -> tuple[EnginePlan | None, str]:
         return None, "synapse linear is not a SparseConn"
     if conn.bias is not None:
         return None, "SparseConn bias"
+    if conn.indices.shape[1] == 0:
+        # the per-module path runs it (its products read no edge arrays then)
+        return None, "the connection has no synapses"
     n = neuron.size
     if conn.out_features != n * n_rec or conn.in_features != n * (n_bins if hetero else 1):
         return None, "connectivity shape does not match the neuron count"

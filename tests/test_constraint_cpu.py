@@ -170,3 +170,14 @@ def test_error_behaviour():
     # cell types are always read from "cell_type" first
     with pytest.raises(KeyError):
         make_hetersynapse_constraint(neu.rename(columns={"cell_type": "ct"}), con, cell_type_col="ct")
+
+
+def test_empty_connection_table():
+    """An empty table gives empty constraint matrices of the full shape, as
+    in the reference."""
+    neu, con = _toy()
+    con = con.iloc[:0]
+    assert make_constraint_by_neuron_type(neu, con).shape == (4, 4)
+    for mode in ("full", "cell_only", "cell_and_receptor"):
+        c = make_hetersynapse_constraint(neu, con, constraint_mode=mode)
+        assert c.shape == (4, 16) and c.nnz == 0

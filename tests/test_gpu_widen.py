@@ -62,3 +62,47 @@ def test_two_receptor_hetersynapse_matches_reference(direction):
     np.testing.assert_array_equal(st["neuron.v"].cpu().numpy()[:K], d["v"])
     np.testing.assert_array_equal(st["synapse.psc"].cpu().numpy()[:K], d["psc"])
     np.testing.assert_array_equal(st["synapse.base_psc.psc"].cpu().numpy()[:K], d["psc_rec"])
+
+
+@pytest.mark.parametrize("direction", ["gather", "scatter"])
+def test_empty_connection_equals_zero_weight_network(direction):
+    """A connection without synapses (valid in the reference: torch.sparse.mm
+    of an empty matrix) runs on the per-module kernels and gives the same
+    rasters, states and input gradients as the same network with one
+    zero-weight synapse on the fused paths; its weight gradient is empty."""
+    n, B, T = 64, 3, 40
+    rng = np.random.default_rng(5)
+    x = torch.tensor((rng.poisson(0.3, (T, B, n)) * 0.75).astype(np.float32), device=DEV)
+    r = torch.tensor(rng.standard_normal((T, B, n)).astype(np.float32), device=DEV)
+
+    def model(mat):
+        conn = SparseConn(mat, sparse_config={"direction": direction})
+        rnn = RecurrentNN(LIF(n, v_threshold=1.0, v_reset=0.0, tau=20.0, tau_ref=2.0, hard_reset=True),
+                          ExponentialPSC(n, tau_syn=5.0, linear=conn)).to(DEV)
+        init_net_state(rnn, batch_size=B, dtype=torch.float32, device=DEV)
+        return rnn, conn
+
+    empty, c_empty = model(sp.coo_array((n, n), dtype=np.float32))
+    zero, _ = model(sp.coo_array((np.zeros(1, np.float32), ([0], [1])), shape=(n, n)))
+    with torch.no_grad(), environ.context(dt=1.0):
+        z0, s0 = empty(x)
+        z1, s1 = zero(x)
+    assert empty.last_path == "modular" and zero.last_path == "fused"
+    assert torch.equal(z0, z1) and z0.sum() > 0
+    assert s0.keys() == s1.keys()
+    for k in s0:
+        assert torch.equal(s0[k], s1[k]), k
+
+    grads = []
+    for rnn in (empty, zero):
+        init_net_state(rnn, batch_size=B, dtype=torch.float32, device=DEV)
+        xg = x.clone().requires_grad_(True)
+        with environ.context(dt=1.0):
+            z, _ = rnn(xg)
+        (z * r).sum().backward()
+        grads.append(xg.grad)
+    assert empty.last_path == "modular" and zero.last_path == "fused-bptt"
+    assert grads[0].abs().sum() > 0
+    # fused BPTT and per-module backward: same chain, summed in its own order
+    assert (grads[0] - grads[1]).norm() <= 1e-5 * grads[1].norm()
+    assert c_empty.magnitude.grad is not None and c_empty.magnitude.grad.shape == (0,)

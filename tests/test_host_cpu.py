@@ -148,6 +148,24 @@ def test_engine_plan_matching_on_cpu_modules():
     assert plan2 is None and "SparseConn" in why2
 
 
+def test_empty_connection_runs_per_module():
+    """A connection without synapses (valid in the reference) is declined by
+    the fused engine and the fused BPTT, so the per-module kernels run it;
+    its layout keeps non-null padded CSR arrays."""
+    from btorch_b200.models import bptt
+
+    n = 16
+    conn = SparseConn(sp.coo_array((n, n), dtype=np.float32))
+    rnn = RecurrentNN(LIF(n, tau_ref=2.0, hard_reset=True), ExponentialPSC(n, 5.0, conn))
+    plan, why = rnn.fused_plan()
+    assert plan is None and "no synapses" in why
+    paths, why = bptt.match(rnn)
+    assert paths is None and "no synapses" in why
+    lay = build_layout(conn.indices, n, n)
+    assert lay.nnz == 0 and lay.csr_dst.numel() == 4
+    assert np.array_equal(lay.csc_ptr.numpy(), np.zeros(n + 1)) and np.array_equal(lay.csr_ptr.numpy(), np.zeros(n + 1))
+
+
 def test_neuron_desc_cache_follows_parameter_changes():
     """The per-module path's neuron descriptor is cached on the module and
     rebuilt when a parameter is modified in place, rebound, or dt changes."""
