@@ -112,6 +112,46 @@ def set_hidden_states(mod: nn.Module, hidden_states: dict[str, Any], allow_buffe
 set_memory_values = set_hidden_states
 
 
+def named_memory_reset_values(mod: nn.Module, names: Sequence[str] | None = None) -> dict[str, Any]:
+    """Dotted dict of every memory's reset value (base.ResetValue), e.g. to
+    save beside state_dict so a reloaded model resets to the same values
+    (functional.py:311-326); `names` filters like named_hidden_states."""
+    names_set = _strip_self(set(names)) if names is not None else None
+    ret = {}
+    for name, m in mod.named_modules():
+        if not isinstance(m, base.MemoryModule):
+            continue
+        prefix = "" if name == "" else f"{name}."
+        for k, rv in m.memories_rv.items():
+            key = prefix + k
+            if names_set is None or name in names_set or key in names_set:
+                ret[key] = rv
+    return ret
+
+
+def set_memory_reset_values(mod: nn.Module, reset_values: dict[str, Any] | None, strict: bool = True):
+    """Set reset values from a dotted dict (functional.py:329-351): "a.b.v"
+    sets memory v of module a.b (a ResetValue, or a value keeping the
+    registered sizes); a key naming a module ("" or "self" for `mod` itself)
+    takes a dict of that module's memories.  `strict` is passed to
+    set_reset_value."""
+    if reset_values is None:
+        return
+    for name, value in reset_values.items():
+        if value is None:
+            continue
+        path = name.removeprefix("self.").removeprefix("self")
+        parent, _, leaf = path.rpartition(".")
+        owner = mod.get_submodule(parent)
+        if leaf == "" or leaf in owner._modules:
+            target = owner if leaf == "" else owner._modules[leaf]
+            assert isinstance(target, base.MemoryModule), f"{name or 'self'} is not a MemoryModule"
+            target.set_memories_rv(value, strict=strict)
+        else:
+            assert isinstance(owner, base.MemoryModule), f"{parent or 'self'} is not a MemoryModule"
+            owner.set_reset_value(leaf, value, strict=strict)
+
+
 def detach_net(net: nn.Module):
     """Cut the autograd history of every memory (truncated BPTT boundary)."""
     for m in net.modules():
@@ -120,7 +160,8 @@ def detach_net(net: nn.Module):
 
 
 __all__ = ["init_net_state", "reset_net", "reset_net_state", "prepare_sparse_modules", "named_hidden_states",
-           "filter_hidden_states", "set_hidden_states", "detach_net"]
+           "filter_hidden_states", "set_hidden_states", "named_memory_reset_values", "set_memory_reset_values",
+           "detach_net", "reset_rows"]
 
 
 @torch.no_grad()

@@ -570,6 +570,7 @@ def case_connectome_constraint(rng):
         kw = dict(kw, receptor_type_col="EI" if kw["receptor_type_mode"] == "neuron" else "nt")
         _save_coo(out, f"hetero.{i}", make_hetersynapse_constraint(neu, con, **kw))
         out[f"hetero.{i}.kwargs"] = np.array(json.dumps(kw))
+    import torch
     from btorch.models.linear import SparseConstrainedConn
 
     for mode in ("cell_only", "cell_and_receptor"):
@@ -580,6 +581,16 @@ def case_connectome_constraint(rng):
         lin = SparseConstrainedConn.from_hetersynapse(m.astype(np.float32), c, idx, enforce_dale=True)
         out[f"combined.{mode}.group"] = lin._constraint_scatter_indices.numpy().astype(np.int64)
         out[f"combined.{mode}.n_groups"] = np.int64(lin.magnitude.numel())
+        # the inspection helpers after two magnitude edits
+        with torch.no_grad():
+            lin.magnitude.copy_(torch.linspace(0.5, 1.5, lin.magnitude.numel()))
+        lin.set_group_magnitude(group_id=1, value=2.5)
+        lin.set_group_magnitude(receptor_pair=("E", "I"), value=0.25)
+        out[f"combined.{mode}.group_info"] = np.array(lin.get_group_info(include_weights=True).to_json(
+            orient="split", double_precision=15))
+        wbg = lin.get_weights_by_group()
+        out[f"combined.{mode}.by_group_len"] = np.array([len(wbg[g]) for g in sorted(wbg)], np.int64)
+        out[f"combined.{mode}.by_group"] = np.concatenate([wbg[g].detach().numpy() for g in sorted(wbg)])
     return out
 
 

@@ -181,3 +181,38 @@ def test_empty_connection_table():
     for mode in ("full", "cell_only", "cell_and_receptor"):
         c = make_hetersynapse_constraint(neu, con, constraint_mode=mode)
         assert c.shape == (4, 16) and c.nnz == 0
+
+
+@pytest.mark.parametrize("mode", ["cell_only", "cell_and_receptor"])
+def test_group_helpers_match_reference(mode):
+    """get_group_info / set_group_magnitude (by group and by receptor pair) /
+    get_weights_by_group as the reference's (linear.py:763-867)."""
+    import torch
+
+    from btorch_b200.models import SparseConstrainedConn
+
+    neu, con = tables()
+    m, c, idx = make_hetersynapse_constrained_conn(neu, con, constraint_mode=mode)
+    lin = SparseConstrainedConn.from_hetersynapse(m.astype(np.float32), c, idx, enforce_dale=True)
+    with torch.no_grad():
+        lin.magnitude.copy_(torch.linspace(0.5, 1.5, lin.magnitude.numel()))
+    lin.set_group_magnitude(group_id=1, value=2.5)
+    lin.set_group_magnitude(receptor_pair=("E", "I"), value=0.25)
+    got = lin.get_group_info(include_weights=True)
+    want = pd.read_json(io.StringIO(str(G[f"combined.{mode}.group_info"])), orient="split")
+    assert list(got.columns) == list(want.columns)
+    for col in got.columns:
+        if got[col].dtype.kind in "iu" or want[col].dtype.kind in "iu":
+            np.testing.assert_array_equal(got[col].to_numpy(), want[col].to_numpy(), err_msg=col)
+        elif got[col].dtype.kind == "f":
+            np.testing.assert_allclose(got[col].to_numpy(), want[col].to_numpy(), rtol=1e-6, err_msg=col)
+        else:
+            np.testing.assert_array_equal(got[col].astype(str).to_numpy(), want[col].astype(str).to_numpy())
+    wbg = lin.get_weights_by_group()
+    np.testing.assert_array_equal([len(wbg[g]) for g in sorted(wbg)], G[f"combined.{mode}.by_group_len"])
+    np.testing.assert_array_equal(np.concatenate([wbg[g].detach().numpy() for g in sorted(wbg)]),
+                                  G[f"combined.{mode}.by_group"])
+    with pytest.raises(ValueError, match="Exactly one"):
+        lin.set_group_magnitude()
+    with pytest.raises(ValueError, match="Exactly one"):
+        lin.set_group_magnitude(group_id=0, receptor_pair=("E", "E"))
