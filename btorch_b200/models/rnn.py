@@ -6,7 +6,8 @@ gradient is needed; otherwise it steps module by module -- each module's
 step is one of the sm_100a kernels with a hand-written backward -- using the
 reference's chunking: unroll blocks, large chunks with optional gradient
 checkpointing per chunk (truncated-BPTT windows recompute their forward in
-backward) and optional CPU offload of per-chunk outputs (rnn.py:200-332).
+backward), optional CPU offload of per-chunk outputs and the per-step
+gradient history of named states (rnn.py:85-106, 200-332).
 """
 
 from __future__ import annotations
@@ -72,7 +73,33 @@ class RecurrentNNAbstract(base.MemoryModule):
                 raise ValueError(f"chunk_size ({large}) must be a multiple of unroll ({unroll})")
         return T, loop_args, unroll, large, (T + large - 1) // large
 
-    def _process_chunk(self, *chunk_args, loop_args=(0,), **kwargs):
+    def _start_grad_history(self, T: int):
+        """A fresh gradient history per call (rnn.py:255-265): with
+        grad_state_names, one slot per step for each named state (even
+        without save_grad_history); otherwise empty until hooks add states."""
+        if self.save_grad_history:
+            self._grad_history = {}
+        if self.grad_state_names:
+            self._grad_history = {name: [None] * T for name in self.grad_state_names}
+
+    def _hook_grad(self, name: str, tensor, t: int, T: int):
+        """Record the gradient that reaches state `name` of step t -- through
+        the returned stack and through the recurrence (rnn.py:97-106,
+        319-326)."""
+        if not self.save_grad_history or (self.grad_state_names is not None and name not in self.grad_state_names):
+            return
+        slots = self._grad_history.setdefault(name, [None] * T)
+        if torch.is_tensor(tensor) and tensor.requires_grad:
+            def hook(grad):
+                if grad is not None:
+                    slots[t] = grad.detach().clone()
+                return grad
+
+            tensor.register_hook(hook)
+
+    def _process_chunk(self, *chunk_args, loop_args=(0,), grad_steps=None, **kwargs):
+        """Step through one chunk.  grad_steps = (first step, T) registers the
+        gradient-history hooks on each step's states."""
         T = chunk_args[loop_args[0]].shape[0]
         zs, states = [], {}
         a = list(chunk_args)
@@ -83,15 +110,19 @@ class RecurrentNNAbstract(base.MemoryModule):
             zs.append(z)
             for k, v in st.items():
                 states.setdefault(k, []).append(v)
+                if grad_steps is not None:
+                    self._hook_grad(k, v, grad_steps[0] + t, grad_steps[1])
         return zs, states
 
-    def _checkpointed_chunk(self, *chunk_args, loop_args=(0,), **kwargs):
+    def _checkpointed_chunk(self, *chunk_args, loop_args=(0,), grad_steps=None, **kwargs):
         """One chunk under activation checkpointing (rnn.py:177-197): the
         forward keeps only the chunk's inputs and entry state; backward
         recomputes the chunk from them.  The recomputation runs on the
         modules themselves, so it restores the modules' state afterwards --
         the reference leaves them at wherever the (possibly early-stopped)
-        recomputation got to, which truncated BPTT would then continue from."""
+        recomputation got to, which truncated BPTT would then continue from.
+        Gradient-history hooks go on the first run's states: backward runs
+        through that run's graph, the recomputation only refills it."""
         memories = named_hidden_states(self)
         env = environ.all()
         calls = [0]
@@ -103,7 +134,8 @@ class RecurrentNNAbstract(base.MemoryModule):
             try:
                 set_hidden_states(self, memories)
                 with environ.context(**env):
-                    zs, st = self._process_chunk(*inner, loop_args=loop_args, **kwargs)
+                    zs, st = self._process_chunk(*inner, loop_args=loop_args,
+                                                 grad_steps=None if recompute else grad_steps, **kwargs)
                 return torch.stack(zs), {k: torch.stack(v) for k, v in st.items()}
             finally:
                 if recompute:
@@ -114,9 +146,11 @@ class RecurrentNNAbstract(base.MemoryModule):
     def _modular_forward(self, *args, loop_args=None, **kwargs):
         T, loop_args, unroll, large, n_chunks = self._chunk_plan(*args, loop_args=loop_args)
         splits = {i: torch.split(args[i], large, dim=0) for i in loop_args}
+        self._start_grad_history(T)
         all_z, all_st = [], {}
         for c in range(n_chunks):
             cargs = tuple(splits[i][c] if i in loop_args else args[i] for i in range(len(args)))
+            grad_steps = (c * large, T) if self.save_grad_history else None
             if self.cudagraph:
                 def fn(*inner):
                     zs, sts = self._process_chunk(*inner, loop_args=loop_args, **kwargs)
@@ -125,9 +159,9 @@ class RecurrentNNAbstract(base.MemoryModule):
                 # offloading copies out of the graph pool itself
                 z, st = self._cudagraph_runner(self, fn, cargs, clone_outputs=not self.cpu_offload)
             elif self.grad_checkpoint:
-                z, st = self._checkpointed_chunk(*cargs, loop_args=loop_args, **kwargs)
+                z, st = self._checkpointed_chunk(*cargs, loop_args=loop_args, grad_steps=grad_steps, **kwargs)
             else:
-                zs, sts = self._process_chunk(*cargs, loop_args=loop_args, **kwargs)
+                zs, sts = self._process_chunk(*cargs, loop_args=loop_args, grad_steps=grad_steps, **kwargs)
                 z, st = torch.stack(zs), {k: torch.stack(v) for k, v in sts.items()}
             if self.cpu_offload:
                 z = z.cpu()
@@ -194,6 +228,8 @@ class RecurrentNN(RecurrentNNAbstract):
             any(p.requires_grad for p in self.parameters())
             or any(torch.is_tensor(a) and a.requires_grad for a in args))
         extra = len(args) > 1 and any(a is not None for a in args[1:])
+        if torch.is_tensor(args[0]) and args[0].ndim > 0:
+            self._start_grad_history(int(args[0].shape[0]))
         plan, reason = (None, "disabled")
         if self.fused and not needs_grad and not extra and not kwargs and loop_args in (None, (0,)):
             plan, reason = _engine.match(self)
