@@ -81,12 +81,23 @@ def _is_uniform(t: torch.Tensor, atol: float = 1e-6) -> bool:
 
 class ParamBufferMixin(torch.nn.Module):
     """def_param: a named value stored as a trainable Parameter or a buffer, in
-    its compact (scalar) or full per-neuron form (btorch/models/base.py:305-332).
-    Uniform values are saved compactly and broadcast back on load."""
+    its compact (scalar) or full per-neuron form (btorch/models/base.py:75-457).
+
+    Checkpoint shape policy, so that state dicts interchange with the
+    reference's:
+    * only neuron-sized values (sizes == n_neuron) are compacted: a uniform one
+      is saved as a scalar; values with extra axes keep their full shape and a
+      compact checkpoint value is broadcast back to it;
+    * trainable_shape "full" keeps the full shape on load (broadcasting a
+      compact value), "scalar" keeps a scalar -- a non-scalar checkpoint is an
+      error for a trainable scalar and replaces a buffer's storage;
+    * "auto" (and every buffer) becomes a scalar when the loaded value is
+      uniform and takes the loaded shape otherwise."""
 
     def __init__(self, *args, **kwargs):
         super().__init__(*args, **kwargs)
         self._param_shape_mode: dict[str, str] = {}
+        self._param_allow_compact: dict[str, bool] = {}
 
     def _resolve_is_trainable(self, name, trainable_param):
         if isinstance(trainable_param, bool):
@@ -106,8 +117,14 @@ class ParamBufferMixin(torch.nn.Module):
         t = torch.as_tensor(val, **kwargs)
         if t.dtype == torch.float64 and kwargs.get("dtype") is None:
             t = t.to(torch.get_default_dtype())
-        if t.ndim == 1 and t.numel() == int(np.prod(sizes)) and len(sizes) > 1:
-            t = t.reshape(sizes)
+        if len(sizes) > 1:
+            # a flat full value, or one value per neuron without the last axis
+            if t.ndim == 1 and t.numel() == int(np.prod(sizes)):
+                t = t.reshape(sizes)
+            elif t.ndim == len(sizes) - 1 and tuple(t.shape) == sizes[:-1]:
+                t = t[..., None]
+            elif t.ndim == 1 and t.numel() == int(np.prod(sizes[:-1])):
+                t = t.reshape(sizes[:-1] + (1,))
         try:
             torch.broadcast_shapes(tuple(t.shape), sizes)
         except RuntimeError as e:
@@ -123,16 +140,30 @@ class ParamBufferMixin(torch.nn.Module):
         if hasattr(self, name):
             delattr(self, name)
         self._param_shape_mode[name] = trainable_shape if trainable else "auto"
+        self._param_allow_compact[name] = sizes == tuple(getattr(self, "n_neuron", sizes))
         if trainable:
             self.register_parameter(name, torch.nn.Parameter(t))
         else:
             self.register_buffer(name, t, persistent=True)
 
+    def _rebind(self, name: str, value: torch.Tensor):
+        """Replace the storage of `name` (its shape changes), keeping its kind."""
+        cur = getattr(self, name)
+        value = value.detach().clone().to(device=cur.device, dtype=cur.dtype)
+        if name in self._parameters:
+            rg = self._parameters[name].requires_grad
+            delattr(self, name)
+            self.register_parameter(name, torch.nn.Parameter(value, requires_grad=rg))
+        else:
+            persistent = name not in self._non_persistent_buffers_set
+            delattr(self, name)
+            self.register_buffer(name, value, persistent=persistent)
+
     def _save_to_state_dict(self, destination, prefix, keep_vars):
         super()._save_to_state_dict(destination, prefix, keep_vars)
         for name, mode in self._param_shape_mode.items():
             key = prefix + name
-            if mode == "full" or key not in destination:
+            if mode == "full" or not self._param_allow_compact.get(name, True) or key not in destination:
                 continue
             v = destination[key]
             if torch.is_tensor(v) and v.numel() > 1 and _is_uniform(v):
@@ -140,21 +171,29 @@ class ParamBufferMixin(torch.nn.Module):
 
     def _load_from_state_dict(self, state_dict, prefix, local_metadata, strict, missing_keys, unexpected_keys,
                               error_msgs):
-        for name in self._param_shape_mode:
+        for name, mode in self._param_shape_mode.items():
             key = prefix + name
-            if key not in state_dict or not hasattr(self, name):
+            if key not in state_dict or not hasattr(self, name) or not torch.is_tensor(state_dict[key]):
                 continue
             loaded = state_dict[key]
-            cur = getattr(self, name)
-            if torch.is_tensor(loaded) and tuple(loaded.shape) != tuple(cur.shape):
-                new = loaded.detach().clone().to(device=cur.device, dtype=cur.dtype)
-                if name in self._parameters:
-                    rg = self._parameters[name].requires_grad
-                    delattr(self, name)
-                    self.register_parameter(name, torch.nn.Parameter(new, requires_grad=rg))
-                else:
-                    delattr(self, name)
-                    self.register_buffer(name, new, persistent=True)
+            cur_shape, new_shape = tuple(getattr(self, name).shape), tuple(loaded.shape)
+            if mode == "full" or not self._param_allow_compact.get(name, True):
+                if new_shape != cur_shape:
+                    try:
+                        state_dict[key] = torch.broadcast_to(loaded, cur_shape).clone()
+                    except RuntimeError:
+                        self._rebind(name, loaded)
+                continue
+            if loaded.numel() == 1 or (mode == "auto" and _is_uniform(loaded)):
+                scalar = loaded.reshape(-1)[:1].reshape(())
+                state_dict[key] = scalar
+                if cur_shape != ():
+                    self._rebind(name, scalar)
+            elif mode == "scalar" and name in self._parameters:
+                error_msgs.append(f"{key}: received non-scalar checkpoint tensor for trainable_shape='scalar' "
+                                  "trainable parameter.")
+            elif new_shape != cur_shape:
+                self._rebind(name, loaded)
         super()._load_from_state_dict(state_dict, prefix, local_metadata, strict, missing_keys, unexpected_keys,
                                       error_msgs)
 

@@ -594,6 +594,63 @@ def case_connectome_constraint(rng):
     return out
 
 
+STATE_DICT_MODULES = [
+    ("LIF", dict(n_neuron=8)),
+    ("LIF", dict(n_neuron=8, tau=[10.0 + 2.5 * i for i in range(8)], v_threshold=[1.5] * 8, tau_ref=2.0,
+                 trainable_param=["tau"])),
+    ("ALIF", dict(n_neuron=8, tau_adapt=[50.0 + 5 * i for i in range(8)], dg_k=0.3)),
+    ("ExponentialPSC", dict(n_neuron=8, tau_syn=[5.0 + i for i in range(8)])),
+]
+
+
+def _module_kwargs(kw):
+    """JSON-able constructor arguments -> the module's (lists of per-neuron
+    values become tensors, trainable_param a set)."""
+    import torch
+
+    out = {}
+    for k, v in kw.items():
+        if k == "trainable_param":
+            out[k] = set(v)
+        elif isinstance(v, list):
+            out[k] = torch.tensor(v, dtype=torch.float32)
+        else:
+            out[k] = v
+    return out
+
+
+def case_state_dict(rng):
+    """state_dicts of the reference's LIF / ALIF / ExponentialPSC for scalar,
+    uniform and per-neuron parameters, and the parameter shapes after loading
+    a checkpoint into a module built with other values."""
+    import json
+
+    import torch
+    from btorch.models.neurons import ALIF, LIF
+    from btorch.models.synapse import ExponentialPSC
+
+    classes = {"LIF": LIF, "ALIF": ALIF,
+               "ExponentialPSC": lambda **kw: ExponentialPSC(linear=torch.nn.Identity(), **kw)}
+    out = {"modules": np.array(json.dumps(STATE_DICT_MODULES))}
+    for i, (cls, kw) in enumerate(STATE_DICT_MODULES):
+        m = classes[cls](**_module_kwargs(kw))
+        sd = m.state_dict()
+        out[f"m{i}.keys"] = np.array(json.dumps(list(sd)))
+        for k, v in sd.items():
+            out[f"m{i}.{k}"] = v.detach().numpy()
+        # into a module built with the defaults: which shapes the checkpoint gives
+        fresh = classes[cls](n_neuron=8, **({"tau_syn": 5.0} if cls == "ExponentialPSC" else {}))
+        fresh.load_state_dict(sd, strict=False)
+        out[f"m{i}.reloaded"] = np.array(json.dumps({k: list(v.shape) for k, v in fresh.state_dict(keep_vars=True).items()}))
+    # a full uniform value collapses to a scalar, a non-uniform one expands
+    lif = LIF(n_neuron=8)
+    lif.load_state_dict({"tau": torch.full((8,), 25.0)}, strict=False)
+    out["uniform_tau_shape"] = np.array(list(lif.tau.shape), np.int64)
+    lif.load_state_dict({"tau": torch.arange(8.0) + 1}, strict=False)
+    out["nonuniform_tau_shape"] = np.array(list(lif.tau.shape), np.int64)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -626,6 +683,7 @@ def main():
         "connectome_format": lambda r: case_connectome_format(r),
         "receptors_delay": lambda r: case_receptors_delay(r, n=300, n_conn=9000, batch=3, steps=120, D=5),
         "connectome_constraint": lambda r: case_connectome_constraint(r),
+        "state_dict": lambda r: case_state_dict(r),
     }
     only = set(args.only.split(",")) if args.only else None
     for i, (name, fn) in enumerate(cases.items()):

@@ -113,3 +113,99 @@ def test_constrained_get_sparse_matrix():
     torch.testing.assert_close(mat.to_dense(), torch.tensor([[2.0, -9.0], [-10.0, 2.0]]))
     mat.values().sum().backward()
     assert m.magnitude.grad is not None
+
+
+def _module_kwargs(kw):
+    out = {}
+    for k, v in kw.items():
+        if k == "trainable_param":
+            out[k] = set(v)
+        elif isinstance(v, list):
+            out[k] = torch.tensor(v, dtype=torch.float32)
+        else:
+            out[k] = v
+    return out
+
+
+def _build(cls, **kw):
+    from btorch_b200.models import ALIF
+
+    if cls == "ExponentialPSC":
+        return ExponentialPSC(linear=torch.nn.Identity(), **{"tau_syn": 5.0, **kw})
+    return {"LIF": LIF, "ALIF": ALIF}[cls](**kw)
+
+
+def test_state_dicts_interchange_with_the_reference():
+    """The reference's state_dicts (tests/golden/state_dict.npz): the same
+    keys, shapes and values from the same constructor arguments, and loading
+    one into a module built with other values gives the reference's shapes
+    (uniform values compacted to scalars, per-neuron ones kept)."""
+    import json
+
+    from tests import cases
+
+    G = cases.load("state_dict")
+    for i, (cls, kw) in enumerate(json.loads(str(G["modules"]))):
+        m = _build(cls, **_module_kwargs(kw))
+        sd = m.state_dict()
+        keys = json.loads(str(G[f"m{i}.keys"]))
+        assert sorted(sd) == sorted(keys), (cls, kw)
+        for k in keys:
+            np.testing.assert_array_equal(sd[k].detach().numpy(), G[f"m{i}.{k}"], err_msg=f"{cls} {k}")
+            assert tuple(sd[k].shape) == G[f"m{i}.{k}"].shape
+        fresh = _build(cls, n_neuron=8)
+        fresh.load_state_dict({k: torch.tensor(G[f"m{i}.{k}"]) for k in keys}, strict=False)
+        want = json.loads(str(G[f"m{i}.reloaded"]))
+        assert {k: list(v.shape) for k, v in fresh.state_dict(keep_vars=True).items()} == want, (cls, kw)
+    lif = LIF(n_neuron=8)
+    lif.load_state_dict({"tau": torch.full((8,), 25.0)}, strict=False)
+    assert list(lif.tau.shape) == G["uniform_tau_shape"].tolist()
+    lif.load_state_dict({"tau": torch.arange(8.0) + 1}, strict=False)
+    assert list(lif.tau.shape) == G["nonuniform_tau_shape"].tolist()
+
+
+def _param_module(n_neuron, w, **kw):
+    from btorch_b200.models.base import ParamBufferMixin
+
+    class P(ParamBufferMixin):
+        def __init__(self):
+            super().__init__()
+            self.n_neuron = (n_neuron,) if isinstance(n_neuron, int) else tuple(n_neuron)
+            self.def_param("w", w, **kw)
+
+    return P()
+
+
+def test_param_checkpoint_policy():
+    """The reference's shape policy (tests/models/test_param_buffer_mixin.py):
+    extra axes are never compacted; scalar / full trainable shapes hold on
+    load; a trainable scalar rejects a non-scalar checkpoint."""
+    m = _param_module((2, 3), torch.ones(2, 3, 4), sizes=(2, 3, 4))
+    assert m.state_dict()["w"].shape == (2, 3, 4)
+    m.load_state_dict({"w": torch.tensor(5.0)})
+    assert m.w.shape == (2, 3, 4) and torch.all(m.w == 5.0)
+    # one value per neuron without the last axis gets a unit axis
+    assert _param_module(2, torch.tensor([1.0, 2.0]), sizes=(2, 3)).w.shape == (2, 1)
+
+    auto = _param_module(4, 20.0)
+    auto.load_state_dict({"w": torch.full((4,), 20.0)})
+    assert auto.w.shape == ()
+    auto.load_state_dict({"w": torch.tensor([1.0, 2.0, 3.0, 4.0])})
+    assert auto.w.shape == (4,)
+
+    full = _param_module(4, 2.0, trainable_param=True, trainable_shape="full")
+    assert isinstance(full.w, torch.nn.Parameter) and full.w.shape == (4,)
+    full.load_state_dict({"w": torch.tensor(3.0)})
+    assert full.w.shape == (4,) and torch.all(full.w == 3.0)
+
+    with pytest.raises(ValueError, match="must be uniform"):
+        _param_module(4, torch.tensor([1.0, 2.0, 3.0, 4.0]), trainable_param=True, trainable_shape="scalar")
+    scalar = _param_module(4, 2.0, trainable_param=True, trainable_shape="scalar")
+    assert scalar.w.shape == ()
+    scalar.load_state_dict({"w": torch.tensor(3.0)})
+    assert scalar.w.shape == () and scalar.w.item() == 3.0
+    with pytest.raises(RuntimeError, match="non-scalar checkpoint tensor"):
+        scalar.load_state_dict({"w": torch.full((4,), 3.0)})
+    buf = _param_module(4, 2.0, trainable_param=False, trainable_shape="scalar")
+    buf.load_state_dict({"w": torch.tensor([1.0, 2.0, 3.0, 4.0])})
+    assert buf.w.shape == (4,)
