@@ -651,6 +651,30 @@ def case_state_dict(rng):
     return out
 
 
+SURROGATE_RUNS = [dict(alpha=a, damping_factor=d, spiking=sp)
+                  for a in (2.0, 5.0, 0.7) for d in (1.0, 0.3) for sp in (True, False)]
+
+
+def case_surrogate(rng):
+    """The reference's Sigmoid surrogate called directly: forward and the
+    gradient of sum(forward * r) on a seeded grid around the threshold."""
+    import json
+
+    import torch
+    from btorch.models.surrogate import Sigmoid
+
+    x = np.concatenate([np.linspace(-3, 3, 601), rng.standard_normal(400) * 2, [0.0, -0.0]]).astype(np.float32)
+    r = rng.standard_normal(x.size).astype(np.float32)
+    out = {"x": x, "r": r, "runs": np.array(json.dumps(SURROGATE_RUNS))}
+    for i, kw in enumerate(SURROGATE_RUNS):
+        xt = torch.tensor(x, requires_grad=True)
+        y = Sigmoid(**kw)(xt)
+        (y * torch.tensor(r)).sum().backward()
+        out[f"y{i}"] = y.detach().numpy()
+        out[f"g{i}"] = xt.grad.numpy()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -684,6 +708,7 @@ def main():
         "receptors_delay": lambda r: case_receptors_delay(r, n=300, n_conn=9000, batch=3, steps=120, D=5),
         "connectome_constraint": lambda r: case_connectome_constraint(r),
         "state_dict": lambda r: case_state_dict(r),
+        "surrogate": lambda r: case_surrogate(r),
     }
     only = set(args.only.split(",")) if args.only else None
     for i, (name, fn) in enumerate(cases.items()):
