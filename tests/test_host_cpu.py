@@ -85,6 +85,9 @@ def test_sparse_config_registry_semantics():
         reg.backend("cusparse")
     with pytest.raises(ValueError):
         reg.resolve("b200", {"direction": "sideways"})
+    # the process-wide registry modules resolve against (btorch.config.sparse)
+    assert isinstance(config.sparse, SparseConfigRegistry)
+    assert isinstance(config.sparse.backend("triton"), TritonSparseConfig)
 
 
 def test_sparseconn_state_dict_and_prepare_scope():

@@ -11,8 +11,6 @@ caller scratch) bit for bit, and that oversize requests are refused.
 The file is named to be collected last; it passes alone and after the others.
 """
 
-import ctypes as C
-
 import numpy as np
 import pytest
 import scipy.sparse as sp
