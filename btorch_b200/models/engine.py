@@ -196,6 +196,22 @@ def graph_entries(rnn) -> dict:
     return rnn.__dict__.setdefault("_bt_engine_graphs", {})
 
 
+def _check_input(plan: EnginePlan, x: torch.Tensor):
+    """The input shape the kernels index by, checked before any device work:
+    with an input layer, x is [T, *batch, in_features] for the network's
+    batch (the reference's nn.Linear raises on other widths; here a wider row
+    would index past the projection weights)."""
+    if plan.inp is None:
+        return  # [T, *batch, n] or broadcastable: reshape / broadcast_to raise otherwise
+    c_in = plan.inp.in_features
+    if x.ndim < 2 or x.shape[-1] != c_in:
+        raise RuntimeError(f"RecurrentNN input has shape {tuple(x.shape)}; its input layer takes {c_in} channels.")
+    v = plan.neuron.v
+    if torch.is_tensor(v) and v.numel() and x.numel() != x.shape[0] * (v.numel() // plan.neuron.size) * c_in:
+        raise RuntimeError(f"RecurrentNN input of shape {tuple(x.shape)} does not match the network state's batch "
+                           f"{tuple(v.shape[:-1])}.")
+
+
 def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None = None,
         chunk: int | None = None, spikes_out: str = "dense", stats: bool = False, profile: list | None = None,
         chunk_hook=None, choice: _autotune.EngineChoice | None = None):
@@ -216,6 +232,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     that starts at step k0 (e.g. to open a profiler window).
     choice: delivery mode and tiles (default: the autotuner's cached or fresh
     choice for this problem shape, see autotune.py)."""
+    _check_input(plan, x)
     launches = 0
 
     def _ev():

@@ -236,7 +236,11 @@ class SimulationServer:
             synchronize: bool = True) -> ServeReport:
         """Serve `requests` (their `arrival` times are seconds after start)."""
         for r in requests:
-            if self.pools[r.network].request_bytes(r) > self.budget:
+            pool = self.pools[r.network]
+            st = r.stimulus
+            if st.ndim != 2 or st.shape[0] < 1 or st.shape[1] != pool.c_in:
+                raise ValueError(f"request {r.rid}: stimulus must be [steps >= 1, {pool.c_in}], got {tuple(st.shape)}")
+            if pool.request_bytes(r) > self.budget:
                 raise ValueError(f"request {r.rid} needs more device memory than the whole budget")
         arrivals = [(r.arrival, i, r) for i, r in enumerate(requests)]
         heapq.heapify(arrivals)

@@ -221,3 +221,22 @@ def test_fused_bptt_match_rules():
     assert bptt.match(net(cpu_offload=True))[0] is None
     rect = sp.coo_array(sp.random(n, 2 * n, density=0.2, random_state=1, dtype=np.float32))
     assert bptt.match(net(syn=ExponentialPSC(n, 5.0, SparseConn(rect))))[0] is None
+
+
+def test_engine_checks_the_input_shape_before_any_device_work():
+    """With an input layer, x must be [T, *batch, in_features] for the
+    network's batch: a wider row would index past the projection weights."""
+    from btorch_b200.models import DenseConn
+    from btorch_b200.models import engine
+
+    n = 16
+    rnn = RecurrentNN(LIF(n), ExponentialPSC(n, 5.0, SparseConn(sp.coo_array(np.eye(n, dtype=np.float32)))),
+                      neuron_inp_module=DenseConn(4, n))
+    init_net_state(rnn, batch_size=3)
+    plan, _ = rnn.fused_plan()
+    with pytest.raises(RuntimeError, match="takes 4 channels"):
+        engine.run(plan, rnn, torch.zeros(5, 3, 5))
+    with pytest.raises(RuntimeError, match="batch"):
+        engine.run(plan, rnn, torch.zeros(5, 6, 4))
+    with pytest.raises(RuntimeError, match="CUDA"):  # a well-formed input gets as far as the device check
+        engine.run(plan, rnn, torch.zeros(5, 3, 4))

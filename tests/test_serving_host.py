@@ -132,3 +132,14 @@ def test_request_larger_than_budget_is_rejected():
     server = SimulationServer({"a": a}, hbm_budget_bytes=10)
     with pytest.raises(ValueError):
         server.run([req("a", 100, 0.0, 0)], clock=Clock([a]), synchronize=False)
+
+
+def test_malformed_stimulus_is_refused_before_serving():
+    a = FakePool(slots=2, chunk=10)
+    server = SimulationServer({"a": a}, hbm_budget_bytes=1 << 20)
+    for bad in (torch.zeros(10, 5), torch.zeros(10), torch.zeros(0, 4)):
+        with pytest.raises(ValueError, match="stimulus must be"):
+            server.run([SimRequest(network="a", stimulus=bad, rid=7)], clock=Clock([a]))
+    with pytest.raises(KeyError):
+        server.run([req("nope", 10, 0.0, 8)], clock=Clock([a]))
+    assert a.admitted == []
