@@ -199,6 +199,10 @@ class BaseSparseConn(nn.Module):
         no_batch = x.ndim == 1
         if no_batch:
             x = x[None, :]
+        if x.shape[-1] != self.in_features:
+            # (the reference's torch.sparse.mm raises here; the kernels would
+            # index x and the source rows by the layout's width)
+            raise RuntimeError(f"SparseConn takes {self.in_features} input features, got shape {tuple(x.shape)}.")
         leading = x.shape[:-1]
         x2 = x.reshape(-1, x.shape[-1])
         w = self._get_effective_weight()

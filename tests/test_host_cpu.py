@@ -111,6 +111,10 @@ def test_sparseconn_has_no_cpu_path():
     m = SparseConn(sp.coo_array(np.eye(3, dtype=np.float32)))
     with pytest.raises(RuntimeError, match="CUDA"):
         m(torch.ones(3))
+    # a width other than in_features is refused before any kernel sees it
+    for bad in (torch.ones(2), torch.ones(4, 5)):
+        with pytest.raises(RuntimeError, match="takes 3 input features"):
+            m(bad)
 
 
 def test_memory_module_reset_inplace_and_state_names():
