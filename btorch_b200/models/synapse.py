@@ -59,6 +59,10 @@ class ExponentialPSC(BasePSC):
         """(coef, tau) device fp32 vectors for the kernels; coef is rounded on
         the host exactly as the reference computes expm1(dt*lin)/lin."""
         tau = self.tau_syn.detach().float().reshape(-1).contiguous()
+        if tau.numel() not in (1, self.size):
+            # the kernels read one time constant per neuron (the reference's
+            # broadcast against psc raises for other lengths)
+            raise RuntimeError(f"ExponentialPSC tau_syn has {tau.numel()} values; expected 1 or {self.size}.")
         return exp_euler_coef(self.tau_syn, dt, owner=self, name="psc"), tau
 
     def conductance_charge(self):

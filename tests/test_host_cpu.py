@@ -244,3 +244,13 @@ def test_engine_checks_the_input_shape_before_any_device_work():
         engine.run(plan, rnn, torch.zeros(5, 6, 4))
     with pytest.raises(RuntimeError, match="CUDA"):  # a well-formed input gets as far as the device check
         engine.run(plan, rnn, torch.zeros(5, 3, 4))
+
+
+def test_psc_time_constants_must_be_scalar_or_per_neuron():
+    """The kernels read one time constant per neuron: other lengths are refused
+    on the host (the reference's broadcast against psc raises for them)."""
+    for tau in (5.0, torch.full((8,), 5.0)):
+        coef, t = ExponentialPSC(8, tau_syn=tau, linear=torch.nn.Identity()).coefficients(1.0)
+        assert coef.numel() == t.numel() in (1, 8)
+    with pytest.raises(RuntimeError, match="expected 1 or 8"):
+        ExponentialPSC(8, tau_syn=torch.full((3,), 5.0), linear=torch.nn.Identity()).coefficients(1.0)
