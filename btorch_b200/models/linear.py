@@ -286,6 +286,9 @@ class SparseConstrainedConn(BaseSparseConn, HasConstraint):
         if not isinstance(c, scipy.sparse.coo_array):
             c = scipy.sparse.coo_array(c)
         c.eliminate_zeros()
+        if c.nnz and (c.data.min() < 1 or not np.all(np.mod(c.data, 1) == 0)):
+            # ids index the magnitudes on the device (id - 1)
+            raise ValueError("constraint group ids must be integers >= 1 (0 means no constraint)")
         self._constraint_matrix = c
         super().__init__(conn, bias=bias, sparse_backend=sparse_backend, sparse_config=sparse_config,
                          device=device, dtype=dtype)

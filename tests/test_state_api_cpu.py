@@ -209,3 +209,11 @@ def test_param_checkpoint_policy():
     buf = _param_module(4, 2.0, trainable_param=False, trainable_shape="scalar")
     buf.load_state_dict({"w": torch.tensor([1.0, 2.0, 3.0, 4.0])})
     assert buf.w.shape == (4,)
+
+
+def test_constraint_group_ids_must_be_positive_integers():
+    W = sp.coo_array(([1.0, -2.0], ([0, 1], [0, 0])), shape=(2, 2))
+    for bad in ([1, -1], [1, 1.5]):
+        C = sp.coo_array((bad, ([0, 1], [0, 0])), shape=(2, 2))
+        with pytest.raises(ValueError, match="group ids"):
+            SparseConstrainedConn(W, C, enforce_dale=False)
