@@ -198,6 +198,7 @@ def run(rnn, x: torch.Tensor, paths: dict):
     psc0 = syn.psc.reshape(B, n)
     gk0 = neuron.g_k.reshape(B, n) if isinstance(neuron, ALIF) else None
     ref0 = neuron.refractory.reshape(B, n).detach() if neuron._use_refractory else None
+    syn.linear._edge_weight()  # one weight per stored nonzero, or an error before any launch
     outs = _FusedBPTT.apply(P, syn.linear.magnitude, v0, psc0, gk0, ref0, rnn, frozenset(paths.values()))
     Z, Vst, Pst, GKst, REFst, vT, pT, gT, rT = outs
     neuron.v = vT.reshape(shape)

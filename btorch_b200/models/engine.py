@@ -318,7 +318,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         desc.psc_fast_div, desc.psc_rcp = int(ok), r
     desc.mode = mode
     lay = conn.engine_layout(R, plan.uniform_delay, dev)
-    w = static("w", conn._get_effective_weight().detach().float().contiguous())
+    w = static("w", conn._edge_weight().detach().float().contiguous())
     keep.append(w)
     desc.n, desc.batch, desc.n_bins, desc.n_rec = n, B, R, n_rec
     desc.hist_len = H

@@ -161,11 +161,23 @@ class BaseSparseConn(nn.Module):
         self._layout = None
         self._engine_layouts = {}
 
+    def _edge_weight(self) -> torch.Tensor:
+        """The effective weight, one value per stored nonzero in canonical
+        order.  The kernels index it by edge, so a weight whose length is not
+        the number of stored nonzeros (a mismatched checkpoint, a reassigned
+        magnitude) is refused here, where the reference's
+        torch.sparse_coo_tensor raises."""
+        w = self._get_effective_weight()
+        if w.numel() != self.indices.shape[1]:
+            raise RuntimeError(f"{type(self).__name__} has {self.indices.shape[1]} stored nonzeros but "
+                               f"{w.numel()} weights.")
+        return w
+
     # -- prepare scope (linear.py:375-415) -----------------------------------
     def prepare_sparse(self, batch_size: int | None = None) -> None:
         """Pack the effective weight into CSR order once for a multi-step run."""
         if self._prepared_sparse_weight is None and self.indices.is_cuda:
-            w = self._get_effective_weight()
+            w = self._edge_weight()
             self._prepared_sparse_weight = pack_csr_weights(self.layout(w.device), w.float())
         self._sparse_prepare_depth += 1
 
@@ -205,7 +217,7 @@ class BaseSparseConn(nn.Module):
             raise RuntimeError(f"SparseConn takes {self.in_features} input features, got shape {tuple(x.shape)}.")
         leading = x.shape[:-1]
         x2 = x.reshape(-1, x.shape[-1])
-        w = self._get_effective_weight()
+        w = self._edge_weight()
         if w.dtype != torch.float32:
             raise TypeError("SparseConn supports float32 only.")
         lay = self.layout(x2.device) if x2.is_cuda else None

@@ -254,3 +254,13 @@ def test_psc_time_constants_must_be_scalar_or_per_neuron():
         assert coef.numel() == t.numel() in (1, 8)
     with pytest.raises(RuntimeError, match="expected 1 or 8"):
         ExponentialPSC(8, tau_syn=torch.full((3,), 5.0), linear=torch.nn.Identity()).coefficients(1.0)
+
+
+def test_weight_length_must_match_the_stored_nonzeros():
+    m = SparseConn(sp.coo_array(np.eye(4, dtype=np.float32)), enforce_dale=False)
+    assert m._edge_weight().numel() == 4
+    m.magnitude = torch.nn.Parameter(torch.ones(3))
+    with pytest.raises(RuntimeError, match="4 stored nonzeros but 3 weights"):
+        m._edge_weight()
+    with pytest.raises(RuntimeError, match="4 stored nonzeros but 3 weights"):
+        m(torch.ones(2, 4))
