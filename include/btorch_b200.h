@@ -23,6 +23,13 @@
  *                       (post | bin << BT_BIN_SHIFT), csr_perm[nnz] maps a
  *                       CSR position to its canonical index.
  *
+ * Trust boundary: the device entry points check sizes, null pointers and
+ * alignment, but read the contents of the layout arrays (row pointers,
+ * packed ids) as indices without checking them on the device.  Pass arrays
+ * made by bt_layout_build / bt_layout_slices, which reject COO indices that
+ * are out of range or not canonical (BT_ERR_LAYOUT), with the sizes they were
+ * built for, and weight arrays with one value per stored nonzero.
+ *
  * Numerics: every elementwise update is evaluated op by op with IEEE
  * round-to-nearest single precision in the reference's operator order (no
  * contraction to FMA); the ordered gather accumulates each output in
