@@ -332,9 +332,19 @@ def _build_neuron_desc(node, dt: float):
 
     keep = []
     sources = {}
+    nshape = tuple(node.n_neuron)
 
     def P(t, slot=None):
         t = torch.as_tensor(t)
+        if t.numel() != 1:
+            # the kernels read a scalar or one value per neuron: broadcast
+            # anything narrower (a per-axis value) to the neuron shape
+            try:
+                t = torch.broadcast_to(t, nshape)
+            except RuntimeError:
+                raise NotImplementedError(
+                    f"{type(node).__name__}: a parameter of shape {tuple(t.shape)} does not broadcast to the neuron "
+                    f"shape {nshape} (per-sample parameters have no B200 kernel)") from None
         f = _flat(t)
         keep.append(f)
         if slot is not None:

@@ -264,3 +264,19 @@ def test_weight_length_must_match_the_stored_nonzeros():
         m._edge_weight()
     with pytest.raises(RuntimeError, match="4 stored nonzeros but 3 weights"):
         m(torch.ones(2, 4))
+
+
+def test_neuron_parameters_reach_the_kernels_per_neuron():
+    """A parameter narrower than the neuron shape (one value per column of a
+    2-D population) is broadcast to one value per neuron before the kernels
+    read it; per-sample parameters, which the kernels cannot express, are
+    refused instead of being read past their end."""
+    from btorch_b200.models._ops import _build_neuron_desc
+
+    lif = LIF((4, 5), tau=torch.tensor([10.0, 20.0, 30.0, 40.0, 50.0]))
+    _, keep = _build_neuron_desc(lif, 1.0)
+    taus = [k for k in keep if k.numel() == 20 and float(k.max()) == 50.0]
+    assert taus and torch.equal(taus[0].reshape(4, 5), torch.tensor([10.0, 20.0, 30.0, 40.0, 50.0]).expand(4, 5))
+    for bad in (torch.full((2, 8), 20.0), torch.full((3, 1), 20.0)):
+        with pytest.raises(NotImplementedError, match="per-sample"):
+            _build_neuron_desc(LIF(8, tau=bad), 1.0)
