@@ -197,10 +197,20 @@ def graph_entries(rnn) -> dict:
 
 
 def _check_input(plan: EnginePlan, x: torch.Tensor):
-    """The input shape the kernels index by, checked before any device work:
-    with an input layer, x is [T, *batch, in_features] for the network's
-    batch (the reference's nn.Linear raises on other widths; here a wider row
-    would index past the projection weights)."""
+    """The shapes the kernels index by, checked before any device work: every
+    state has the batch of v (a state reset at another batch size would be
+    read past its end), and with an input layer x is [T, *batch,
+    in_features] for that batch (the reference's nn.Linear raises on other
+    widths; here a wider row would index past the projection weights)."""
+    neuron, n = plan.neuron, plan.neuron.size
+    states = [("v", neuron.v, n), ("psc", plan.psc_mod.psc, n * plan.n_rec)]
+    if neuron._use_refractory:
+        states.append(("refractory", neuron.refractory, n))
+    if isinstance(neuron, ALIF):
+        states.append(("g_k", neuron.g_k, n))
+    rows = {name: t.numel() // width for name, t, width in states if torch.is_tensor(t)}
+    if len(set(rows.values())) > 1:
+        raise RuntimeError(f"network states disagree on the batch size {rows}; reset the network with one batch size.")
     if plan.inp is None:
         return  # [T, *batch, n] or broadcastable: reshape / broadcast_to raise otherwise
     c_in = plan.inp.in_features

@@ -280,3 +280,15 @@ def test_neuron_parameters_reach_the_kernels_per_neuron():
     for bad in (torch.full((2, 8), 20.0), torch.full((3, 1), 20.0)):
         with pytest.raises(NotImplementedError, match="per-sample"):
             _build_neuron_desc(LIF(8, tau=bad), 1.0)
+
+
+def test_engine_refuses_states_of_different_batch():
+    from btorch_b200.models import engine
+
+    n = 16
+    rnn = RecurrentNN(LIF(n, tau_ref=2.0), ExponentialPSC(n, 5.0, SparseConn(sp.coo_array(np.eye(n, dtype=np.float32)))))
+    init_net_state(rnn, batch_size=3)
+    rnn.synapse.reset(batch_size=5)
+    plan, _ = rnn.fused_plan()
+    with pytest.raises(RuntimeError, match="disagree on the batch size"):
+        engine.run(plan, rnn, torch.zeros(4, 3, n))
