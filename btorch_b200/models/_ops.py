@@ -438,6 +438,10 @@ class NeuronStep(torch.autograd.Function):
 
 def neuron_step(node, x, v, ref, gk, dt):
     """(spike, v, ref, gk) after one step, as new tensors."""
+    for t in (x, v, ref, gk):
+        if t is not None and t.shape != x.shape:  # the launch covers x's rows in every array
+            raise RuntimeError(f"{type(node).__name__}: state of shape {tuple(t.shape)} does not match the input "
+                               f"{tuple(x.shape)}; reset the network with one batch size.")
     L.require_cuda(x, v, what=type(node).__name__)
     for t in (x, v, ref, gk):
         if t is not None and t.dtype != torch.float32:

@@ -292,3 +292,14 @@ def test_engine_refuses_states_of_different_batch():
     plan, _ = rnn.fused_plan()
     with pytest.raises(RuntimeError, match="disagree on the batch size"):
         engine.run(plan, rnn, torch.zeros(4, 3, n))
+
+
+def test_neuron_step_refuses_states_of_another_batch():
+    from btorch_b200.models._ops import neuron_step
+
+    lif = LIF(8, tau_ref=2.0)
+    x, v = torch.zeros(3, 8), torch.zeros(3, 8)
+    with pytest.raises(RuntimeError, match="does not match the input"):
+        neuron_step(lif, x, v, torch.zeros(5, 8), None, 1.0)
+    with pytest.raises(RuntimeError, match="CUDA"):  # matching shapes get as far as the device check
+        neuron_step(lif, x, v, torch.zeros(3, 8), None, 1.0)
