@@ -303,3 +303,23 @@ def test_neuron_step_refuses_states_of_another_batch():
         neuron_step(lif, x, v, torch.zeros(5, 8), None, 1.0)
     with pytest.raises(RuntimeError, match="CUDA"):  # matching shapes get as far as the device check
         neuron_step(lif, x, v, torch.zeros(3, 8), None, 1.0)
+
+
+def test_product_package_never_reaches_the_oracle():
+    """The oracle is test infrastructure: no module of the package imports,
+    loads or names it, so the product path cannot route through it (tests,
+    smoke() and the bench's CPU arms are its only callers)."""
+    pkg = ROOT / "btorch_b200"
+    offenders = [str(p.relative_to(ROOT)) for p in pkg.rglob("*")
+                 if p.suffix in (".py", ".cu", ".cuh", ".cpp", ".h")
+                 and re.search(r"\boracle\b|liboracle|orc_run", p.read_text())]
+    assert offenders == []
+    import subprocess
+    import sys
+
+    # a fresh interpreter importing the whole module API loads no oracle module
+    code = ("import sys, btorch_b200, btorch_b200.models, btorch_b200.serving, btorch_b200.io, "
+            "btorch_b200.connectome; print(any(m == 'oracle' or m.startswith('oracle.') for m in sys.modules))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert out.stdout.strip().splitlines()[-1] == "False"
