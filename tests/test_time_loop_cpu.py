@@ -150,3 +150,45 @@ def test_make_rnn_forms():
         assert m(torch.randn(4, 2, 3))[0].shape == (4, 2, 4)
     with pytest.raises(TypeError):
         make_rnn(3)
+
+
+class GainCell(MemoryModule):
+    """h <- tanh(W_x x + W_h h) * g, with g either per step or fixed."""
+
+    def __init__(self, n_in, n_h):
+        super().__init__()
+        self.inner = TanhCell(n_in, n_h)
+        self.register_memory("h", torch.zeros(1), n_h)
+
+    def single_step_forward(self, x, g):
+        self.h = self.inner.single_step_forward(x) * g
+        return self.h
+
+
+def _manual(cell, x, g, stepped, B):
+    reset_net_state(cell, batch_size=B)
+    return torch.stack([cell(x[t], g[t] if stepped else g).clone() for t in range(x.shape[0])])
+
+
+@pytest.mark.parametrize("chunk", [None, 3])
+def test_loop_args_step_time_indexed_inputs_only(chunk):
+    """Arguments whose first axis has the first argument's length are stepped,
+    the others are passed to every step unchanged (rnn.py:69-80), also across
+    chunks, and loop_args= overrides the detection."""
+    torch.manual_seed(3)
+    rnn = make_rnn(GainCell, unroll=1, chunk_size=chunk)(3, 4)
+    T, B = 7, 2
+    x = torch.randn(T, B, 3)
+    for g, stepped in ((torch.rand(T, B, 4) + 0.5, True), (torch.rand(B, 4) + 0.5, False)):
+        reset_net_state(rnn, batch_size=B)
+        out, _ = rnn(x, g)
+        torch.testing.assert_close(out, _manual(rnn.rnn_cell, x, g, stepped, B), atol=1e-6, rtol=0)
+    # with as many samples as steps a per-sample gain [B, 4] looks time-indexed:
+    # detection steps it, loop_args=(0,) keeps it fixed
+    B = T
+    x = torch.randn(T, B, 3)
+    g = torch.rand(B, 4) + 0.5
+    for loop_args, stepped in ((None, True), ((0,), False)):
+        reset_net_state(rnn, batch_size=B)
+        out, _ = rnn(x, g, loop_args=loop_args)
+        torch.testing.assert_close(out, _manual(rnn.rnn_cell, x, g, stepped, B), atol=1e-6, rtol=0)
