@@ -95,7 +95,10 @@ def parse():
     ap.add_argument("--no-cudagraph", action="store_true", help="launch every chunk eagerly")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample-steps", type=int, default=2, help="time steps per CPU-port sample")
+    ap.add_argument("--cpu-prewarm-steps", type=int, default=20,
+                    help="untimed CPU-port steps from rest before its samples (past the start-up burst)")
+    ap.add_argument("--no-parity", action="store_true", help="skip the parity checks against the oracle")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--ncu-window", type=int, default=None,
                     help="profile only time steps [S, S+64) (S a multiple of 64) of one extra batch after "
@@ -492,26 +495,175 @@ def oracle_spec(cfg, net):
                      max_delay=net["n_bins"] - 1)
 
 
-def cpu_sample(cfg, net, x_cpu, steps):
-    """Oracle port of the reference's CPU step on the first `steps` time steps
-    of the batch; returns (events, seconds, threads)."""
+class CpuPort:
+    """The oracle's port of the reference's CPU step -- every synapse every
+    step, as torch.sparse.mm computes it, and the dense input layer's
+    projection -- on all host threads, its state carried from one sample of
+    time steps to the next (so a sample can start past the start-up burst)."""
+
+    def __init__(self, cfg, net, batch):
+        from oracle import oracle as O
+
+        self.O = O
+        self.cfg, self.net = cfg, net
+        self.spec = oracle_spec(cfg, net)
+        self.state = O.init_state(self.spec, batch)
+        self.threads = os.cpu_count() or 1
+        self.outdeg = np.bincount(net["pre"], minlength=cfg["n"]).astype(np.int64)
+        self.steps = 0
+
+    def advance(self, x_cpu):
+        """Run len(x_cpu) steps; returns (synaptic events, seconds, spikes uint8 [S, B, n])."""
+        S, B = x_cpu.shape[:2]
+        t0 = time.perf_counter()
+        if self.net["w_in"] is not None:
+            xp = self.O.linear_t(x_cpu.reshape(S * B, -1), self.net["w_in"], threads=self.threads).reshape(S, B, -1)
+        else:
+            xp = x_cpu
+        out = self.O.run(self.spec, self.state, xp, threads=self.threads)
+        dt = time.perf_counter() - t0
+        self.steps += S
+        events = int((out["spikes"].astype(np.int64) * self.outdeg[None, None, :]).sum())
+        return events, dt, out["spikes"]
+
+
+def cpu_sample(cfg, net, x_cpu, steps, prewarm=0):
+    """The port on `steps` time steps of the batch after `prewarm` untimed
+    ones (x_cpu holds prewarm + steps); returns (events, seconds, threads,
+    spikes of the timed steps)."""
+    port = CpuPort(cfg, net, x_cpu.shape[1])
+    if prewarm:
+        port.advance(x_cpu[:prewarm])
+    e, t, z = port.advance(x_cpu[prewarm:prewarm + steps])
+    return e, t, port.threads, z
+
+
+def host_inputs(cfg, seed, steps):
+    """Seeded host-side input of the workload's shape for `steps` steps (the
+    reference arm has no GPU): per-sample Poisson rates over the input
+    channels, or the background drive."""
+    rng = np.random.default_rng(10_000 + seed)
+    B = cfg["batch"]
+    if cfg["model"] in ("alif_dense_input",):
+        rates = rng.uniform(*cfg["rate"], size=B)
+        return rng.poisson(np.broadcast_to((rates * 1e-3)[None, :, None], (steps, B, cfg["c_in"]))).astype(np.float32)
+    if cfg["model"] == "lif_plain":
+        return rng.poisson(cfg["in_rate"], (steps, B, cfg["c_in"])).astype(np.float32)
+    lam, amp = cfg["drive"]
+    return (rng.poisson(lam, (steps, B, cfg["n"])) * amp).astype(np.float32)
+
+
+# -------------------------------------------------------------- parity --
+#
+# The checker: the engine on the configurations' own networks and inputs at
+# their full sizes, against the oracle (event-driven push, bit-identical to
+# the reference's per-synapse chain), outside every timed region.
+
+
+def raster_bits(raster, n):
+    """[T, B, ceil(n/32)] int32 bitmask raster (device or host) -> uint8 [T, B, n]."""
+    r = raster.cpu().numpy() if torch.is_tensor(raster) else raster
+    return np.unpackbits(np.ascontiguousarray(r).view(np.uint8), axis=-1, bitorder="little")[..., :n]
+
+
+def engine_window(cfg, net, x, lens, dev, direction, steps, trace_v=False, cudagraph=True):
+    """A fresh model of the workload run for `steps` steps on x[:steps].
+    Returns (spikes uint8 [steps, B, n], final state dict of numpy arrays,
+    v trace or None, the model's delivery direction)."""
+    from btorch_b200.models import environ
+    from btorch_b200.models import engine as E
+
+    rnn = build_model(cfg, net, dev, direction)
+    rnn.cudagraph = cudagraph
+    if trace_v:
+        rnn.update_state_names = ("neuron.v",)
+    sl = None if lens is None else lens.clamp(max=steps)
+    with torch.inference_mode(), environ.context(dt=1.0):
+        raster, st = rnn(x[:steps].contiguous(), sample_len=sl, spikes_out="bitmask")
+    plan, _ = E.match(rnn)
+    final = {"v": rnn.neuron.v, "psc": plan.psc_mod.psc, "ref": rnn.neuron.refractory}
+    if cfg["model"] == "alif_dense_input":
+        final["gk"] = rnn.neuron.g_k
+    final = {k: t.reshape(t.shape[0], -1).cpu().numpy() for k, t in final.items()}
+    vtr = st["neuron.v"].cpu().numpy() if trace_v else None
+    direction = rnn.last_engine_direction
+    del rnn
+    return raster_bits(raster, cfg["n"]), final, vtr, direction
+
+
+def oracle_window(cfg, net, x_host, steps, lens=None, trace_v=False):
+    """The oracle over the same steps (event-driven push; the projection of a
+    dense input layer as the ascending-channel chain the engine uses)."""
     from oracle import oracle as O
 
-    n, B = cfg["n"], cfg["batch"]
-    spec = oracle_spec(cfg, net)
     threads = os.cpu_count() or 1
-    st = O.init_state(spec, B)
-    outdeg = np.bincount(net["pre"], minlength=n).astype(np.int64)
-    t0 = time.perf_counter()
+    spec = oracle_spec(cfg, net)
+    B = x_host.shape[1]
     if net["w_in"] is not None:
-        xin = x_cpu[:steps].reshape(steps * B, -1)
-        xp = O.linear(xin, net["w_in"].T.copy()).reshape(steps, B, n)
+        xp = O.linear_t(x_host[:steps].reshape(steps * B, -1), net["w_in"], threads=threads).reshape(steps, B, -1)
     else:
-        xp = x_cpu[:steps]
-    out = O.run(spec, st, xp, threads=threads)
-    dt = time.perf_counter() - t0
-    events = int((out["spikes"].astype(np.int64) * outdeg[None, None, :]).sum())
-    return events, dt, threads
+        xp = x_host[:steps]
+    st = O.init_state(spec, B)
+    sl = None if lens is None else np.minimum(np.asarray(lens), steps).astype(np.int32)
+    out = O.run(spec, st, xp, sample_len=sl, threads=threads, want_v=trace_v, events=True)
+    final = {"v": st.v, "psc": st.psc, "ref": st.ref}
+    if spec.kind == 1:
+        final["gk"] = st.gk
+    return out["spikes"], final, out["v"]
+
+
+def first_divergence(a, b):
+    """First step at which two [T, B, n] rasters differ (T if never)."""
+    bad = np.nonzero((a != b).reshape(len(a), -1).any(1))[0]
+    return int(bad[0]) if bad.size else len(a)
+
+
+def _sample_divergence(a, b):
+    """Per sample: the first step at which its rasters differ (T if never)."""
+    T, B = a.shape[:2]
+    bad = (a != b).any(-1)  # [T, B]
+    return np.where(bad.any(0), bad.argmax(0), T)
+
+
+def parity_bitwise(name, cfg, net, x, lens, dev, steps, direction):
+    """Rasters of every step and the final state bit for bit (dyadic
+    weights, or an ordered delivery mode)."""
+    t0 = time.perf_counter()
+    z, fin, _, used = engine_window(cfg, net, x, lens, dev, direction, steps)
+    oz, ofin, _ = oracle_window(cfg, net, x.cpu().numpy() if torch.is_tensor(x) else x, steps,
+                                None if lens is None else lens.cpu().numpy())
+    k = first_divergence(z, oz)
+    state_equal = {key: bool(np.array_equal(fin[key], ofin[key])) for key in ofin if ofin[key] is not None}
+    ok = k == steps and all(state_equal.values())
+    return {"check": "bitwise" if ok else "MISMATCH", "steps": steps, "direction": used,
+            "rasters_equal_steps": k, "final_state_equal": state_equal, "spikes": int(oz.sum()),
+            "seconds": round(time.perf_counter() - t0, 1)}
+
+
+def parity_tolerance(name, cfg, net, x, lens, dev, steps, direction, rtol=1e-5):
+    """Non-dyadic weights summed in arrival order: per sample, the raster
+    equal and v within rel `rtol` (atol rtol) of the oracle until that
+    sample's first spike divergence."""
+    t0 = time.perf_counter()
+    z, _, vtr, used = engine_window(cfg, net, x, lens, dev, direction, steps, trace_v=True)
+    oz, _, ov = oracle_window(cfg, net, x.cpu().numpy() if torch.is_tensor(x) else x, steps,
+                              None if lens is None else lens.cpu().numpy(), trace_v=True)
+    ks = _sample_divergence(z, oz)
+    worst = 0.0
+    ok = True
+    for b, k in enumerate(ks):
+        if k == 0:
+            continue
+        a, r = vtr[:k, b].astype(np.float64), ov[:k, b].astype(np.float64)
+        err = np.abs(a - r) / (np.abs(r) + rtol)
+        worst = max(worst, float(err.max()))
+        ok &= bool(np.all(np.abs(a - r) <= rtol * np.abs(r) + rtol))
+    ok &= bool(ks.min() >= 1)
+    return {"check": f"within rel {rtol:g} until divergence" if ok else "MISMATCH", "steps": steps,
+            "direction": used, "first_divergence": int(ks.min()),
+            "median_sample_divergence": float(np.median(ks)), "samples_never_diverged": int((ks == steps).sum()),
+            "max_rel_err_before_divergence": worst, "spikes": int(oz.sum()),
+            "seconds": round(time.perf_counter() - t0, 1)}
 
 
 # ---------------------------------------------------------------- main --
@@ -531,33 +683,46 @@ def dist_setup(args):
 
 
 def reference_arm(args, cfg, world, rank):
+    """The reference's CPU algorithm (the oracle's port of btorch's native
+    backend: torch.sparse.mm over every synapse each step, eager neuron and
+    synapse updates, the dense input layer), on all host threads.  The
+    simulation starts from rest and first runs --cpu-prewarm-steps untimed
+    steps, past the network's start-up burst; each bench step then advances
+    it by --cpu-sample-steps time steps of the whole batch.  The reference
+    package itself cannot be installed here (its build backend is not in the
+    offline wheel set), so its own modules do not run on this host."""
     if rank != 0:
         return
     net = make_network(cfg, args.seed)
-    rng = np.random.default_rng(10_000 + args.seed)
-    S = args.cpu_sample_steps
-    B = cfg["batch"]
-    if net["w_in"] is not None:
-        rates = rng.uniform(*cfg["rate"], size=B)
-        x = rng.poisson(np.broadcast_to((rates * 1e-3)[None, :, None], (S, B, cfg["c_in"]))).astype(np.float32)
-    else:
-        lam, amp = cfg["drive"]
-        x = (rng.poisson(lam, (S, B, cfg["n"])) * amp).astype(np.float32)
-    for _ in range(min(args.warmup, 1)):
-        cpu_sample(cfg, net, x, 1)
-    tot_e, tot_t, thr = 0, 0.0, 1
+    P, S = args.cpu_prewarm_steps, args.cpu_sample_steps
+    x = host_inputs(cfg, args.seed, P + (args.warmup + args.steps) * S)
+    port = CpuPort(cfg, net, cfg["batch"])
+    if P:
+        port.advance(x[:P])
+    k = P
+    for _ in range(args.warmup):
+        port.advance(x[k:k + S])
+        k += S
+    tot_e, tot_t = 0, 0.0
     for _ in range(args.steps):
-        e, t, thr = cpu_sample(cfg, net, x, S)
+        e, t, _ = port.advance(x[k:k + S])
+        k += S
         tot_e += e
         tot_t += t
     val = tot_e / tot_t
-    sample = f"{S} time steps of the {B}-sample batch per step (of up to {cfg['t_max']})"
+    B = cfg["batch"]
+    sample = (f"{S} time steps of the {B}-sample batch per step (of up to {cfg['t_max']}), after {P} untimed "
+              f"steps from rest and {args.warmup} warm-up steps")
     line = {"metric": "synaptic_events_per_s", "value": val, "unit": "events/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": describe(args.config, cfg), "parallelism": "replicas"},
-            "cpu_baseline": {"value": val, "unit": "events/s", "cores": thr, "kind": "port", "sample": sample},
+            "neuron_steps_per_s": cfg["n"] * B * S * args.steps / tot_t,
+            "cpu_baseline": {"value": val, "unit": "events/s", "cores": port.threads, "kind": "port",
+                             "sample": sample,
+                             "note": "the reference package cannot be installed offline (build backend hatchling "
+                                     "absent), so its algorithm runs as the oracle's C port"},
             "e2e": {"value": val, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -599,7 +764,8 @@ def _allreduce(v, dev, op):
 
 def measure(name, cfg, args, dev, world, rank, local):
     """Time args.steps whole batches of workload `name`.  Returns (line dict,
-    or None on ranks > 0; model; input; lengths; network; step function)."""
+    or None on ranks > 0; model; input; lengths; network; step function; the
+    last timed batch's bitmask raster)."""
     from btorch_b200.models import environ
     from btorch_b200.models.functional import reset_net
 
@@ -630,8 +796,9 @@ def measure(name, cfg, args, dev, world, rank, local):
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         ev_start.record(stream)
+        last_raster = None
         for _ in range(args.steps):
-            one_step(x)
+            last_raster = one_step(x)
             stats_list.append(rnn.last_engine_stats.clone())
         ev_end.record(stream)
         torch.cuda.synchronize()
@@ -688,7 +855,7 @@ def measure(name, cfg, args, dev, world, rank, local):
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
-    return line, rnn, x, lens, net, one_step
+    return line, rnn, x, lens, net, one_step, last_raster
 
 
 def plain_step(cfg, net, x, lens, args, dev):
@@ -703,7 +870,7 @@ def plain_step(cfg, net, x, lens, args, dev):
     def go():
         reset_net(m, inplace=True)
         with torch.inference_mode(), environ.context(dt=1.0):
-            m(x1, sample_len=l1, spikes_out="bitmask", engine_stats=True)
+            return m(x1, sample_len=l1, spikes_out="bitmask", engine_stats=True)[0]
 
     for _ in range(2):
         go()
@@ -712,15 +879,16 @@ def plain_step(cfg, net, x, lens, args, dev):
     stream = torch.cuda.current_stream(dev)
     ev = 0
     e0.record(stream)
+    raster = None
     for _ in range(args.steps):
-        go()
+        raster = go()
         ev += m.last_engine_stats[:, 1].sum()
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     return {"value": int(ev) / (ms * 1e-3), "unit": "events/s", "ms_per_step": ms / args.steps,
             "batch": 1, "cudagraph": False, "direction": m.last_engine_direction,
-            "gpu_launches": m.last_engine_launches * args.steps}
+            "gpu_launches": m.last_engine_launches * args.steps, "_raster": raster}
 
 
 def main():
@@ -737,7 +905,8 @@ def main():
     from btorch_b200.models import environ
     from btorch_b200.models.functional import reset_net
 
-    line, rnn, x, lens, net, one_step = measure(args.config, cfg, args, dev, world, rank, local)
+    line, rnn, x, lens, net, one_step, _ = measure(args.config, cfg, args, dev, world, rank, local)
+    checks = rank == 0 and world == 1 and not args.no_parity
     stream = torch.cuda.current_stream(dev)
     T, B, n = cfg["t_max"], cfg["batch"], cfg["n"]
     # e2e: host buffers through the public API -- the input in pinned host
@@ -793,13 +962,22 @@ def main():
                 engine_choice=parse_choice(args.engine_choice))
         torch.cuda.synchronize()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        S = args.cpu_sample_steps
-        x_cpu = x[:S].cpu().numpy()
-        e, t, thr = cpu_sample(cfg, net, x_cpu, S)
+        S, P = args.cpu_sample_steps, args.cpu_prewarm_steps
+        x_cpu = x[:P + S].cpu().numpy()
+        e, t, thr, _ = cpu_sample(cfg, net, x_cpu, S, prewarm=P)
         line["cpu_baseline"] = {"value": e / t, "unit": "events/s", "cores": thr, "kind": "port",
-                                "sample": f"first {S} time steps of the {B}-sample batch ({t:.1f} s)"}
-    del rnn, x, lens, net, one_step
+                                "sample": f"time steps {P}..{P + S - 1} of the {B}-sample batch, after {P} "
+                                          f"untimed steps from rest ({t:.1f} s)",
+                                "neuron_steps_per_s": n * B * S / t}
+    del rnn, one_step
     torch.cuda.empty_cache()
+    parity = {}
+    if checks and cfg["model"] == "alif_dense_input":
+        # the start-up burst of the headline workload (dense steps included)
+        parity[f"{args.config}_100"] = parity_tolerance(args.config, cfg, net, x, lens, dev, min(100, T),
+                                                          args.direction)
+        torch.cuda.empty_cache()
+    del x, lens, net
     for extra in [e for e in args.extra.split(",") if e and e != args.config]:
         ecfg = CONFIGS[extra]
         if ecfg["model"] in ("lif_train", "serving"):
@@ -808,22 +986,45 @@ def main():
                 line[extra] = sub
             torch.cuda.empty_cache()
             continue
-        sub, m, xe, le, ne, _ = measure(extra, ecfg, args, dev, world, rank, local)
+        sub, m, xe, le, ne, _, raster = measure(extra, ecfg, args, dev, world, rank, local)
         if rank == 0 and world == 1 and ecfg["batch"] > 1 and ecfg.get("receptors", 1) == 1:
             sub["plain_step"] = plain_step(ecfg, ne, xe, le, args, dev)
             sub["vs_plain_step"] = sub["value"] / sub["plain_step"]["value"]
+            # "at identical spike rasters": the plain step's raster is sample 0's of the batched run
+            one = raster_bits(sub["plain_step"].pop("_raster"), ecfg["n"])[:, 0]
+            k = first_divergence(one[:, None], raster_bits(raster, ecfg["n"])[:, :1])
+            sub["plain_step"]["raster_equals_batch_sample0"] = bool(k == len(one))
+            sub["plain_step"]["raster_equal_steps"] = k
         if rank == 0 and world == 1 and ecfg["model"] == "lif_plain" and not args.no_cpu_baseline:
-            # the reference's CPU case at full length
-            e, t, thr = cpu_sample(ecfg, ne, xe.cpu().numpy(), ecfg["t_max"])
+            # the reference's CPU case at full length (its spike raster is kept
+            # for the comparison with the timed scatter run below)
+            e, t, thr, z_port = cpu_sample(ecfg, ne, xe.cpu().numpy(), ecfg["t_max"])
             sub["cpu_baseline"] = {"value": e / t, "unit": "events/s", "cores": thr, "kind": "port",
                                    "sample": f"all {ecfg['t_max']} steps ({t:.2f} s)", "ms_per_step": 1e3 * t / ecfg["t_max"]}
+            if checks:
+                # the port forms W z over every synapse in the reference's order;
+                # the timed run sums non-dyadic weights in arrival order
+                parity[f"{extra}_timed_vs_port_raster_equal_steps"] = first_divergence(
+                    raster_bits(raster, ecfg["n"]), z_port)
+        del raster
+        del m
+        torch.cuda.empty_cache()
+        if checks and ecfg["model"] == "lif_plain":
+            parity[f"{extra}_gather"] = parity_bitwise(extra, ecfg, ne, xe, le, dev, ecfg["t_max"], "gather")
+            parity[f"{extra}_scatter"] = parity_tolerance(extra, ecfg, ne, xe, le, dev, ecfg["t_max"], "scatter")
+        if checks and ecfg["model"] == "lif_hetero_delay":
+            parity[f"{extra}_200"] = parity_bitwise(extra, ecfg, ne, xe, le, dev, min(200, ecfg["t_max"]),
+                                                   args.direction)
+        torch.cuda.empty_cache()
         if rank == 0:
             for k in ("metric", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline",
                       "dtype", "data"):
                 sub.pop(k, None)
             line[extra] = sub
-        del m, xe, le, ne
+        del xe, le, ne
         torch.cuda.empty_cache()
+    if checks:
+        line["parity"] = parity
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

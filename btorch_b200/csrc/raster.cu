@@ -80,9 +80,10 @@ extern "C" int bt_raster_count(int64_t rows, int64_t n, const uint32_t* bits, in
 
 extern "C" int bt_raster_coords(int64_t rows, int64_t batch, int64_t n, const uint32_t* bits, const int64_t* offsets,
                                 int32_t* idx_time, int32_t* idx_batch, int32_t* idx_neuron, void* stream) {
-  BT_CHECK_ARG(rows >= 0 && n >= 0 && batch > 0 && rows % batch == 0, "rows must be a multiple of batch");
+  BT_CHECK_ARG(rows >= 0 && n >= 0, "negative size");
+  if (rows == 0) return BT_OK;  // an empty raster (T = 0 or batch = 0) has no coordinates
+  BT_CHECK_ARG(batch > 0 && rows % batch == 0, "rows must be a multiple of batch");
   BT_CHECK_ARG(n < (int64_t(1) << 31) && rows / batch < (int64_t(1) << 31), "coordinates exceed int32");
-  if (rows == 0) return BT_OK;
   BT_CHECK_ARG(bits && offsets && idx_time && idx_batch && idx_neuron, "null pointer");
   k_raster_coords<<<int(ceil_div(rows * 32, 256)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       rows, batch, n, bits, offsets, idx_time, idx_batch, idx_neuron);

@@ -373,6 +373,9 @@ uint32_t* g_noalloc_addr[kNoAllocMaxDevices] = {};
 // Device address of g_noalloc_gather_bits on the current device.  The array's
 // name in host code is only a host-side stand-in, so the address must come
 // from cudaGetSymbolAddress, looked up once per device with that device current.
+// The address is cached for the life of the process: it is not looked up
+// again after cudaDeviceReset or after the primary context is destroyed and
+// recreated, so the library must not be used across such a reset.
 int noalloc_scratch(uint32_t** out) {
   int dev = 0;
   cudaError_t err = cudaGetDevice(&dev);
@@ -398,11 +401,13 @@ extern "C" int bt_spmv_gather_noalloc(int64_t batch, int64_t n_in, int64_t n_out
   BT_CHECK_ARG(batch >= 0 && n_in >= 0 && n_out >= 0, "negative size");
   BT_CHECK_ARG(n_in < BT_MAX_NEURONS && n_out < BT_MAX_NEURONS, "sizes must be below 2^25");
   const int64_t words = ceil_div(n_in, 32);
-  BT_CHECK_ARG(batch * words <= BT_NOALLOC_GATHER_MAX_WORDS,
-               "batch * ceil(n_in / 32) = %lld exceeds the built-in scratch of %d words; use bt_spmv_gather",
-               (long long)(batch * words), BT_NOALLOC_GATHER_MAX_WORDS);
+  // compare without forming batch * words first: a huge batch must not wrap
+  // the product back under the limit
+  BT_CHECK_ARG(words == 0 || batch <= BT_NOALLOC_GATHER_MAX_WORDS / words,
+               "batch %lld x ceil(n_in / 32) = %lld words exceeds the built-in scratch of %d words; use "
+               "bt_spmv_gather", (long long)batch, (long long)words, BT_NOALLOC_GATHER_MAX_WORDS);
   if (batch == 0 || n_out == 0) return BT_OK;
-  BT_CHECK_ARG(csc_ptr && x && out, "null pointer");
+  BT_CHECK_ARG(csc_ptr && out && (n_in == 0 || x), "null pointer");
   uint32_t* bits = nullptr;
   if (int st = noalloc_scratch(&bits)) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -135,9 +135,13 @@ BT_API int bt_spmv_scatter(int64_t batch, int64_t n_in, int64_t n_out,
  * library holds until exit.  batch * ceil(n_in / 32) above that limit is
  * rejected with BT_ERR_INVALID.  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress with that device current);
- * make that first call before any stream capture.  Every call shares the one
- * array: calls that overlap on the GPU (other streams, other threads) race
- * and must be serialised by the caller.  Nothing is allocated or freed. */
+ * make that first call before any stream capture.  The address is cached
+ * per device for the life of the process and is not refreshed after
+ * cudaDeviceReset or a re-created primary context: do not call this entry
+ * point across such a reset.  Every call shares the one array: calls that
+ * overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller.  x may be NULL when n_in == 0.  Nothing is
+ * allocated or freed. */
 #define BT_NOALLOC_GATHER_MAX_WORDS (1 << 18)
 BT_API int bt_spmv_gather_noalloc(int64_t batch, int64_t n_in, int64_t n_out,
                                   const int32_t* csc_ptr, const uint32_t* csc_src,

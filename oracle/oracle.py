@@ -44,6 +44,8 @@ class _Net(C.Structure):
         ("t0", C.c_int64),
         ("spikes", _u8), ("v_trace", _f), ("psc_trace", _f),
         ("threads", C.c_int32), ("n_rec", C.c_int32),
+        ("row_ptr", _i64), ("row_col", _i32), ("row_w", _f), ("acc", _f),
+        ("zmask", C.POINTER(C.c_uint64)),
     ]
 
 
@@ -70,6 +72,9 @@ def lib():
     if _lib is None:
         _lib = C.CDLL(str(build()))
         _lib.orc_run.argtypes = [C.POINTER(_Net)]
+        _lib.orc_run_events.argtypes = [C.POINTER(_Net)]
+        _lib.orc_linear_mt.argtypes = [C.c_int64, C.c_int64, C.c_int64, _f, _f, _f, _f, C.c_int32]
+        _lib.orc_linear_t.argtypes = [C.c_int64, C.c_int64, C.c_int64, _f, _f, _f, _f, C.c_int32]
         _lib.orc_spmm.argtypes = [C.c_int64, C.c_int64, C.c_int64, _i64, _i64, _f, _f, _f, C.c_int32]
         _lib.orc_linear.argtypes = [C.c_int64, C.c_int64, C.c_int64, _f, _f, _f, _f]
     return _lib
@@ -95,15 +100,32 @@ def spmm(ptr, src, w, x, n_out, threads=1):
     return out
 
 
-def linear(x, W, bias=None):
-    """x [rows, c_in] @ W[n, c_in]^T (+ bias), ascending-channel fmaf chain."""
+def linear(x, W, bias=None, threads=1):
+    """x [rows, c_in] @ W[n, c_in]^T (+ bias), ascending-channel fmaf chain
+    (rows split over `threads` host threads; the result does not depend on it)."""
     x = _f32(x)
     W = _f32(W)
     rows, c_in = x.shape
     n = W.shape[0]
     out = np.zeros((rows, n), np.float32)
     b = None if bias is None else _f32(bias)
-    lib().orc_linear(rows, c_in, n, _p(x, _f), _p(W, _f), _p(b, _f), _p(out, _f))
+    if lib().orc_linear_mt(rows, c_in, n, _p(x, _f), _p(W, _f), _p(b, _f), _p(out, _f), int(threads)) != 0:
+        raise MemoryError("oracle projection failed")
+    return out
+
+
+def linear_t(x, W_t, bias=None, threads=1):
+    """linear() from the transposed weight W_t [c_in, n] (DenseConn's weight
+    transposed; the bench keeps it in this layout): the same chain per output,
+    computed row by row as channel-ordered axpys."""
+    x = _f32(x)
+    W_t = _f32(W_t)
+    rows, c_in = x.shape
+    n = W_t.shape[1]
+    out = np.empty((rows, n), np.float32)
+    b = None if bias is None else _f32(bias)
+    if lib().orc_linear_t(rows, c_in, n, _p(x, _f), _p(W_t, _f), _p(b, _f), _p(out, _f), int(threads)) != 0:
+        raise MemoryError("oracle projection failed")
     return out
 
 
@@ -128,6 +150,25 @@ class NetSpec:
     w: np.ndarray  # float32 [nnz]
     max_delay: int = 0
     n_rec: int = 1  # receptor columns per neuron: ptr, psc_coef, psc_tau span n * n_rec columns
+
+
+def source_rows(spec: NetSpec):
+    """The spec's edges by source row r = pre * (max_delay + 1) + delay (rows
+    ascending; within a row, ascending PSC column): (row_ptr int64, row_col
+    int32, row_w float32), built once per spec for the event-driven run."""
+    cached = getattr(spec, "_rows", None)
+    if cached is not None:
+        return cached
+    R = spec.max_delay + 1
+    nc = spec.n * max(1, spec.n_rec)
+    col = np.repeat(np.arange(nc, dtype=np.int64), np.diff(spec.ptr))
+    key = spec.pre.astype(np.int64) * R + spec.delay.astype(np.int64)
+    order = np.argsort(key, kind="stable")  # canonical order is by column: columns ascend within a row
+    row_ptr = np.zeros(spec.n * R + 1, np.int64)
+    np.cumsum(np.bincount(key, minlength=spec.n * R), out=row_ptr[1:])
+    rows = (row_ptr, np.ascontiguousarray(col[order], np.int32), np.ascontiguousarray(spec.w[order], np.float32))
+    spec._rows = rows
+    return rows
 
 
 @dataclass
@@ -155,8 +196,14 @@ def init_state(spec: NetSpec, batch: int, v0=None, gk0=0.0) -> NetState:
 
 
 def run(spec: NetSpec, state: NetState, x, steps=None, sample_len=None, threads=None,
-        want_v=False, want_psc=False):
-    """Run the recurrent loop in place on `state`; returns dict(spikes, v, psc)."""
+        want_v=False, want_psc=False, events=False):
+    """Run the recurrent loop in place on `state`; returns dict(spikes, v, psc).
+
+    events=False forms W z the reference's way, over every synapse each step
+    (its cost is what the CPU baseline times); events=True pushes only the
+    rows of neurons that spiked, in the same per-column order, which gives
+    bit-identical results at a cost proportional to the spikes (parity checks
+    at full network size)."""
     B, n = state.v.shape
     if x is not None:
         x = _f32(x)
@@ -191,8 +238,20 @@ def run(spec: NetSpec, state: NetState, x, steps=None, sample_len=None, threads=
         spikes=_p(spikes, _u8), v_trace=_p(v_tr, _f), psc_trace=_p(p_tr, _f), threads=threads,
         n_rec=max(1, spec.n_rec),
     )
-    keep = (x, P, spikes, v_tr, p_tr, sl)  # noqa: F841 -- buffers live across the call
-    if lib().orc_run(C.byref(net)) != 0:
+    acc = zmask = None
+    if events:
+        row_ptr, row_col, row_w = source_rows(spec)
+        acc = np.zeros((B, nc), np.float32)
+        # the history slots as per-neuron sample bit masks [H, n, ceil(B / 64)]
+        W64 = (B + 63) // 64
+        nz = np.zeros((state.hist.shape[0], n, W64 * 64), bool)
+        nz[:, :, :B] = (state.hist != 0).transpose(0, 2, 1)
+        zmask = np.ascontiguousarray(np.packbits(nz, axis=-1, bitorder="little")).view(np.uint64)
+        net.row_ptr, net.row_col, net.row_w, net.acc = (_p(row_ptr, _i64), _p(row_col, _i32), _p(row_w, _f),
+                                                        _p(acc, _f))
+        net.zmask = zmask.ctypes.data_as(C.POINTER(C.c_uint64))
+    keep = (x, P, spikes, v_tr, p_tr, sl, acc, zmask)  # noqa: F841 -- buffers live across the call
+    if (lib().orc_run_events if events else lib().orc_run)(C.byref(net)) != 0:
         raise RuntimeError("oracle run failed")
     state.t += steps
     return {"spikes": spikes, "v": v_tr, "psc": p_tr}

@@ -1,19 +1,22 @@
 """Generate golden vectors from the reference btorch (run in the build container).
 
-The reference checkout is imported read-only from REF_ROOT (default
-/root/reference).  Each case builds the reference's own modules on seeded
+The reference checkout is imported read-only from the directory given by
+--ref, or else by the BTORCH_REFERENCE environment variable.  Each case
+builds the reference's own modules on seeded
 synthetic inputs, runs them on the CPU (native sparse backend, fp32) and
 saves inputs, parameters and outputs to tests/golden/<case>.npz.  The tests
 replay these cases through the CPU oracle (pinning it to the reference) and
 through the CUDA engine.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    BTORCH_REFERENCE=<reference checkout> python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --ref <reference checkout>
 """
 
 from __future__ import annotations
 
 import argparse
 import importlib.metadata as md
+import os
 import sys
 from pathlib import Path
 
@@ -677,9 +680,12 @@ def case_surrogate(rng):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("BTORCH_REFERENCE"),
+                    help="reference checkout (default: $BTORCH_REFERENCE)")
     ap.add_argument("--only", default="", help="comma-separated case names (default: all)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference checkout with --ref or BTORCH_REFERENCE")
     _import_reference(args.ref)
     import torch
 

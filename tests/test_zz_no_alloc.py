@@ -71,3 +71,8 @@ def test_no_alloc_gather_rejects_oversize_requests():
     st = L.lib().bt_spmv_gather_noalloc(batch, words, 8, None, None, None, None, None, None)
     assert st == L.BT_ERR_INVALID
     assert b"scratch" in L.lib().bt_last_error()
+    # a batch whose product with the word count wraps 64 bits is refused too
+    wrap = 1 << 44  # x 2^20 words = 2^64
+    st = L.lib().bt_spmv_gather_noalloc(wrap, words, 8, None, None, None, None, None, None)
+    assert st == L.BT_ERR_INVALID
+    assert b"scratch" in L.lib().bt_last_error()
