@@ -17,7 +17,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libbtorch_b200.so"
 
 BT_OK, BT_ERR_INVALID, BT_ERR_CUDA, BT_ERR_TIMEOUT, BT_ERR_UNSUPPORTED, BT_ERR_LAYOUT = range(6)
 BT_NEURON_LIF, BT_NEURON_ALIF = 0, 1
-BT_MODE_SCATTER, BT_MODE_GATHER, BT_MODE_PULL = 0, 1, 2
+BT_MODE_SCATTER, BT_MODE_GATHER, BT_MODE_PULL, BT_MODE_TILE = 0, 1, 2, 3
 BT_BIN_SHIFT = 25
 BT_MAX_BINS = 128
 
@@ -26,7 +26,7 @@ _i64 = C.c_int64
 _i32 = C.c_int32
 
 
-ABI_VERSION = 7  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
+ABI_VERSION = 8  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
 
 
 class BtParam(C.Structure):
@@ -60,6 +60,7 @@ class BtEngineDesc(C.Structure):
         ("work", _vp), ("stats", _vp), ("dense_rows", _i64),
         ("psc_uniform", _i32), ("psc_coef_s", C.c_float), ("psc_tau_s", C.c_float), ("psc_fast_div", _i32),
         ("psc_rcp", C.c_float), ("n_rec", _i32), ("csr_edges", _vp),
+        ("tile_posts", _i32), ("n_tiles", _i32), ("tile_off", _vp), ("tile_work", _vp), ("spin_limit", _i32),
     ]
 
 
@@ -91,6 +92,9 @@ _PROTOS = {
     "bt_mask_stride": (C.c_int, [_i64]),
     "bt_engine_work_words": (C.c_int64, [_i64, _i64, _i32]),
     "bt_masks_to_float": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
+    "bt_tile_work_words": (C.c_int64, [_i64, _i32, _i32]),
+    "bt_tile_smem_bytes": (C.c_int64, [_i64, _i32, _i32]),
+    "bt_tile_offsets": (C.c_int, [_i64, _vp, _vp, _i32, _i32, _vp, _vp]),
 }
 
 _lock = threading.Lock()

@@ -1370,6 +1370,10 @@ __global__ void k_float_to_bits(int64_t rows, int64_t n, const float* __restrict
 
 using namespace bt;
 
+namespace bt {
+int run_tile(const bt_engine_desc& d, bool fast, cudaStream_t s);  // tile.cu
+}
+
 namespace {
 
 int engine_check(const bt_engine_desc* d) {
@@ -1380,8 +1384,9 @@ int engine_check(const bt_engine_desc* d) {
   BT_CHECK_ARG(d->n_bins >= 1 && d->n_bins <= BT_MAX_BINS, "n_bins=%d outside [1, 128]", d->n_bins);
   BT_CHECK_ARG(d->hist_len >= d->n_bins + 2, "hist_len=%d must be >= n_bins + 2", d->hist_len);
   BT_CHECK_ARG(d->n_steps >= 0 && d->t0 >= 0, "negative step index");
-  BT_CHECK_ARG(d->mode == BT_MODE_SCATTER || d->mode == BT_MODE_GATHER || d->mode == BT_MODE_PULL, "mode=%d",
-               d->mode);
+  BT_CHECK_ARG(d->mode == BT_MODE_SCATTER || d->mode == BT_MODE_GATHER || d->mode == BT_MODE_PULL ||
+                   d->mode == BT_MODE_TILE,
+               "mode=%d", d->mode);
   BT_CHECK_ARG(d->v && d->psc && d->hist, "state pointer missing (v / psc / hist)");
   BT_CHECK_ARG(!d->neuron.use_refractory || d->refractory, "refractory state missing");
   BT_CHECK_ARG(d->neuron.kind != BT_NEURON_ALIF || d->g_k, "g_k state missing");
@@ -1403,6 +1408,18 @@ int engine_check(const bt_engine_desc* d) {
                  "dense delivery needs a single delay bin and the sliced in-edge view");
     BT_CHECK_ARG(d->neuron_spt == 0 || d->neuron_spt == 1 || d->neuron_spt == 2 || d->neuron_spt == 4,
                  "neuron_spt=%d (0, 1, 2 or 4)", d->neuron_spt);
+  } else if (d->mode == BT_MODE_TILE) {
+    BT_CHECK_ARG(d->csr_ptr && d->csr_edges && d->ring && d->tile_off && d->tile_work,
+                 "tile mode needs CSR, ring, tile offsets and tile work");
+    BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->csr_edges) & 15) == 0, "csr_edges must be 16-byte aligned");
+    BT_CHECK_ARG(d->n_bins == 1 && d->bin_lo == 0 && d->bin_hi == 0, "tile mode has no synaptic delays");
+    BT_CHECK_ARG(n_rec(*d) == 1, "tile mode has no receptor channels");
+    BT_CHECK_ARG(d->tile_posts > 0 && (d->tile_posts & 31) == 0, "tile_posts=%d must be a positive multiple of 32",
+                 d->tile_posts);
+    BT_CHECK_ARG(d->n_tiles > 0 && int64_t(d->n_tiles) * d->tile_posts >= d->n &&
+                     int64_t(d->n_tiles - 1) * d->tile_posts < d->n,
+                 "n_tiles=%d x tile_posts=%d does not tile n=%lld", d->n_tiles, d->tile_posts, (long long)d->n);
+    BT_CHECK_ARG(d->batch <= 256 && d->batch * d->n < (int64_t(1) << 31), "tile mode: batch <= 256, batch * n < 2^31");
   } else if (d->mode == BT_MODE_GATHER) {
     BT_CHECK_ARG(d->csc_ptr && d->csc_src && d->csc_w, "gather needs CSC");
   } else {
@@ -1433,6 +1450,12 @@ bool fast_divisors(const bt_engine_desc& d, int kind) {
 template <int KIND, bool HARD, bool USE_REF>
 int run_typed(const bt_engine_desc& d, cudaStream_t s) {
   const int64_t n = d.n;
+  if (d.mode == BT_MODE_TILE) {
+    if (int st = run_tile(d, fast_divisors(d, KIND), s)) return st;
+    k_eng_scatter_final<<<int(ceil_div(d.batch * n, 256)), 256, 0, s>>>(d);
+    BT_CHECK_LAUNCH("k_eng_scatter_final");
+    return BT_OK;
+  }
   if (d.mode == BT_MODE_SCATTER) {
     const int S = d.neuron_spt > 0 ? d.neuron_spt : 4;
     const dim3 grid(unsigned(ceil_div(n, kEngThreads)), unsigned(ceil_div(d.batch, S)));

@@ -41,24 +41,30 @@ class EngineChoice:
     pull_words: int = 0        # pull: 32-sample mask words per warp (0 = one)
     dense_rows: int = -1       # scatter, one delay bin: spiking neurons from which a step is pulled
                                # densely (-1 = n / engine.DENSE_FRACTION, 0 = never)
+    tile_posts: int = 0        # tile: posts per CTA (0 = one tile per SM)
 
     def describe(self) -> dict:
-        name = {L.BT_MODE_SCATTER: "scatter", L.BT_MODE_GATHER: "gather", L.BT_MODE_PULL: "pull"}[self.mode]
+        name = {L.BT_MODE_SCATTER: "scatter", L.BT_MODE_GATHER: "gather", L.BT_MODE_PULL: "pull",
+                L.BT_MODE_TILE: "tile"}[self.mode]
         return {"mode": name, "neuron_spt": self.neuron_spt, "scatter_lanes": self.scatter_lanes,
-                "pull_words": self.pull_words, "dense_rows": self.dense_rows}
+                "pull_words": self.pull_words, "dense_rows": self.dense_rows, "tile_posts": self.tile_posts}
 
 
-def allowed_modes(conn, batch: int, receptors: int = 1) -> list[int]:
+def allowed_modes(conn, batch: int, receptors: int = 1, n_bins: int = 1) -> list[int]:
     """Delivery modes the sparse config admits (the sliced pull has no
-    receptor channels: with receptors > 1 it is left out)."""
+    receptor channels: with receptors > 1 it is left out; the tile mode
+    delivers push-wise like scatter, without delays or receptor channels)."""
     cfg = conn.sparse_config
     if cfg.deterministic or cfg.direction == "gather":
         modes = [L.BT_MODE_GATHER, L.BT_MODE_PULL]
     elif cfg.direction == "scatter":
-        modes = [L.BT_MODE_SCATTER]
+        modes = [L.BT_MODE_SCATTER, L.BT_MODE_TILE]
     else:
-        modes = [L.BT_MODE_SCATTER, L.BT_MODE_PULL, L.BT_MODE_GATHER]
-    return [m for m in modes if receptors == 1 or m != L.BT_MODE_PULL]
+        modes = [L.BT_MODE_SCATTER, L.BT_MODE_TILE, L.BT_MODE_PULL, L.BT_MODE_GATHER]
+    modes = [m for m in modes if receptors == 1 or m != L.BT_MODE_PULL]
+    if receptors > 1 or n_bins > 1 or batch > 256:
+        modes = [m for m in modes if m != L.BT_MODE_TILE]
+    return modes
 
 
 def heuristic(conn, batch: int, receptors: int = 1) -> EngineChoice:
@@ -74,11 +80,22 @@ def heuristic(conn, batch: int, receptors: int = 1) -> EngineChoice:
     return EngineChoice(mode)
 
 
-def candidates(conn, batch: int, receptors: int = 1) -> list[EngineChoice]:
+def candidates(conn, batch: int, receptors: int = 1, n_bins: int = 1, n: int = 0, dev=None) -> list[EngineChoice]:
     out = []
     mw = L.lib().bt_mask_stride(batch)
-    modes = allowed_modes(conn, batch, receptors)
+    modes = allowed_modes(conn, batch, receptors, n_bins)
     for mode in modes:
+        if mode == L.BT_MODE_TILE:
+            from .engine import tile_shape
+
+            base = tile_shape(n, batch, dev) if n and dev is not None else None
+            if base is not None:
+                for mult in (1, 2, 4):
+                    tp = base[0] * mult
+                    if mult > 1 and (tile_shape(n, batch, dev, tp) is None or -(-n // tp) < 8):
+                        continue
+                    out.append(EngineChoice(mode, tile_posts=0 if mult == 1 else tp))
+            continue
         if mode == L.BT_MODE_SCATTER:
             for spt in (1, 2, 4):
                 if spt > 1 and spt > batch:
@@ -97,7 +114,7 @@ def _key(plan, batch: int, c_in: int) -> tuple:
     conn = plan.conn
     return (torch.cuda.get_device_name(plan.neuron.v.device), plan.neuron.size, batch, plan.n_bins,
             plan.uniform_delay, int(conn.indices.shape[1]), c_in, type(plan.neuron).__name__, plan.n_rec,
-            tuple(allowed_modes(conn, batch, plan.n_rec)))
+            tuple(allowed_modes(conn, batch, plan.n_rec, plan.n_bins)))
 
 
 def tuned(rnn) -> dict:
@@ -116,7 +133,7 @@ def choose(plan, rnn, x: torch.Tensor, sample_len, run) -> EngineChoice:
         return cache[key][0]
     if not plan.conn.sparse_config.autotune or T < TUNE_MIN_STEPS:
         return heuristic(plan.conn, B, plan.n_rec)
-    cands = candidates(plan.conn, B, plan.n_rec)
+    cands = candidates(plan.conn, B, plan.n_rec, plan.n_bins, plan.neuron.size, plan.neuron.v.device)
     if len(cands) == 1:
         cache[key] = (cands[0], {})
         return cands[0]

@@ -147,6 +147,40 @@ def _state2d(t: torch.Tensor, n: int) -> torch.Tensor:
     return t.view(-1, n)
 
 
+MAX_TILE_SMEM = 227 * 1024  # dynamic shared memory one CTA may opt into on sm_100
+
+
+def tile_shape(n: int, batch: int, dev, tile_posts: int = 0):
+    """(tile_posts, n_tiles) of the tile mode for this network and batch, or
+    None when a tile's accumulators do not fit in shared memory.  By default
+    one tile per SM (the fewest posts per CTA with every SM busy); a tuned
+    choice may ask for larger tiles (fewer CTAs, each walking the spike lists
+    once per step)."""
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    tp = int(tile_posts) or 32 * -(-(-(-n // sms)) // 32)
+    tp = 32 * -(-tp // 32)
+    P = -(-n // tp)
+    if P > sms or batch > 256:
+        return None
+    if L.lib().bt_tile_smem_bytes(batch, tp, P) > MAX_TILE_SMEM:
+        return None
+    return tp, P
+
+
+def tile_offsets(lay, edges: torch.Tensor, tp: int, P: int, dev) -> torch.Tensor:
+    """The CSR rows split at the tile boundaries ([rows][P + 1] int32), cached
+    on the layout per tile shape (they depend on the posts only)."""
+    cache = lay.__dict__.setdefault("tile_offsets", {})
+    off = cache.get((tp, P))
+    if off is None:
+        rows = lay.csr_ptr.numel() - 1
+        off = torch.empty((rows, P + 1), device=dev, dtype=torch.int32)
+        L.check(L.lib().bt_tile_offsets(rows, lay.csr_ptr.data_ptr(), edges.data_ptr(), tp, P, off.data_ptr(),
+                                        L.stream_of(dev)), "bt_tile_offsets")
+        cache[(tp, P)] = off
+    return off
+
+
 def graph_hist_len(n_bins: int) -> int:
     """History ring length for graph replay: 2 (R + 1), a multiple of the
     R + 1 spike-set slots of scatter mode and at least R + 2, so that the
@@ -359,6 +393,24 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         work = alloc("work", (L.lib().bt_engine_work_words(n, B, R),), torch.int32)
         keep += [ring, work]
         desc.ring, desc.work = ring.data_ptr(), work.data_ptr()
+    tile_ws = None
+    if mode == L.BT_MODE_TILE:
+        lay_s = conn.scatter_layout(R, plan.uniform_delay, dev)
+        w_csr = pack_csr_weights(lay_s, w)
+        edges = static("csr_edges", torch.stack([lay_s.csr_dst, w_csr.view(torch.int32)], 1).reshape(-1))
+        shape = tile_shape(n, B, dev, choice.tile_posts)
+        if shape is None:
+            raise NotImplementedError("tile mode: the tile accumulators do not fit in shared memory")
+        tp, P = shape
+        toff = tile_offsets(lay_s, edges, tp, P, dev)
+        ring = alloc("ring", (B, nc), torch.float32, zero=True)  # W z handed to the final launch
+        tile_ws = alloc("tile_work", (L.lib().bt_tile_work_words(B, tp, P),), torch.int32, zero=True)
+        keep += [w_csr, edges, ring, tile_ws, toff]
+        desc.csr_ptr, desc.csr_edges, desc.ring = lay_s.csr_ptr.data_ptr(), edges.data_ptr(), ring.data_ptr()
+        desc.bin_lo = desc.bin_hi = 0
+        desc.tile_posts, desc.n_tiles = tp, P
+        desc.tile_off, desc.tile_work = toff.data_ptr(), tile_ws.data_ptr()
+        desc.spin_limit = int(getattr(rnn, "engine_spin_limit", 0))
     if mode == L.BT_MODE_PULL:
         sl = getattr(lay, "slices", None)
         if sl is None:
@@ -502,7 +554,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         set_desc(k0, kc, xp, slc, outs)
         e0 = _ev() if profile is not None else None
         L.check(L.lib().bt_engine_run(C.byref(desc), stream), "bt_engine_run")
-        nl += (2 * kc if mode == L.BT_MODE_SCATTER else kc) + 1
+        nl += 2 if mode == L.BT_MODE_TILE else (2 * kc if mode == L.BT_MODE_SCATTER else kc) + 1
         if profile is not None:
             profile.append(("step", e0, _ev()))
         return nl
@@ -569,6 +621,12 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
                 out_full[kind][k0:k0 + kc].copy_(t[:kc])
     if host_io:
         io.finish()
+    if tile_ws is not None:
+        status = int(tile_ws[2].item())  # the launches' status word (a barrier wait that gave up)
+        if status:
+            tile_ws[:32].zero_()
+            raise RuntimeError("fused engine, tile mode: a grid barrier wait gave up (BT_ERR_TIMEOUT); "
+                               "the call's results are invalid")
 
     if use_graph:
         v_mod.copy_(v)
@@ -618,7 +676,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             states[key] = traces[kind].view(T, *batch_shape, *_nshape(plan, key))
     rnn.last_engine_stats = stat_t
     rnn.last_engine_direction = {L.BT_MODE_SCATTER: "scatter", L.BT_MODE_GATHER: "gather",
-                                 L.BT_MODE_PULL: "pull"}[mode]
+                                 L.BT_MODE_PULL: "pull", L.BT_MODE_TILE: "scatter"}[mode]
     rnn.last_engine_launches = launches
     rnn.last_engine_choice = choice
     if z is not None:

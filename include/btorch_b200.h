@@ -51,7 +51,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 7
+#define BT_ABI_VERSION 8
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -282,6 +282,9 @@ BT_API int bt_psc_step(int64_t batch, int64_t n, bt_param coef, bt_param tau_syn
 #define BT_MODE_GATHER 1   /* pull, warp per post: 1 launch per step, ordered, bit-exact */
 #define BT_MODE_PULL 2     /* pull over SELL-32 slices, lane per post, sample masks:
                               1 launch per step, ordered, bit-exact, for batches */
+#define BT_MODE_TILE 3     /* persistent: one launch for all n_steps, one CTA per tile
+                              of posts with its synaptic input in shared memory, a
+                              bounded grid barrier per step; single delay bin 0 */
 
 typedef struct bt_engine_desc {
   /* sizes */
@@ -368,7 +371,37 @@ typedef struct bt_engine_desc {
      post, weight bits, post, weight bits, ... (one 8-byte record per edge, so
      a short row occupies the fewest memory sectors); 16-byte aligned */
   const uint32_t* csr_edges;
+
+  /* tile mode (BT_MODE_TILE, no counterpart in the reference: its time loop
+     launches per step).  Tile t owns posts [t * tile_posts, (t + 1) *
+     tile_posts); tile_posts is a multiple of 32 and n_tiles the number of
+     tiles covering n, all co-resident (at most one per SM for large tiles).
+     tile_off: [n][n_tiles + 1] from bt_tile_offsets (the CSR row of each
+     source split at the tile boundaries).  tile_work:
+     bt_tile_work_words(batch, tile_posts, n_tiles) int32 words whose first
+     32 are zero before the first call; word 2 is the status word, nonzero
+     (BT_ERR_TIMEOUT) after a grid barrier wait gave up -- the caller reads
+     it after the call and clears the first 32 words before reusing them.
+     spin_limit: polls of one barrier wait before it gives up (0 = about a
+     second). */
+  int32_t tile_posts;
+  int32_t n_tiles;
+  const int32_t* tile_off;
+  int32_t* tile_work;
+  int32_t spin_limit;
 } bt_engine_desc;
+
+/* Tile mode scratch words and shared memory bytes per CTA for a shape
+   (0 for a bad shape). */
+BT_API int64_t bt_tile_work_words(int64_t batch, int32_t tile_posts, int32_t n_tiles);
+BT_API int64_t bt_tile_smem_bytes(int64_t batch, int32_t tile_posts, int32_t n_tiles);
+
+/* off[r][t] (r < rows, t <= n_tiles) = the first edge of CSR row r whose post
+   is >= t * tile_posts; rows must be sorted by post (bt_layout_build's CSR
+   is).  csr_edges: the interleaved (post, weight) records of
+   bt_engine_desc.csr_edges. */
+BT_API int bt_tile_offsets(int64_t rows, const int32_t* csr_ptr, const uint32_t* csr_edges,
+                           int32_t tile_posts, int32_t n_tiles, int32_t* off, void* stream);
 
 /* Scratch words (int32) the scatter mode needs in bt_engine_desc.work. */
 BT_API int64_t bt_engine_work_words(int64_t n, int64_t batch, int32_t n_bins);

@@ -16,7 +16,7 @@ def test_reference_arm_two_ranks_prints_one_line():
     port = 29700 + os.getpid() % 1000
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl", "reference",
-           "--gpus", "2", "--steps", "1", "--warmup", "0", "--cpu-sample-steps", "1", "--cpu-prewarm-steps", "1"]
+           "--gpus", "2", "--steps", "1", "--warmup", "0", "--cpu-sample-steps", "1", "--cpu-events-steps", "3"]
     env = dict(os.environ, OMP_NUM_THREADS="2")
     r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
@@ -31,7 +31,7 @@ def test_reference_arm_two_ranks_prints_one_line():
     assert line["config"]["workload"].startswith("batched:")
     cb = line["cpu_baseline"]
     assert cb["value"] == line["value"] and cb["kind"] == "port" and cb["cores"] >= 1
-    assert "after 1 untimed steps from rest" in cb["sample"]
+    assert "events per live sample-step" in cb["sample"] and "event-driven run of 3 steps" in cb["sample"]
     assert line["neuron_steps_per_s"] > 0
     assert line["e2e"] == {"value": line["value"], "unit": "events/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}

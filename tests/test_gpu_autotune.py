@@ -41,10 +41,11 @@ def test_tuned_run_equals_untuned(name, direction):
             cache = autotune.tuned(rnn)
             assert len(cache) == 1
             best, timings = next(iter(cache.values()))
-            cands = autotune.candidates(conn, int(d["batch"]))
+            n_bins = int(d["n_bins"]) if int(d["n_bins"]) > 1 else 1
+            cands = autotune.candidates(conn, int(d["batch"]), 1, n_bins, int(d["n"]), rnn.neuron.v.device)
             assert set(timings) == set(cands) and best in cands
             assert rnn.last_engine_choice == best
-            assert best.mode in autotune.allowed_modes(conn, int(d["batch"]))
+            assert best.mode in autotune.allowed_modes(conn, int(d["batch"]), 1, n_bins)
     for a, b in zip(outs[False], outs[True]):
         np.testing.assert_array_equal(a, b)
 
