@@ -218,10 +218,12 @@ def make_training_network(cfg, seed=0):
 
 def measure_training(cfg, args, dev):
     """Truncated BPTT on the training workload: per window, forward through
-    the per-module path (hand-written forward and backward kernels, chunks
-    checkpointed), readout + MSE, backward, Adam step, detach_net.  Returns the
-    sub-object of the JSON line (forward synaptic events per second of
-    training time, windows per second)."""
+    the fused BPTT (one autograd Function over the hand-written forward and
+    backward kernels, input projection included; with grad_checkpoint the
+    forward keeps the state at every chunk start and the backward recomputes
+    each chunk of `chunk` steps), readout + MSE, backward, Adam step,
+    detach_net.  Returns the sub-object of the JSON line (forward synaptic
+    events per second of training time, windows per second)."""
     from btorch_b200.models import LIF, DenseConn, ExponentialPSC, RecurrentNN, Sigmoid, SparseConn, environ
     from btorch_b200.models.functional import detach_net, init_net_state
 
@@ -277,11 +279,11 @@ def measure_training(cfg, args, dev):
             "ms_per_window": ms / steps, "windows": steps, "window_steps": Wn,
             "neuron_steps_per_s": n * B * Wn * steps / (ms * 1e-3),
             "loss_first_last": [float(losses[0]), float(losses[-1])], "direction": conn.direction(B),
-            "path": brain.last_path,
+            "path": brain.last_path, "bptt": getattr(brain, "last_bptt", None),
             "config": {"workload": f"training: LIF+ExpPSC N={n} p={cfg['p']} ({len(net['w'])} trainable weights) "
                                    f"batch {B} T {cfg['t_max']} TBPTT windows {Wn} checkpoint chunks "
-                                   f"{cfg['chunk']} sigmoid alpha {cfg['alpha']} readout {cfg['n_out']} "
-                                   f"sinusoids, MSE, Adam"}}
+                                   f"{cfg['chunk']} (recomputed in backward) sigmoid alpha {cfg['alpha']} "
+                                   f"readout {cfg['n_out']} sinusoids, MSE, Adam"}}
 
 
 def measure_serving(cfg, args, dev):

@@ -95,6 +95,7 @@ _PROTOS = {
     "bt_tile_work_words": (C.c_int64, [_i64, _i32, _i32]),
     "bt_tile_smem_bytes": (C.c_int64, [_i64, _i32, _i32]),
     "bt_tile_offsets": (C.c_int, [_i64, _vp, _vp, _i32, _i32, _vp, _vp]),
+    "bt_input_grad_weight": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _i32, _vp, _vp]),
 }
 
 _lock = threading.Lock()

@@ -1345,6 +1345,58 @@ __global__ void __launch_bounds__(256) k_input_project(int64_t rows, int64_t c_i
   }
 }
 
+// Per channel c, the rows r (ascending) whose input x[r][c] is nonzero, and
+// their count: one warp per channel (ballot + prefix keeps the order).
+__global__ void k_channel_rows(int64_t rows, int64_t c_in, const float* __restrict__ x, int32_t* __restrict__ lists,
+                               int32_t* __restrict__ counts) {
+  const int64_t c = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (c >= c_in) return;
+  const unsigned lane = lane_id();
+  int32_t total = 0;
+  for (int64_t r0 = 0; r0 < rows; r0 += 32) {
+    const int64_t r = r0 + lane;
+    const bool nz = r < rows && x[r * c_in + c] != 0.0f;
+    const uint32_t m = __ballot_sync(0xffffffffu, nz);
+    if (nz) lists[c * rows + total + __popc(m & ((1u << lane) - 1u))] = int32_t(r);
+    total += __popc(m);
+  }
+  if (lane == 0) counts[c] = total;
+}
+
+// Gradient of the input layer's weight (w_t [c_in][n]) from the gradient of
+// its projection g [rows][n]: out[c][i] = sum over the rows r of channel c
+// (ascending) of x[r][c] * g[r][i] -- an fmaf chain over the nonzero inputs
+// only; accumulate adds it to out.  Block = (channel, 1024 columns), each
+// thread kProjNPT columns spaced by the block size (coalesced rows of g).
+__global__ void __launch_bounds__(256) k_input_grad_weight(int64_t rows, int64_t c_in, int64_t n,
+                                                           const float* __restrict__ x, const float* __restrict__ g,
+                                                           const int32_t* __restrict__ lists,
+                                                           const int32_t* __restrict__ counts,
+                                                           float* __restrict__ out, int accumulate) {
+  const int64_t c = blockIdx.x;
+  const int64_t tile = int64_t(blockIdx.y) * (256 * kProjNPT);
+  const int32_t cnt = counts[c];
+  const int32_t* rl = lists + c * rows;
+  float acc[kProjNPT];
+#pragma unroll
+  for (int j = 0; j < kProjNPT; ++j) acc[j] = 0.0f;
+  for (int32_t q = 0; q < cnt; ++q) {
+    const int64_t r = __ldg(rl + q);
+    const float xv = __ldg(x + r * c_in + c);
+    const float* gr = g + r * n;
+#pragma unroll
+    for (int j = 0; j < kProjNPT; ++j) {
+      const int64_t i = tile + threadIdx.x + j * 256;
+      if (i < n) acc[j] = fmaf(xv, __ldg(gr + i), acc[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kProjNPT; ++j) {
+    const int64_t i = tile + threadIdx.x + j * 256;
+    if (i < n) out[c * n + i] = accumulate ? add(out[c * n + i], acc[j]) : acc[j];
+  }
+}
+
 // --------------------------------------------------------------- bitmaps --
 
 __global__ void k_bits_to_float(int64_t rows, int64_t n, const uint32_t* __restrict__ bits, float* __restrict__ out) {
@@ -1621,6 +1673,24 @@ extern "C" int bt_input_project_live(int64_t steps, int64_t batch, int64_t c_in,
                                      int32_t* work, void* stream) {
   BT_CHECK_ARG(steps >= 0 && batch > 0, "bad steps / batch");
   return input_project(steps * batch, c_in, n, xin, w_t, bias, out, work, sample_len, batch, stream);
+}
+
+extern "C" int bt_input_grad_weight(int64_t rows, int64_t c_in, int64_t n, const float* x, const float* g,
+                                    float* out, int32_t accumulate, int32_t* work, void* stream) {
+  BT_CHECK_ARG(rows >= 0 && c_in >= 0 && n >= 0, "negative size");
+  if (c_in == 0 || n == 0) return BT_OK;
+  BT_CHECK_ARG(x && g && out && work, "null pointer");
+  BT_CHECK_ARG(c_in * (rows + 1) < (int64_t(1) << 31), "c_in * rows too large");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int32_t* lists = work;
+  int32_t* counts = work + c_in * rows;
+  k_channel_rows<<<int(ceil_div(c_in * 32, 256)), 256, 0, s>>>(rows, c_in, x, lists, counts);
+  BT_CHECK_LAUNCH("k_channel_rows");
+  const dim3 grid(unsigned(c_in), unsigned(ceil_div(n, 256 * kProjNPT)));
+  BT_CHECK_ARG(grid.y < 65536, "n too large");
+  k_input_grad_weight<<<grid, 256, 0, s>>>(rows, c_in, n, x, g, lists, counts, out, accumulate);
+  BT_CHECK_LAUNCH("k_input_grad_weight");
+  return BT_OK;
 }
 
 extern "C" int bt_bits_to_float(int64_t rows, int64_t n, const uint32_t* bits, float* out, void* stream) {

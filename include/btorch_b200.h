@@ -403,6 +403,15 @@ BT_API int64_t bt_tile_smem_bytes(int64_t batch, int32_t tile_posts, int32_t n_t
 BT_API int bt_tile_offsets(int64_t rows, const int32_t* csr_ptr, const uint32_t* csr_edges,
                            int32_t tile_posts, int32_t n_tiles, int32_t* off, void* stream);
 
+/* Weight gradient of the input layer (replaces the autograd of the
+ * reference's DenseConn / nn.Linear, btorch/models/linear.py:163-228):
+ * out[c][i] (+)= sum over rows r with x[r][c] != 0, ascending, of
+ * x[r][c] * g[r][i] (fmaf chain), for x [rows][c_in] and the projection's
+ * gradient g [rows][n]; out is the gradient of the transposed weight
+ * [c_in][n]; accumulate != 0 adds to it.  `work`: c_in * (rows + 1) int32. */
+BT_API int bt_input_grad_weight(int64_t rows, int64_t c_in, int64_t n, const float* x, const float* g,
+                                float* out, int32_t accumulate, int32_t* work, void* stream);
+
 /* Scratch words (int32) the scatter mode needs in bt_engine_desc.work. */
 BT_API int64_t bt_engine_work_words(int64_t n, int64_t batch, int32_t n_bins);
 

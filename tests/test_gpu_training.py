@@ -192,3 +192,57 @@ def test_fused_bptt_releases_buffers_and_supports_retain_graph():
     # the step buffers of this call take ~31 MB; what stays is the gradients
     # and cached packed weights (tens of KB)
     assert held < (8 << 20), held
+
+
+@pytest.mark.parametrize("kind", ["lif", "alif"])
+def test_fused_bptt_checkpointed_recompute_equals_stored_buffers(kind):
+    """grad_checkpoint=True: the fused BPTT keeps the state at each chunk start
+    and recomputes every chunk in backward.  Spikes, loss, the recurrent,
+    input-layer and readout gradients equal those of the run that stores
+    every step's buffers (dyadic weights: the recomputation is exact; the
+    weight gradients are summed chunk by chunk, so within 1e-6), and the
+    buffers take at most a quarter of the stored run's."""
+    import scipy.sparse as sp
+
+    from btorch_b200.models import ALIF
+
+    rng = np.random.default_rng(21)
+    n, B, T, c_in = 512, 8, 60, 32
+    dense = (rng.random((n, n)) < 0.05) * rng.geometric(0.25, (n, n)) * 2.0**-8
+    dense[int(0.8 * n):] *= -4.0
+    W = sp.coo_array(dense.astype(np.float32))
+    w_in = (np.round(rng.normal(0, 0.2, (c_in, n)) * 64) / 64).astype(np.float32)
+    x = torch.tensor(rng.poisson(0.2, (T, B, c_in)).astype(np.float32), device=DEV)
+    w_out = torch.tensor(rng.normal(0, 0.1, (5, n)).astype(np.float32))
+    outs = []
+    for ckpt in (False, True):
+        conn = SparseConn(W, sparse_config={"direction": "gather"})
+        if kind == "lif":
+            neuron = LIF(n, tau_ref=2.0, hard_reset=True, surrogate_function=Sigmoid(alpha=5.0))
+        else:
+            neuron = ALIF(n, g_leak=0.05, E_leak=0.0, E_k=-1.0, tau_adapt=50.0, dg_k=0.0625, tau_ref=2.0,
+                          hard_reset=True, surrogate_function=Sigmoid(alpha=5.0))
+        inp = DenseConn(c_in, n, weight=torch.tensor(w_in))
+        brain = RecurrentNN(neuron, ExponentialPSC(n, tau_syn=5.0, linear=conn), neuron_inp_module=inp,
+                            update_state_names=(), grad_checkpoint=ckpt, chunk_size=12, unroll=4).to(DEV)
+        readout = torch.nn.Linear(n, 5).to(DEV)
+        with torch.no_grad():
+            readout.weight.copy_(w_out)
+            readout.bias.zero_()
+        init_net_state(brain, batch_size=B, dtype=torch.float32, device=DEV)
+        with environ.context(dt=1.0):
+            z, _ = brain(x)
+        assert brain.last_path == "fused-bptt"
+        assert brain.last_bptt["recomputed"] == ckpt
+        loss = (readout(z) - 0.1).square().mean() + brain.neuron.v.square().mean()
+        loss.backward()
+        outs.append({"z": z.detach().cpu().numpy(), "loss": float(loss), "w": conn.magnitude.grad.cpu().numpy(),
+                     "win": inp.weight.grad.cpu().numpy(), "wout": readout.weight.grad.cpu().numpy(),
+                     "bytes": brain.last_bptt["bytes"]})
+    a, b = outs
+    assert a["z"].sum() > 100
+    np.testing.assert_array_equal(a["z"], b["z"])
+    assert a["loss"] == b["loss"]
+    for key in ("w", "win", "wout"):
+        assert rel_err(b[key], a[key]) < 1e-6, (key, rel_err(b[key], a[key]))
+    assert b["bytes"] <= 0.35 * a["bytes"]  # T 60, chunks of 12: the spikes are most of what remains
