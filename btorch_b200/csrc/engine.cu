@@ -1463,6 +1463,7 @@ int engine_check(const bt_engine_desc* d) {
   } else if (d->mode == BT_MODE_TILE) {
     BT_CHECK_ARG(d->csr_ptr && d->csr_edges && d->ring && d->tile_off && d->tile_work,
                  "tile mode needs CSR, ring, tile offsets and tile work");
+    BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->tile_work) & 63) == 0, "tile_work must be 64-byte aligned");
     BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->csr_edges) & 15) == 0, "csr_edges must be 16-byte aligned");
     BT_CHECK_ARG(d->n_bins == 1 && d->bin_lo == 0 && d->bin_hi == 0, "tile mode has no synaptic delays");
     BT_CHECK_ARG(n_rec(*d) == 1, "tile mode has no receptor channels");

@@ -47,32 +47,41 @@
 
 namespace bt {
 
-constexpr int kTileThreads = 1024;
+constexpr int kTileThreads = 512;
 constexpr int kTileWarps = kTileThreads / 32;
 constexpr unsigned kDefaultSpinLimit = 4u << 20;  // polls with a 256 ns back-off: about a second
 
 __host__ __device__ __forceinline__ int tile_mask_words(int64_t batch) { return int((batch + 31) >> 5); }
 
-// Words of one spike-list record: the neuron id and its sample mask words,
-// rounded up to a power of two (2, 4, 8 or 16) for vector loads.
-__host__ __device__ __forceinline__ int tile_rec_words(int64_t batch) {
-  const int need = 1 + tile_mask_words(batch);
-  return need <= 2 ? 2 : need <= 4 ? 4 : need <= 8 ? 8 : 16;
+// Mask words a record is laid out for: the kernel's compile-time bucket
+// MS >= the batch's mask words (1, 2, 4 or 8).
+__host__ __device__ __forceinline__ int tile_mask_bucket(int64_t batch) {
+  const int ms = tile_mask_words(batch);
+  return ms <= 1 ? 1 : ms <= 2 ? 2 : ms <= 4 ? 4 : 8;
 }
 
+// Words of one spike-list record: the neuron id and MS mask words, padded to
+// 2, 4, 8 or 16 words (MS = 1, 2, 4, 8) -- exactly what load_record<MS>
+// reads with 8- or 16-byte vector loads.
+__host__ __device__ __forceinline__ int tile_rec_words(int64_t batch) { return 2 * tile_mask_bucket(batch); }
+
 // Work layout (int32 words): [0, 32) control (0: barrier arrivals,
-// 1: barrier generation, 2: status), then counts [2][n_tiles], then records
-// [2][n_tiles][tile_posts][rec_words].
+// 1: barrier generation, 2: status), then counts [2][n_tiles], then, from
+// the next multiple of 16 words (64 bytes: every record 16-byte aligned),
+// records [2][n_tiles][tile_posts][rec_words].
 constexpr int kTileCtrl = 32;
+__host__ __device__ __forceinline__ int64_t tile_rec_offset(int n_tiles) {
+  return (kTileCtrl + 2 * int64_t(n_tiles) + 15) & ~int64_t(15);
+}
 __host__ __device__ __forceinline__ int64_t tile_work_words(int64_t batch, int tile_posts, int n_tiles) {
-  return kTileCtrl + 2 * int64_t(n_tiles) + 2 * int64_t(n_tiles) * tile_posts * tile_rec_words(batch);
+  return tile_rec_offset(n_tiles) + 2 * int64_t(n_tiles) * tile_posts * tile_rec_words(batch);
 }
 
 // Dynamic shared memory: accumulators [batch][tile_posts], sample masks
 // [tile_posts][mask words], list offsets [n_tiles + 1] (+ scan scratch).
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int64_t batch, int tile_posts, int n_tiles) {
   return sizeof(float) * size_t(batch) * tile_posts + sizeof(uint32_t) * size_t(tile_posts) * tile_mask_words(batch) +
-         sizeof(int32_t) * (size_t(n_tiles) + 1 + kTileWarps + 2);
+         sizeof(int32_t) * (size_t(n_tiles) + 1 + kTileWarps + 2 + size_t(batch));
 }
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -113,59 +122,126 @@ __device__ bool tile_barrier(unsigned* ctrl, unsigned nblocks, unsigned& gen, un
   return *s_flag == 0;
 }
 
-// One (sample b, 32-neuron word) item of the neuron phase: the lanes are the
-// word's neurons.  Returns the spike (0 or 1) of this lane's neuron.
-template <int KIND, bool HARD, bool USE_REF, bool FAST, bool TRACES>
-__device__ __forceinline__ float tile_neuron_item(const bt_engine_desc& d, const NeuronParams& prm_u, int64_t k,
-                                                  int64_t b, int64_t i, bool valid, float* acc, float pc,
-                                                  const Div& dpt, int n32) {
-  const int64_t len = d.sample_len ? d.sample_len[b] : INT64_MAX;
-  const bool live = valid && k < len, edge = valid && k <= len;
-  const int off = int(b) * n32 + int(valid ? i : 0);
-  const bool frozen = valid && TRACES;
-  float* __restrict__ psc_p = d.psc + off;
-  float* __restrict__ v_p = d.v + off;
-  float* __restrict__ ref_p = USE_REF ? d.refractory + off : nullptr;
-  float* __restrict__ gk_p = KIND == BT_NEURON_ALIF ? d.g_k + off : nullptr;
-  // loads before stores (a load behind a store to a maybe-aliasing pointer waits)
-  const float pend = edge ? *acc : 0.0f;
-  const float pv = (edge || frozen) ? *psc_p : 0.0f;
-  const float xv = (live && d.x) ? __ldcs(d.x + k * int64_t(n32) * d.batch + off) : 0.0f;
-  float v = (live || frozen) ? *v_p : 0.0f;
-  float ref = ((live || frozen) && USE_REF) ? *ref_p : 0.0f;
-  float gk = ((live || frozen) && KIND == BT_NEURON_ALIF) ? *gk_p : 0.0f;
+constexpr int kTileU = 4;     // samples per warp item of the neuron phase (loads in flight)
+constexpr int kTileGroups = 4;  // groups of 32 spike records a warp prefetches in the delivery
+
+// One item of the neuron phase: a 32-neuron word of the tile (lane = neuron)
+// for kTileU consecutive samples b0 .. b0+kTileU-1.  All the samples' loads
+// are issued before the first update (memory-level parallelism for a phase
+// that streams the state once); per sample the update is the reference's
+// (see k_eng_neuron), the spike bitmaps go out by warp ballot and the
+// neuron's sample bits of this word are or-ed into the tile's mask with one
+// shared atomic.
+template <int KIND, bool HARD, bool USE_REF, bool FAST>
+__device__ __forceinline__ void tile_neuron_item(const bt_engine_desc& d, const NeuronParams& prm_u, int64_t k,
+                                                 int b0, int64_t i, bool valid, int l, int Tp, float* s_acc,
+                                                 const int* s_len, uint32_t* s_mask, int ms, float pc_u,
+                                                 const Div& dpt_u, int h_t, int64_t words, int64_t wg,
+                                                 bool traces) {
+  const int B = int(d.batch), n32 = int(d.n);
+  const unsigned lane = lane_id();
+  float pend[kTileU], pv[kTileU], xv[kTileU], vv[kTileU], rv[kTileU], gv[kTileU];
+  bool live[kTileU], edge[kTileU];
+  const int off0 = b0 * n32 + int(valid ? i : 0);
+  const float* xk = d.x ? d.x + k * int64_t(n32) * B : nullptr;
+#pragma unroll
+  for (int u = 0; u < kTileU; ++u) {
+    const int b = b0 + u;
+    const bool in = valid && b < B;
+    const int len = in ? s_len[b] : 0;
+    live[u] = in && k < len;
+    edge[u] = in && k <= len;
+    const bool rd = live[u] || (in && traces);
+    const int off = off0 + u * n32;
+    pend[u] = edge[u] ? s_acc[b * Tp + l] : 0.0f;
+    pv[u] = (edge[u] || (in && traces)) ? d.psc[off] : 0.0f;
+    xv[u] = (live[u] && xk) ? __ldcs(xk + off) : 0.0f;
+    vv[u] = rd ? d.v[off] : 0.0f;
+    rv[u] = (rd && USE_REF) ? d.refractory[off] : 0.0f;
+    gv[u] = (rd && KIND == BT_NEURON_ALIF) ? d.g_k[off] : 0.0f;
+  }
   NeuronParams prm = prm_u;
+  float pc = pc_u;
+  Div dpt = dpt_u;
   if (!d.neuron.uniform) prm = load_params<KIND, USE_REF>(d.neuron, valid ? i : 0);
-  float s = 0.0f;
-  if (valid) {
-    float P = pv;
-    if (edge) *acc = 0.0f;
-    if (live) {
-      P = add(pv, pend);
-      const float I = d.x ? add(P, xv) : P;
+  if (!d.psc_uniform) {
+    const int64_t ip = valid ? i : 0;
+    pc = ld(d.psc_coef, ip);
+    dpt = make_div(ld(d.psc_tau, ip), false, 0.0f);
+  }
+  uint32_t bits = 0;
+#pragma unroll
+  for (int u = 0; u < kTileU; ++u) {
+    const int b = b0 + u;
+    if (b >= B) break;  // warp-uniform
+    const int off = off0 + u * n32;
+    float s = 0.0f;
+    float v = vv[u], ref = rv[u], gk = gv[u];
+    float P = pv[u];
+    if (edge[u]) s_acc[b * Tp + l] = 0.0f;
+    if (live[u]) {
+      P = add(pv[u], pend[u]);
+      const float I = xk ? add(P, xv[u]) : P;
       s = neuron_update<KIND, HARD, USE_REF, true, FAST>(prm, I, v, ref, gk).spike;
-      *v_p = v;
-      if (USE_REF) *ref_p = ref;
-      if (KIND == BT_NEURON_ALIF) *gk_p = gk;
-      *psc_p = psc_decay_k<FAST>(pc, dpt, P);
-    } else if (edge) {
+      d.v[off] = v;
+      if (USE_REF) d.refractory[off] = ref;
+      if (KIND == BT_NEURON_ALIF) d.g_k[off] = gk;
+      d.psc[off] = psc_decay_k<FAST>(pc, dpt, P);
+    } else if (edge[u]) {
       // the first step past the sample's end completes psc of its last step
-      P = add(P, pend);
-      *psc_p = P;
+      P = add(P, pend[u]);
+      d.psc[off] = P;
     }
-    if (TRACES) {
-      const int64_t tix = (k * d.batch + b) * d.n + i;
-      if (d.psc_trace && k > 0) d.psc_trace[tix - d.batch * d.n] = P;
+    if (traces && valid) {
+      const int64_t tix = (k * B + b) * d.n + i;
+      if (d.psc_trace && k > 0) d.psc_trace[tix - int64_t(B) * d.n] = P;
       if (d.v_trace) d.v_trace[tix] = v;
       if (USE_REF && d.ref_trace) d.ref_trace[tix] = ref;
       if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[tix] = gk;
       if (d.spikes) d.spikes[tix] = s;
     }
+    const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
+    if (lane == 0 && wg < words) {
+      d.hist[(int64_t(h_t) * B + b) * words + wg] = word;
+      if (d.raster) d.raster[(k * B + b) * words + wg] = word;
+    }
+    if (s != 0.0f) bits |= 1u << (b & 31);
   }
-  return s;
+  if (bits) atomicOr(s_mask + l * ms + (b0 >> 5), bits);
 }
 
-template <int KIND, bool HARD, bool USE_REF, bool FAST, bool TRACES>
+// Record loads of the delivery: the neuron id and MS mask words (records of
+// tile_rec_words(batch) words, 16-byte aligned for MS >= 2).
+template <int MS>
+__device__ __forceinline__ uint32_t load_record(const uint32_t* r, uint32_t (&m)[MS]) {
+  if constexpr (MS == 1) {
+    const uint2 a = __ldcg(reinterpret_cast<const uint2*>(r));
+    m[0] = a.y;
+    return a.x;
+  } else if constexpr (MS == 2) {
+    const uint4 a = __ldcg(reinterpret_cast<const uint4*>(r));
+    m[0] = a.y;
+    m[1] = a.z;
+    return a.x;
+  } else {
+    // MS = 4: records of 8 words, two 16-byte loads; MS = 8: records of 16
+    // words, the first 12 read (the id and 8 mask words)
+    uint32_t w[MS + 4];
+#pragma unroll
+    for (int q = 0; q < (MS + 4) / 4; ++q) {
+      const uint4 a = __ldcg(reinterpret_cast<const uint4*>(r) + q);
+      w[4 * q] = a.x;
+      w[4 * q + 1] = a.y;
+      w[4 * q + 2] = a.z;
+      w[4 * q + 3] = a.w;
+    }
+#pragma unroll
+    for (int q = 0; q < MS; ++q) m[q] = w[1 + q];
+    return w[0];
+  }
+}
+
+template <int KIND, bool HARD, bool USE_REF, bool FAST, int MS>
 __global__ void __launch_bounds__(kTileThreads, 1) k_tile_engine(bt_engine_desc d) {
   extern __shared__ float tile_smem[];
   const int Tp = d.tile_posts, P = d.n_tiles;
@@ -175,20 +251,24 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_engine(bt_engine_desc 
   const int tile = blockIdx.x;
   const int64_t p0 = int64_t(tile) * Tp;
   const int NW = Tp >> 5;  // 32-neuron words of the tile
+  const int NG = int((B + kTileU - 1) / kTileU);
   float* s_acc = tile_smem;                                            // [B][Tp]
   uint32_t* s_mask = reinterpret_cast<uint32_t*>(s_acc + B * Tp);     // [Tp][ms]
   int32_t* s_pre = reinterpret_cast<int32_t*>(s_mask + Tp * ms);      // [P + 1] list offsets
   int32_t* s_scan = s_pre + P + 1;                                    // [kTileWarps] + flag + total
   int* s_flag = s_scan + kTileWarps;
+  int* s_len = s_flag + 2;                                            // [B] sample lengths
   unsigned* ctrl = reinterpret_cast<unsigned*>(d.tile_work);
   int32_t* counts = d.tile_work + kTileCtrl;                            // [2][P]
-  uint32_t* recs = reinterpret_cast<uint32_t*>(counts + 2 * P);        // [2][P][Tp][RW]
+  uint32_t* recs = reinterpret_cast<uint32_t*>(d.tile_work + tile_rec_offset(P));  // [2][P][Tp][RW]
   const unsigned spin = d.spin_limit > 0 ? unsigned(d.spin_limit) : kDefaultSpinLimit;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n32 = int(n);
   const int H = d.hist_len;
+  const bool traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace || d.spikes;
 
   for (int64_t q = threadIdx.x; q < B * Tp; q += kTileThreads) s_acc[q] = 0.0f;
+  for (int q = threadIdx.x; q < int(B); q += kTileThreads)
+    s_len[q] = d.sample_len ? int(min(int64_t(d.sample_len[q]), int64_t(INT32_MAX))) : INT32_MAX;
   unsigned gen = 0;
   if (threadIdx.x == 0) gen = ld_acquire_u32(ctrl + 1);
 
@@ -201,28 +281,14 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_engine(bt_engine_desc 
     const int h_t = int((d.t0 + k) % H);
     for (int q = threadIdx.x; q < Tp * ms; q += kTileThreads) s_mask[q] = 0u;
     __syncthreads();
-    // ---- neuron phase: items (word w, sample b), b fastest
-    for (int64_t it = warp; it < int64_t(NW) * B; it += kTileWarps) {
-      const int w = int(it / B);
-      const int64_t b = it - int64_t(w) * B;
+    // ---- neuron phase: items (word w, group of kTileU samples), groups fastest
+    for (int it = warp; it < NW * NG; it += kTileWarps) {
+      const int w = it / NG;
+      const int b0 = (it - w * NG) * kTileU;
       const int l = w * 32 + lane;
       const int64_t i = p0 + l;
-      const bool valid = i < n;
-      float pc = pc_u;
-      Div dpt = dpt_u;
-      if (!d.psc_uniform) {
-        const int64_t ip = valid ? i : 0;
-        pc = ld(d.psc_coef, ip);
-        dpt = make_div(ld(d.psc_tau, ip), false, 0.0f);
-      }
-      const float s = tile_neuron_item<KIND, HARD, USE_REF, FAST, TRACES>(d, prm_u, k, b, i, valid,
-                                                                          s_acc + b * Tp + l, pc, dpt, n32);
-      const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
-      if (lane == 0 && (p0 >> 5) + w < words) {
-        d.hist[(int64_t(h_t) * B + b) * words + (p0 >> 5) + w] = word;
-        if (d.raster) d.raster[(k * B + b) * words + (p0 >> 5) + w] = word;
-      }
-      if (s != 0.0f) atomicOr(s_mask + l * ms + int(b >> 5), 1u << (b & 31));
+      tile_neuron_item<KIND, HARD, USE_REF, FAST>(d, prm_u, k, b0, i, i < n, l, Tp, s_acc, s_len, s_mask, ms, pc_u,
+                                                  dpt_u, h_t, words, (p0 >> 5) + w, traces);
     }
     __syncthreads();
     // ---- compaction: the tile's spiking neurons, in ascending id order
@@ -239,14 +305,14 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_engine(bt_engine_desc 
       if (lane == 0) s_scan[warp] = __popc(bal);
       __syncthreads();
       if (warp == 0) {
-        const int c = s_scan[lane];
+        const int c = lane < kTileWarps ? s_scan[lane] : 0;
         int incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
           const int y = __shfl_up_sync(0xffffffffu, incl, o);
           if (lane >= o) incl += y;
         }
-        s_scan[lane] = incl - c;
+        if (lane < kTileWarps) s_scan[lane] = incl - c;
         if (lane == 31) s_flag[1] = incl;
       }
       __syncthreads();
@@ -300,7 +366,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_engine(bt_engine_desc 
       int carry = 0;
       for (int q0 = 0; q0 < P; q0 += 32) {
         const int q = q0 + lane;
-        const int c = q < P ? ld_acquire_u32(reinterpret_cast<const unsigned*>(cnt + q)) : 0;
+        const int c = q < P ? int(ld_acquire_u32(reinterpret_cast<const unsigned*>(cnt + q))) : 0;
         int incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -317,34 +383,75 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_engine(bt_engine_desc 
     const uint32_t* recb = recs + int64_t(buf) * P * Tp * RW;
     const int32_t* toff = d.tile_off;
     const uint64_t pol_stream = l2_evict_first();
-    for (int idx = threadIdx.x; idx < total; idx += kTileThreads) {
-      // list holding entry idx: the last q with s_pre[q] <= idx
-      int lo = 0, hi = P - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (s_pre[mid] <= idx) lo = mid;
-        else hi = mid - 1;
+    constexpr int G = kTileGroups;
+    for (int base0 = warp * 32 * G; base0 < total; base0 += kTileWarps * 32 * G) {
+      // kTileGroups records per lane: their ids, masks and tile segments,
+      // every load issued before any is used
+      int32_t e0[G], cntg[G];
+      uint32_t mk[G][MS];
+      uint32_t jj[G];
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const int idx = base0 + g * 32 + lane;
+        jj[g] = 0xffffffffu;
+#pragma unroll
+        for (int q = 0; q < MS; ++q) mk[g][q] = 0u;
+        if (idx < total) {
+          int lo = 0, hi = P - 1;  // the list holding entry idx: the last q with s_pre[q] <= idx
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_pre[mid] <= idx) lo = mid;
+            else hi = mid - 1;
+          }
+          jj[g] = load_record<MS>(recb + (int64_t(lo) * Tp + (idx - s_pre[lo])) * RW, mk[g]);
+        }
       }
-      const uint32_t* r = recb + (int64_t(lo) * Tp + (idx - s_pre[lo])) * RW;
-      const uint32_t j = __ldcg(r);
-      const int32_t* tj = toff + int64_t(j) * (P + 1) + tile;
-      const int32_t e0 = __ldg(tj), e1 = __ldg(tj + 1);
-      if (e0 == e1) continue;
-      uint32_t m[8];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) m[q] = q < ms ? __ldcg(r + 1 + q) : 0u;
-      for (int32_t e = e0; e < e1; ++e) {
-        const uint2 rec2 = ld_nc_u2(d.csr_edges + 2 * int64_t(e), pol_stream);
-        const int lp = int((rec2.x & kIdMask) - uint32_t(p0));
-        const float wv = __uint_as_float(rec2.y);
+      for (int g = 0; g < G; ++g) {
+        e0[g] = 0;
+        cntg[g] = 0;
+        if (jj[g] != 0xffffffffu) {
+          const int32_t* tj = toff + int64_t(jj[g]) * (P + 1) + tile;
+          e0[g] = __ldg(tj);
+          cntg[g] = __ldg(tj + 1) - e0[g];
+        }
+      }
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          if (q >= ms) break;
-          uint32_t mm = m[q];
-          while (mm) {
-            const int bit = __ffs(mm) - 1;
-            mm &= mm - 1;
-            atomicAdd(s_acc + (q * 32 + bit) * Tp + lp, wv);
+      for (int g = 0; g < G; ++g) {
+        // the 32 records' segments walked as one flattened edge range, a lane per edge
+        int incl = cntg[g];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        const int excl = incl - cntg[g];
+        const int tot = __shfl_sync(0xffffffffu, incl, 31);
+        for (int f0 = 0; f0 < tot; f0 += 32) {
+          const int f = f0 + lane;
+          int r = 0;  // the last lane whose excl <= f
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1) {
+            const int x = __shfl_sync(0xffffffffu, excl, r + step);
+            if (x <= f) r += step;
+          }
+          const int eb = __shfl_sync(0xffffffffu, e0[g], r) + (f - __shfl_sync(0xffffffffu, excl, r));
+          uint32_t m[MS];
+#pragma unroll
+          for (int q = 0; q < MS; ++q) m[q] = __shfl_sync(0xffffffffu, mk[g][q], r);
+          if (f < tot) {
+            const uint2 rec2 = ld_nc_u2(d.csr_edges + 2 * int64_t(eb), pol_stream);
+            const int lp = int((rec2.x & kIdMask) - uint32_t(p0));
+            const float wv = __uint_as_float(rec2.y);
+#pragma unroll
+            for (int q = 0; q < MS; ++q) {
+              uint32_t mm = q < ms ? m[q] : 0u;
+              while (mm) {
+                const int bit = __ffs(mm) - 1;
+                mm &= mm - 1;
+                atomicAdd(s_acc + (q * 32 + bit) * Tp + lp, wv);
+              }
+            }
           }
         }
       }
@@ -377,12 +484,19 @@ __global__ void k_tile_offsets(int64_t rows, const int32_t* __restrict__ csr_ptr
   off[gid] = lo;
 }
 
+template <int KIND, bool HARD, bool USE_REF, bool FAST>
+auto tile_kernel(int ms) {
+  // the record layout's bucket (tile_mask_bucket): 1, 2, 4 (3..4 words) or 8 (5..8)
+  return ms == 1 ? k_tile_engine<KIND, HARD, USE_REF, FAST, 1>
+         : ms == 2 ? k_tile_engine<KIND, HARD, USE_REF, FAST, 2>
+         : ms == 4 ? k_tile_engine<KIND, HARD, USE_REF, FAST, 4> : k_tile_engine<KIND, HARD, USE_REF, FAST, 8>;
+}
+
 template <int KIND, bool HARD, bool USE_REF>
-int tile_launch(const bt_engine_desc& d, bool fast, bool traces, cudaStream_t s) {
-  void (*kern)(bt_engine_desc) =
-      fast ? (traces ? k_tile_engine<KIND, HARD, USE_REF, true, true> : k_tile_engine<KIND, HARD, USE_REF, true, false>)
-           : (traces ? k_tile_engine<KIND, HARD, USE_REF, false, true>
-                     : k_tile_engine<KIND, HARD, USE_REF, false, false>);
+int tile_launch(const bt_engine_desc& d, bool fast, cudaStream_t s) {
+  const int ms = tile_mask_bucket(d.batch);
+  void (*kern)(bt_engine_desc) = fast ? tile_kernel<KIND, HARD, USE_REF, true>(ms)
+                                      : tile_kernel<KIND, HARD, USE_REF, false>(ms);
   const size_t smem = tile_smem_bytes(d.batch, d.tile_posts, d.n_tiles);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
     return bt_set_error(BT_ERR_UNSUPPORTED, "tile engine: %zu bytes of shared memory refused", smem);
@@ -410,18 +524,17 @@ int tile_launch(const bt_engine_desc& d, bool fast, bool traces, cudaStream_t s)
 }
 
 int run_tile(const bt_engine_desc& d, bool fast, cudaStream_t s) {
-  const bool traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace || d.spikes;
   const bool h = d.neuron.hard_reset != 0, r = d.neuron.use_refractory != 0;
   if (d.neuron.kind == BT_NEURON_LIF) {
-    if (h && r) return tile_launch<BT_NEURON_LIF, true, true>(d, fast, traces, s);
-    if (h) return tile_launch<BT_NEURON_LIF, true, false>(d, fast, traces, s);
-    if (r) return tile_launch<BT_NEURON_LIF, false, true>(d, fast, traces, s);
-    return tile_launch<BT_NEURON_LIF, false, false>(d, fast, traces, s);
+    if (h && r) return tile_launch<BT_NEURON_LIF, true, true>(d, fast, s);
+    if (h) return tile_launch<BT_NEURON_LIF, true, false>(d, fast, s);
+    if (r) return tile_launch<BT_NEURON_LIF, false, true>(d, fast, s);
+    return tile_launch<BT_NEURON_LIF, false, false>(d, fast, s);
   }
-  if (h && r) return tile_launch<BT_NEURON_ALIF, true, true>(d, fast, traces, s);
-  if (h) return tile_launch<BT_NEURON_ALIF, true, false>(d, fast, traces, s);
-  if (r) return tile_launch<BT_NEURON_ALIF, false, true>(d, fast, traces, s);
-  return tile_launch<BT_NEURON_ALIF, false, false>(d, fast, traces, s);
+  if (h && r) return tile_launch<BT_NEURON_ALIF, true, true>(d, fast, s);
+  if (h) return tile_launch<BT_NEURON_ALIF, true, false>(d, fast, s);
+  if (r) return tile_launch<BT_NEURON_ALIF, false, true>(d, fast, s);
+  return tile_launch<BT_NEURON_ALIF, false, false>(d, fast, s);
 }
 
 }  // namespace bt

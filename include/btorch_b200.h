@@ -378,8 +378,8 @@ typedef struct bt_engine_desc {
      tiles covering n, all co-resident (at most one per SM for large tiles).
      tile_off: [n][n_tiles + 1] from bt_tile_offsets (the CSR row of each
      source split at the tile boundaries).  tile_work:
-     bt_tile_work_words(batch, tile_posts, n_tiles) int32 words whose first
-     32 are zero before the first call; word 2 is the status word, nonzero
+     bt_tile_work_words(batch, tile_posts, n_tiles) int32 words, 64-byte
+     aligned, whose first 32 are zero before the first call; word 2 is the status word, nonzero
      (BT_ERR_TIMEOUT) after a grid barrier wait gave up -- the caller reads
      it after the call and clears the first 32 words before reusing them.
      spin_limit: polls of one barrier wait before it gives up (0 = about a
