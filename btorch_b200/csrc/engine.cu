@@ -41,6 +41,7 @@
 // the receptor sum of its C channels (receptor_sum, the reference's
 // psc.reshape(..., n, C).sum(-1) rounding).  Scatter and gather modes.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <type_traits>
 
@@ -180,13 +181,19 @@ struct ScatterScratch {
   int ms;
 };
 
-__device__ __forceinline__ ScatterScratch scatter_scratch(const bt_engine_desc& d, int q) {
+__host__ __device__ __forceinline__ int log2_pow2(int64_t c) {
+  int s = 0;
+  while ((int64_t(1) << s) < c) ++s;
+  return s;
+}
+
+__host__ __device__ __forceinline__ ScatterScratch scatter_scratch(const bt_engine_desc& d, int q) {
   ScatterScratch w;
   const int64_t n = d.n;
   const int64_t Q = int64_t(d.n_bins) + 1;
   w.ms = mask_stride(d.batch);
   w.cap = sub_cap(n);
-  w.cap_shift = __ffsll(w.cap) - 1;
+  w.cap_shift = log2_pow2(w.cap);
   w.count = d.work + q * 2 * kSub;
   w.spk = w.count + kSub;
   w.flag = d.work + Q * 2 * kSub + q * n;
@@ -196,11 +203,32 @@ __device__ __forceinline__ ScatterScratch scatter_scratch(const bt_engine_desc& 
   return w;
 }
 
-// Publish neuron i's spikes of step t in the step's spike set (bit u of
-// `spiked`: sample b0 + u): the samples' bits in the neuron's mask, and the
-// neuron in the compacted list if this warp's samples are the first to spike
-// (one warp-aggregated atomic on one of kSub counters).  Called by every lane
-// of the warp.
+// Publish neuron i's spikes of step t in the step's spike set `ws` (bit u of
+// `spiked`: sample b0 + u): the samples' bits in the neuron's mask -- one
+// atomic, the S samples lie in one 32-sample word (b0 % S == 0, S | 32) --
+// and the neuron in the compacted list if this warp's samples are the first
+// to spike (one warp-aggregated atomic on one of kSub counters).  Called by
+// every lane of the warp.
+__device__ __forceinline__ void publish_spikes_ws(const ScatterScratch& ws, int i, int b0, uint32_t spiked) {
+  if (__ballot_sync(0xffffffffu, spiked != 0) == 0) return;  // warp-uniform
+  const unsigned lane = lane_id();
+  bool first = false;
+  if (spiked) {
+    atomicOr(ws.mask + int64_t(i) * ws.ms + (b0 >> 5), spiked << (b0 & 31));
+    first = atomicOr(ws.flag + i, 1) == 0;
+  }
+  const uint32_t fb = __ballot_sync(0xffffffffu, first);
+  const int sub = (i - int(lane)) >> ws.cap_shift;  // same for the whole warp (cap % 32 == 0)
+  const int nspk = __reduce_add_sync(0xffffffffu, unsigned(__popc(spiked)));
+  if (lane == 0 && nspk) atomicAdd(ws.spk + sub, nspk);
+  if (fb == 0) return;
+  int32_t base = 0;
+  if (lane == 0) base = atomicAdd(ws.count + sub, __popc(fb));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (first) ws.list[int64_t(sub) * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = i;
+}
+
+// The same for a kernel that derives the spike set from the descriptor.
 template <int S>
 __device__ __forceinline__ void publish_spikes(const bt_engine_desc& d, const StepIdx& si, int64_t i, int64_t b0,
                                                uint32_t spiked) {
@@ -230,39 +258,41 @@ __device__ __forceinline__ void publish_spikes(const bt_engine_desc& d, const St
 // consecutive samples; a warp covers one 32-neuron bitmap word of each of
 // them.  All S samples' state is loaded before any is updated (memory-level
 // parallelism), and the neuron's parameters are read once for the S samples.
+// `ws` is the step's spike set, its pointers computed on the host; indices
+// are 32-bit (batch * n < 2^31 in scatter mode, checked on the host) except
+// into the per-step input and trace arrays.
 template <int KIND, bool HARD, bool USE_REF, int S, bool FAST>
-__global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, int64_t k, StepIdx si) {
-  const int64_t n = d.n, B = d.batch;
-  const int64_t words = (n + 31) >> 5;
-  const int64_t i = int64_t(blockIdx.x) * kEngThreads + threadIdx.x;
-  const int64_t b0 = int64_t(blockIdx.y) * S;
-  if ((i & ~int64_t(31)) >= n) return;  // whole warps past the last word
+__global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, int k, StepIdx si, ScatterScratch ws) {
+  const int n = int(d.n), B = int(d.batch);
+  const int words = (n + 31) >> 5;
+  const int i = int(blockIdx.x) * kEngThreads + int(threadIdx.x);
+  const int b0 = int(blockIdx.y) * S;
+  if ((i & ~31) >= n) return;  // whole warps past the last word
   const bool valid = i < n;
-  const int nb = int(B - b0 < S ? B - b0 : S);  // samples of this block (uniform)
-  // Row pointers of sample b0 for this neuron; sample u is at +u * n.
-  const int64_t off0 = b0 * n + (valid ? i : 0);
+  const int nb = B - b0 < S ? B - b0 : S;  // samples of this block (uniform)
+  const int off0 = b0 * n + (valid ? i : 0);
   float* __restrict__ ring_p = d.ring + off0;  // acc: W z of the previous step
   float* __restrict__ psc_p = d.psc + off0;
   float* __restrict__ v_p = d.v + off0;
   float* __restrict__ ref_p = USE_REF ? d.refractory + off0 : nullptr;
   float* __restrict__ gk_p = KIND == BT_NEURON_ALIF ? d.g_k + off0 : nullptr;
-  const float* __restrict__ x_p = d.x ? d.x + k * B * n + off0 : nullptr;
-  float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
-  int64_t lenv[S];
+  const float* __restrict__ x_p = d.x ? d.x + int64_t(k) * B * n + off0 : nullptr;
   const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
-  const int n32 = int(n);  // batch * n < 2^31 in scatter mode (checked on the host)
   // Every load before the first store: a load behind a store through a
   // pointer that may alias it waits for the store.  A sample past its length
   // (k > len) reads and writes no state unless state traces are requested:
   // its state is frozen and its accumulator is not read again in this call.
+  const bool traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace || d.spikes;
   const bool st_traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace;
+  float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
+  int lenv[S];
 #pragma unroll
-  for (int u = 0; u < S; ++u) lenv[u] = (valid && u < nb && d.sample_len) ? d.sample_len[b0 + u] : INT64_MAX;
+  for (int u = 0; u < S; ++u) lenv[u] = (valid && u < nb && d.sample_len) ? d.sample_len[b0 + u] : INT_MAX;
 #pragma unroll
   for (int u = 0; u < S; ++u) {
     const bool in = valid && u < nb;
     const bool live = in && k < lenv[u], edge = in && k <= lenv[u], frozen = in && st_traces;
-    const int o = u * n32;
+    const int o = u * n;
     pend[u] = edge ? ld_f32(ring_p + o, pol_keep) : 0.0f;
     pv[u] = (edge || frozen) ? psc_p[o] : 0.0f;
     xv[u] = (live && x_p) ? ld_nc_f32(x_p + o, pol_stream) : 0.0f;
@@ -270,23 +300,22 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
     rv[u] = ((live || frozen) && USE_REF) ? ref_p[o] : 0.0f;
     gv[u] = ((live || frozen) && KIND == BT_NEURON_ALIF) ? gk_p[o] : 0.0f;
   }
-  const int64_t ip = valid ? i : 0;
+  const int ip = valid ? i : 0;
   const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, ip);
   const float pc = d.psc_uniform ? d.psc_coef_s : ld(d.psc_coef, ip);
   const float pt = d.psc_uniform ? d.psc_tau_s : ld(d.psc_tau, ip);
   const Div dpt = make_div(pt, d.psc_uniform && d.psc_fast_div, d.psc_rcp);
   const unsigned lane = lane_id();
-  const bool traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace || d.spikes;
   uint32_t* hist_p = d.hist + (int64_t(si.h_t) * B + b0) * words + (i >> 5);
-  uint32_t* raster_p = d.raster ? d.raster + (k * B + b0) * words + (i >> 5) : nullptr;
+  uint32_t* raster_p = d.raster ? d.raster + (int64_t(k) * B + b0) * words + (i >> 5) : nullptr;
   uint32_t spiked = 0;  // bit u: spiked in sample b0 + u
 #pragma unroll
   for (int u = 0; u < S; ++u) {
     if (u >= nb) break;  // uniform across the block
-    const int o = u * n32;
+    const int o = u * n;
     float s = 0.0f;
     if (valid) {
-      const int64_t len = lenv[u];
+      const int len = lenv[u];
       if (k <= len) st_f32(ring_p + o, 0.0f, pol_keep);
       float v = vv[u], ref = rv[u], gk = gv[u];
       float P;
@@ -310,8 +339,8 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
         }
       }
       if (traces) {
-        const int64_t tix = (k * B + b0 + u) * n + i;
-        if (d.psc_trace && k > 0) d.psc_trace[tix - B * n] = P;
+        const int64_t tix = (int64_t(k) * B + b0 + u) * n + i;
+        if (d.psc_trace && k > 0) d.psc_trace[tix - int64_t(B) * n] = P;
         if (d.v_trace) d.v_trace[tix] = v;
         if (USE_REF && d.ref_trace) d.ref_trace[tix] = ref;
         if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[tix] = gk;
@@ -320,12 +349,12 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
     }
     const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
     if (lane == 0) {
-      hist_p[u * int(words)] = word;
-      if (raster_p) raster_p[u * int(words)] = word;
+      hist_p[u * words] = word;
+      if (raster_p) raster_p[u * words] = word;
     }
     if (s != 0.0f) spiked |= 1u << u;
   }
-  publish_spikes<S>(d, si, i, b0, spiked);
+  publish_spikes_ws(ws, i, b0, spiked);
 }
 
 // SCATTER neuron step with receptor channels (n_rec = C > 1): for each
@@ -1436,6 +1465,7 @@ int engine_check(const bt_engine_desc* d) {
   BT_CHECK_ARG(d->n_bins >= 1 && d->n_bins <= BT_MAX_BINS, "n_bins=%d outside [1, 128]", d->n_bins);
   BT_CHECK_ARG(d->hist_len >= d->n_bins + 2, "hist_len=%d must be >= n_bins + 2", d->hist_len);
   BT_CHECK_ARG(d->n_steps >= 0 && d->t0 >= 0, "negative step index");
+  BT_CHECK_ARG(d->n_steps < (int64_t(1) << 31), "n_steps must be below 2^31");
   BT_CHECK_ARG(d->mode == BT_MODE_SCATTER || d->mode == BT_MODE_GATHER || d->mode == BT_MODE_PULL ||
                    d->mode == BT_MODE_TILE,
                "mode=%d", d->mode);
@@ -1548,7 +1578,7 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
     for (int64_t k = 0; k < d.n_steps; ++k) {
       const StepIdx si = step_idx(d.t0 + k, d.n_bins, d.hist_len);
       if (C > 1) rec<<<rgrid, kEngThreads, 0, s>>>(d, k, si);
-      else neuron<<<grid, kEngThreads, 0, s>>>(d, k, si);
+      else neuron<<<grid, kEngThreads, 0, s>>>(d, int(k), si, scatter_scratch(d, si.q_t));
       scatter<<<sgrid, kEngThreads, 0, s>>>(d, k, si);
     }
     BT_CHECK_LAUNCH("k_eng_neuron/k_eng_scatter");
