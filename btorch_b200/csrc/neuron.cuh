@@ -45,16 +45,30 @@ __device__ __forceinline__ float divc(float x, float c, float rc) { return rc !=
 
 // x / c from the correctly rounded reciprocal r of c: q = x r, then one FMA
 // correction with the exact remainder x - q c (Markstein's division step,
-// IBM J. Res. Dev. 34(1), 1990).  Outside 2^-100 <= |q| <= 2^100 (zeros,
-// subnormal or huge quotients, inf, nan) it divides.  Whether this equals the
-// IEEE quotient for every x depends on c; the host enables it only for
-// divisors checked exhaustively against __fdiv_rn (bt_fast_div_check).
+// IBM J. Res. Dev. 34(1), 1990).  A zero x gives q = x r, which is already
+// the IEEE quotient (a zero whose sign is sign(x) xor sign(c)).  A tiny
+// quotient, 2^-124 <= |q| < 2^-100, is computed for x 2^64 and scaled back by
+// 2^-64 (both scalings exact: the result stays normal).  These cases are
+// common -- a silent synapse, a neuron at rest, a decaying trace long after
+// its last input -- and must not take the slow path.  Otherwise, outside
+// 2^-100 <= |q| <= 2^100 (subnormal or huge quotients, inf, nan), it divides.
+// Whether this equals the IEEE quotient for every x depends on c; the host
+// enables it only for divisors checked against __fdiv_rn for every fp32 bit
+// pattern of x (bt_fast_div_check).
 __device__ __forceinline__ float div_recip(float x, float c, float r) {
-  const float q = mul(x, r);
-  const float aq = fabsf(q);
+  float q = mul(x, r);
+  if (x == 0.0f) return q;
+  float aq = fabsf(q);
+  float xs = x, back = 1.0f;
+  if (aq < 0x1p-100f && aq >= 0x1p-124f) {
+    xs = mul(x, 0x1p64f);
+    q = mul(xs, r);
+    aq = fabsf(q);
+    back = 0x1p-64f;
+  }
   if (!(aq >= 0x1p-100f && aq <= 0x1p100f)) return div(x, c);
-  const float e = __fmaf_rn(-q, c, x);
-  return __fmaf_rn(e, r, q);
+  const float e = __fmaf_rn(-q, c, xs);
+  return mul(__fmaf_rn(e, r, q), back);
 }
 
 // A divisor with its exact evaluation: kind 1 = power of two (multiply by the

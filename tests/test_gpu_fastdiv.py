@@ -31,3 +31,12 @@ def test_wrong_reciprocal_is_caught():
     """The correction step absorbs a reciprocal a few ulp off, not a wrong one."""
     c32 = np.float32(20.0)
     assert mismatches(c32, np.float32(1.0) / c32 * np.float32(1.001)) > 0
+
+
+@pytest.mark.parametrize("c", [5.0, 20.0, 200.0])
+def test_benchmark_time_constants_take_the_fast_path(c):
+    """The synaptic (5), membrane (20) and adaptation (200) time constants of
+    the benchmark networks divide exactly through the reciprocal path for
+    every fp32 input, zeros and tiny quotients included."""
+    c32 = np.float32(c)
+    assert mismatches(c32, np.float32(1.0) / c32) == 0
