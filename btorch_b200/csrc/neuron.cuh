@@ -55,20 +55,27 @@ __device__ __forceinline__ float divc(float x, float c, float rc) { return rc !=
 // Whether this equals the IEEE quotient for every x depends on c; the host
 // enables it only for divisors checked against __fdiv_rn for every fp32 bit
 // pattern of x (bt_fast_div_check).
-__device__ __forceinline__ float div_recip(float x, float c, float r) {
-  float q = mul(x, r);
+__device__ __noinline__ float div_recip_rare(float x, float c, float r) {
+  const float q = mul(x, r);
   if (x == 0.0f) return q;
-  float aq = fabsf(q);
-  float xs = x, back = 1.0f;
+  const float aq = fabsf(q);
   if (aq < 0x1p-100f && aq >= 0x1p-124f) {
-    xs = mul(x, 0x1p64f);
-    q = mul(xs, r);
-    aq = fabsf(q);
-    back = 0x1p-64f;
+    const float xs = mul(x, 0x1p64f);
+    const float qs = mul(xs, r);
+    const float e = __fmaf_rn(-qs, c, xs);
+    return mul(__fmaf_rn(e, r, qs), 0x1p-64f);
   }
-  if (!(aq >= 0x1p-100f && aq <= 0x1p100f)) return div(x, c);
-  const float e = __fmaf_rn(-q, c, xs);
-  return mul(__fmaf_rn(e, r, q), back);
+  return div(x, c);
+}
+
+__device__ __forceinline__ float div_recip(float x, float c, float r) {
+  const float q = mul(x, r);
+  const float aq = fabsf(q);
+  if (aq >= 0x1p-100f && aq <= 0x1p100f) {  // the common case: six instructions
+    const float e = __fmaf_rn(-q, c, x);
+    return __fmaf_rn(e, r, q);
+  }
+  return div_recip_rare(x, c, r);
 }
 
 // A divisor with its exact evaluation: kind 1 = power of two (multiply by the
