@@ -55,7 +55,7 @@ __device__ __forceinline__ float divc(float x, float c, float rc) { return rc !=
 // Whether this equals the IEEE quotient for every x depends on c; the host
 // enables it only for divisors checked against __fdiv_rn for every fp32 bit
 // pattern of x (bt_fast_div_check).
-__device__ __noinline__ float div_recip_rare(float x, float c, float r) {
+static __device__ __noinline__ float div_recip_rare(float x, float c, float r) {
   const float q = mul(x, r);
   if (x == 0.0f) return q;
   const float aq = fabsf(q);
