@@ -254,21 +254,63 @@ __device__ __forceinline__ void publish_spikes(const bt_engine_desc& d, const St
   if (first) ws.list[sub * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = int32_t(i);
 }
 
+// The state of one neuron-step item (S samples of one neuron) loaded ahead of
+// its update.
+template <int S>
+struct NeuronItem {
+  float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
+  int len[S];
+  int i, b0, nb, off0;
+  bool valid, any;
+};
+
+// Issue the loads of item `it` (lane-items word-major within a sample group).
+// A sample past its length (k > len) reads no state unless state traces are
+// requested: its state is frozen and its accumulator is not read again.
+template <int KIND, bool USE_REF, int S>
+__device__ __forceinline__ void load_item(NeuronItem<S>& q, int it, int items, int words, int n, int B, int k,
+                                          const float* ring, const float* psc, const float* vs, const float* refs,
+                                          const float* gks, const float* xk, const int32_t* slen, bool st_traces,
+                                          uint64_t pol_stream, uint64_t pol_keep) {
+  q.any = it - int(lane_id()) < items;  // warp-uniform
+  const int g = it / (words * 32);
+  q.i = it - g * (words * 32);
+  q.b0 = g * S;
+  q.valid = q.any && q.i < n;
+  q.nb = B - q.b0 < S ? B - q.b0 : S;
+  q.off0 = q.b0 * n + (q.valid ? q.i : 0);
+#pragma unroll
+  for (int u = 0; u < S; ++u) q.len[u] = (q.valid && u < q.nb && slen) ? slen[q.b0 + u] : INT_MAX;
+#pragma unroll
+  for (int u = 0; u < S; ++u) {
+    const bool in = q.valid && u < q.nb;
+    const bool live = in && k < q.len[u], edge = in && k <= q.len[u], frozen = in && st_traces;
+    const int o = q.off0 + u * n;
+    q.pend[u] = edge ? ld_f32(ring + o, pol_keep) : 0.0f;
+    q.pv[u] = (edge || frozen) ? psc[o] : 0.0f;
+    q.xv[u] = (live && xk) ? ld_nc_f32(xk + o, pol_stream) : 0.0f;
+    q.vv[u] = (live || frozen) ? vs[o] : 0.0f;
+    q.rv[u] = ((live || frozen) && USE_REF) ? refs[o] : 0.0f;
+    q.gv[u] = ((live || frozen) && KIND == BT_NEURON_ALIF) ? gks[o] : 0.0f;
+  }
+}
+
 // Grid-stride over items (32-neuron word, group of S consecutive samples): a
 // thread owns neuron i for S samples per item, a warp one 32-neuron bitmap
 // word of each of them, consecutive warps consecutive words.  The per-thread
 // set-up (parameters, divisors, pointers, cache policies) is done once and
-// amortised over the thread's items.  Within an item all S samples' state is
-// loaded before any is updated (memory-level parallelism).  `ws` is the
-// step's spike set, its pointers computed on the host; indices are 32-bit
-// (batch * n < 2^31 in scatter mode, checked on the host) except into the
-// per-step input and trace arrays.
+// amortised over the thread's items, and the loop is software-pipelined: the
+// next item's loads are issued before this item's update and stores (items
+// touch disjoint state), so a warp keeps two items' loads in flight.  `ws` is
+// the step's spike set, its pointers computed on the host; indices are
+// 32-bit (batch * n < 2^31 in scatter mode, checked on the host) except into
+// the per-step input and trace arrays.
 template <int KIND, bool HARD, bool USE_REF, int S, bool FAST>
 __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, int k, StepIdx si, ScatterScratch ws) {
   const int n = int(d.n), B = int(d.batch);
   const int words = (n + 31) >> 5;
   const int groups = (B + S - 1) / S;
-  const int items = groups * words * 32;  // lane-items: word-major within a sample group
+  const int items = groups * words * 32;
   const int stride = int(gridDim.x) * kEngThreads;
   float* __restrict__ ring = d.ring;
   float* __restrict__ psc = d.psc;
@@ -287,35 +329,17 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   float pc = d.psc_uniform ? d.psc_coef_s : 0.0f;
   Div dpt = make_div(d.psc_uniform ? d.psc_tau_s : 1.0f, d.psc_uniform && d.psc_fast_div, d.psc_rcp);
   const unsigned lane = lane_id();
-  for (int it = int(blockIdx.x) * kEngThreads + int(threadIdx.x); it - int(lane) < items; it += stride) {
-    const int g = it / (words * 32);
-    const int i = it - g * (words * 32);
-    const int b0 = g * S;
-    const bool valid = i < n;
-    const int nb = B - b0 < S ? B - b0 : S;  // samples of this item (uniform across the warp)
-    const int off0 = b0 * n + (valid ? i : 0);
-    // Every load before the first store: a load behind a store through a
-    // pointer that may alias it waits for the store.  A sample past its
-    // length (k > len) reads and writes no state unless state traces are
-    // requested: its state is frozen and its accumulator is not read again.
-    float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
-    int lenv[S];
-#pragma unroll
-    for (int u = 0; u < S; ++u) lenv[u] = (valid && u < nb && slen) ? slen[b0 + u] : INT_MAX;
-#pragma unroll
-    for (int u = 0; u < S; ++u) {
-      const bool in = valid && u < nb;
-      const bool live = in && k < lenv[u], edge = in && k <= lenv[u], frozen = in && st_traces;
-      const int o = off0 + u * n;
-      pend[u] = edge ? ld_f32(ring + o, pol_keep) : 0.0f;
-      pv[u] = (edge || frozen) ? psc[o] : 0.0f;
-      xv[u] = (live && xk) ? ld_nc_f32(xk + o, pol_stream) : 0.0f;
-      vv[u] = (live || frozen) ? vs[o] : 0.0f;
-      rv[u] = ((live || frozen) && USE_REF) ? refs[o] : 0.0f;
-      gv[u] = ((live || frozen) && KIND == BT_NEURON_ALIF) ? gks[o] : 0.0f;
-    }
+  int it = int(blockIdx.x) * kEngThreads + int(threadIdx.x);
+  NeuronItem<S> cur;
+  load_item<KIND, USE_REF, S>(cur, it, items, words, n, B, k, ring, psc, vs, refs, gks, xk, slen, st_traces,
+                              pol_stream, pol_keep);
+  while (cur.any) {
+    NeuronItem<S> nxt;
+    load_item<KIND, USE_REF, S>(nxt, it + stride, items, words, n, B, k, ring, psc, vs, refs, gks, xk, slen,
+                                st_traces, pol_stream, pol_keep);
+    const int i = cur.i, b0 = cur.b0;
     if (!uniform) {
-      const int ip = valid ? i : 0;
+      const int ip = cur.valid ? i : 0;
       prm = load_params<KIND, USE_REF>(d.neuron, ip);
       pc = d.psc_uniform ? d.psc_coef_s : ld(d.psc_coef, ip);
       dpt = make_div(d.psc_uniform ? d.psc_tau_s : ld(d.psc_tau, ip), d.psc_uniform && d.psc_fast_div, d.psc_rcp);
@@ -323,17 +347,17 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
     uint32_t spiked = 0;  // bit u: spiked in sample b0 + u
 #pragma unroll
     for (int u = 0; u < S; ++u) {
-      if (u >= nb) break;  // uniform across the warp
-      const int o = off0 + u * n;
+      if (u >= cur.nb) break;  // uniform across the warp
+      const int o = cur.off0 + u * n;
       float s = 0.0f;
-      if (valid) {
-        const int len = lenv[u];
+      if (cur.valid) {
+        const int len = cur.len[u];
         if (k <= len) st_f32(ring + o, 0.0f, pol_keep);
-        float v = vv[u], ref = rv[u], gk = gv[u];
+        float v = cur.vv[u], ref = cur.rv[u], gk = cur.gv[u];
         float P;
         if (k < len) {
-          P = add(pv[u], pend[u]);
-          const float I = xk ? add(P, xv[u]) : P;
+          P = add(cur.pv[u], cur.pend[u]);
+          const float I = xk ? add(P, cur.xv[u]) : P;
           s = neuron_update<KIND, HARD, USE_REF, true, FAST>(prm, I, v, ref, gk).spike;
           vs[o] = v;
           if (USE_REF) refs[o] = ref;
@@ -343,9 +367,9 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
           // Finished sample: its state freezes at its last step.  On the
           // first step past the end the pending sum completes psc of that
           // last step; later arrivals are dropped.
-          P = pv[u];
+          P = cur.pv[u];
           if (k == len) {
-            P = add(P, pend[u]);
+            P = add(P, cur.pend[u]);
             psc[o] = P;
           }
         }
@@ -367,6 +391,8 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
       if (s != 0.0f) spiked |= 1u << u;
     }
     publish_spikes_ws(ws, i, b0, spiked);
+    cur = nxt;
+    it += stride;
   }
 }
 
