@@ -254,38 +254,28 @@ __device__ __forceinline__ void publish_spikes(const bt_engine_desc& d, const St
   if (first) ws.list[sub * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = int32_t(i);
 }
 
-// The state of one neuron-step item (S samples of one neuron) loaded ahead of
-// its update.
+// The state of S samples of one neuron, loaded ahead of their update.
 template <int S>
 struct NeuronItem {
   float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
   int len[S];
-  int i, b0, nb, off0;
-  bool valid, any;
 };
 
-// Issue the loads of item `it` (lane-items word-major within a sample group).
+// Issue the loads of samples b0 .. b0+S-1 of neuron i (off0 = b0 * n + i).
 // A sample past its length (k > len) reads no state unless state traces are
 // requested: its state is frozen and its accumulator is not read again.
 template <int KIND, bool USE_REF, int S>
-__device__ __forceinline__ void load_item(NeuronItem<S>& q, int it, int items, int words, int n, int B, int k,
+__device__ __forceinline__ void load_item(NeuronItem<S>& q, bool valid, int b0, int nb, int off0, int n, int k,
                                           const float* ring, const float* psc, const float* vs, const float* refs,
                                           const float* gks, const float* xk, const int32_t* slen, bool st_traces,
                                           uint64_t pol_stream, uint64_t pol_keep) {
-  q.any = it - int(lane_id()) < items;  // warp-uniform
-  const int g = it / (words * 32);
-  q.i = it - g * (words * 32);
-  q.b0 = g * S;
-  q.valid = q.any && q.i < n;
-  q.nb = B - q.b0 < S ? B - q.b0 : S;
-  q.off0 = q.b0 * n + (q.valid ? q.i : 0);
 #pragma unroll
-  for (int u = 0; u < S; ++u) q.len[u] = (q.valid && u < q.nb && slen) ? slen[q.b0 + u] : INT_MAX;
+  for (int u = 0; u < S; ++u) q.len[u] = (valid && u < nb && slen) ? slen[b0 + u] : INT_MAX;
 #pragma unroll
   for (int u = 0; u < S; ++u) {
-    const bool in = q.valid && u < q.nb;
+    const bool in = valid && u < nb;
     const bool live = in && k < q.len[u], edge = in && k <= q.len[u], frozen = in && st_traces;
-    const int o = q.off0 + u * n;
+    const int o = off0 + u * n;
     q.pend[u] = edge ? ld_f32(ring + o, pol_keep) : 0.0f;
     q.pv[u] = (edge || frozen) ? psc[o] : 0.0f;
     q.xv[u] = (live && xk) ? ld_nc_f32(xk + o, pol_stream) : 0.0f;
@@ -295,23 +285,23 @@ __device__ __forceinline__ void load_item(NeuronItem<S>& q, int it, int items, i
   }
 }
 
-// Grid-stride over items (32-neuron word, group of S consecutive samples): a
-// thread owns neuron i for S samples per item, a warp one 32-neuron bitmap
-// word of each of them, consecutive warps consecutive words.  The per-thread
-// set-up (parameters, divisors, pointers, cache policies) is done once and
-// amortised over the thread's items, and the loop is software-pipelined: the
-// next item's loads are issued before this item's update and stores (items
-// touch disjoint state), so a warp keeps two items' loads in flight.  `ws` is
-// the step's spike set, its pointers computed on the host; indices are
-// 32-bit (batch * n < 2^31 in scatter mode, checked on the host) except into
-// the per-step input and trace arrays.
+// A warp owns a 32-neuron word (lane = neuron) for every sample of the batch:
+// it walks the samples in groups of S (grid-stride over words), each group's
+// loads issued before the previous group's update and stores
+// (software-pipelined; groups touch disjoint state), and builds each neuron's
+// sample mask in registers.  Since no other warp handles these neurons, the
+// step's spike set is published with plain stores of the mask rows and one
+// warp-aggregated list append per word -- no per-neuron atomics, no waiting on
+// their results.  The per-thread set-up (parameters, divisors, pointers,
+// cache policies) is done once.  `ws` is the step's spike set, its pointers
+// computed on the host; indices are 32-bit (batch * n < 2^31 in scatter mode,
+// checked on the host) except into the per-step input and trace arrays.
 template <int KIND, bool HARD, bool USE_REF, int S, bool FAST>
 __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, int k, StepIdx si, ScatterScratch ws) {
   const int n = int(d.n), B = int(d.batch);
   const int words = (n + 31) >> 5;
   const int groups = (B + S - 1) / S;
-  const int items = groups * words * 32;
-  const int stride = int(gridDim.x) * kEngThreads;
+  const int warps_total = int(gridDim.x) * (kEngThreads / 32);
   float* __restrict__ ring = d.ring;
   float* __restrict__ psc = d.psc;
   float* __restrict__ vs = d.v;
@@ -324,75 +314,112 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
   const bool traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace || d.spikes;
   const bool st_traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace;
-  const bool uniform = d.neuron.uniform && d.psc_uniform;
-  NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, 0);
-  float pc = d.psc_uniform ? d.psc_coef_s : 0.0f;
-  Div dpt = make_div(d.psc_uniform ? d.psc_tau_s : 1.0f, d.psc_uniform && d.psc_fast_div, d.psc_rcp);
   const unsigned lane = lane_id();
-  int it = int(blockIdx.x) * kEngThreads + int(threadIdx.x);
-  NeuronItem<S> cur;
-  load_item<KIND, USE_REF, S>(cur, it, items, words, n, B, k, ring, psc, vs, refs, gks, xk, slen, st_traces,
-                              pol_stream, pol_keep);
-  while (cur.any) {
-    NeuronItem<S> nxt;
-    load_item<KIND, USE_REF, S>(nxt, it + stride, items, words, n, B, k, ring, psc, vs, refs, gks, xk, slen,
-                                st_traces, pol_stream, pol_keep);
-    const int i = cur.i, b0 = cur.b0;
-    if (!uniform) {
-      const int ip = cur.valid ? i : 0;
-      prm = load_params<KIND, USE_REF>(d.neuron, ip);
-      pc = d.psc_uniform ? d.psc_coef_s : ld(d.psc_coef, ip);
-      dpt = make_div(d.psc_uniform ? d.psc_tau_s : ld(d.psc_tau, ip), d.psc_uniform && d.psc_fast_div, d.psc_rcp);
+  const NeuronParams prm_u = load_params<KIND, USE_REF>(d.neuron, 0);
+  const float pc_u = d.psc_uniform ? d.psc_coef_s : 0.0f;
+  const Div dpt_u = make_div(d.psc_uniform ? d.psc_tau_s : 1.0f, d.psc_uniform && d.psc_fast_div, d.psc_rcp);
+  for (int w = int(blockIdx.x) * (kEngThreads / 32) + int(threadIdx.x >> 5); w < words; w += warps_total) {
+    const int i = w * 32 + int(lane);
+    const bool valid = i < n;
+    const int ip = valid ? i : 0;
+    NeuronParams prm = prm_u;
+    float pc = pc_u;
+    Div dpt = dpt_u;
+    if (!d.neuron.uniform) prm = load_params<KIND, USE_REF>(d.neuron, ip);
+    if (!d.psc_uniform) {
+      pc = ld(d.psc_coef, ip);
+      dpt = make_div(ld(d.psc_tau, ip), false, 0.0f);
     }
-    uint32_t spiked = 0;  // bit u: spiked in sample b0 + u
+    // the neuron's sample mask (batch <= 256), a row of 32-sample words per
+    // lane in shared memory (each lane owns its own)
+    __shared__ uint32_t s_m[kEngThreads / 32][8][32];
+    uint32_t(*m)[32] = s_m[threadIdx.x >> 5];
 #pragma unroll
-    for (int u = 0; u < S; ++u) {
-      if (u >= cur.nb) break;  // uniform across the warp
-      const int o = cur.off0 + u * n;
-      float s = 0.0f;
-      if (cur.valid) {
-        const int len = cur.len[u];
-        if (k <= len) st_f32(ring + o, 0.0f, pol_keep);
-        float v = cur.vv[u], ref = cur.rv[u], gk = cur.gv[u];
-        float P;
-        if (k < len) {
-          P = add(cur.pv[u], cur.pend[u]);
-          const float I = xk ? add(P, cur.xv[u]) : P;
-          s = neuron_update<KIND, HARD, USE_REF, true, FAST>(prm, I, v, ref, gk).spike;
-          vs[o] = v;
-          if (USE_REF) refs[o] = ref;
-          if (KIND == BT_NEURON_ALIF) gks[o] = gk;
-          psc[o] = psc_decay_k<FAST>(pc, dpt, P);
-        } else {
-          // Finished sample: its state freezes at its last step.  On the
-          // first step past the end the pending sum completes psc of that
-          // last step; later arrivals are dropped.
-          P = cur.pv[u];
-          if (k == len) {
-            P = add(P, cur.pend[u]);
-            psc[o] = P;
+    for (int q = 0; q < 8; ++q) m[q][lane] = 0u;
+    int nspk = 0;
+    NeuronItem<S> cur;
+    load_item<KIND, USE_REF, S>(cur, valid, 0, B < S ? B : S, ip, n, k, ring, psc, vs, refs, gks, xk, slen,
+                                st_traces, pol_stream, pol_keep);
+    for (int g = 0; g < groups; ++g) {
+      const int b0 = g * S;
+      const int nb = B - b0 < S ? B - b0 : S;  // uniform across the warp
+      NeuronItem<S> nxt;
+      if (g + 1 < groups) {
+        const int b1 = b0 + S;
+        load_item<KIND, USE_REF, S>(nxt, valid, b1, B - b1 < S ? B - b1 : S, b1 * n + ip, n, k, ring, psc, vs, refs,
+                                    gks, xk, slen, st_traces, pol_stream, pol_keep);
+      }
+      const int off0 = b0 * n + ip;
+#pragma unroll
+      for (int u = 0; u < S; ++u) {
+        if (u >= nb) break;  // uniform across the warp
+        const int o = off0 + u * n;
+        float s = 0.0f;
+        if (valid) {
+          const int len = cur.len[u];
+          if (k <= len) st_f32(ring + o, 0.0f, pol_keep);
+          float v = cur.vv[u], ref = cur.rv[u], gk = cur.gv[u];
+          float P;
+          if (k < len) {
+            P = add(cur.pv[u], cur.pend[u]);
+            const float I = xk ? add(P, cur.xv[u]) : P;
+            s = neuron_update<KIND, HARD, USE_REF, true, FAST>(prm, I, v, ref, gk).spike;
+            vs[o] = v;
+            if (USE_REF) refs[o] = ref;
+            if (KIND == BT_NEURON_ALIF) gks[o] = gk;
+            psc[o] = psc_decay_k<FAST>(pc, dpt, P);
+          } else {
+            // Finished sample: its state freezes at its last step.  On the
+            // first step past the end the pending sum completes psc of that
+            // last step; later arrivals are dropped.
+            P = cur.pv[u];
+            if (k == len) {
+              P = add(P, cur.pend[u]);
+              psc[o] = P;
+            }
+          }
+          if (traces) {
+            const int64_t tix = (int64_t(k) * B + b0 + u) * n + i;
+            if (d.psc_trace && k > 0) d.psc_trace[tix - int64_t(B) * n] = P;
+            if (d.v_trace) d.v_trace[tix] = v;
+            if (USE_REF && d.ref_trace) d.ref_trace[tix] = ref;
+            if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[tix] = gk;
+            if (d.spikes) d.spikes[tix] = s;
           }
         }
-        if (traces) {
-          const int64_t tix = (int64_t(k) * B + b0 + u) * n + i;
-          if (d.psc_trace && k > 0) d.psc_trace[tix - int64_t(B) * n] = P;
-          if (d.v_trace) d.v_trace[tix] = v;
-          if (USE_REF && d.ref_trace) d.ref_trace[tix] = ref;
-          if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[tix] = gk;
-          if (d.spikes) d.spikes[tix] = s;
+        const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
+        if (lane == 0) {
+          const int wi = (b0 + u) * words + w;
+          hist[wi] = word;
+          if (raster) raster[wi] = word;
+        }
+        if (s != 0.0f) {
+          const int b = b0 + u;
+          m[b >> 5][lane] |= 1u << (b & 31);
+          ++nspk;
         }
       }
-      const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
-      if (lane == 0) {
-        const int wi = (b0 + u) * words + (i >> 5);
-        hist[wi] = word;
-        if (raster) raster[wi] = word;
-      }
-      if (s != 0.0f) spiked |= 1u << u;
+      if (g + 1 < groups) cur = nxt;
     }
-    publish_spikes_ws(ws, i, b0, spiked);
-    cur = nxt;
-    it += stride;
+    // publish the word's spikes: the mask rows (plain stores: this warp is the
+    // only writer of these neurons' rows, cleared by their last reader), the
+    // spike total and one list append per word
+    const bool any = nspk != 0;
+    const uint32_t fb = __ballot_sync(0xffffffffu, any);
+    if (fb == 0) continue;  // warp-uniform
+    if (any) {
+      uint32_t* mrow = ws.mask + int64_t(i) * ws.ms;
+      for (int q = 0; q < ws.ms; ++q) mrow[q] = m[q][lane];
+    }
+    const int sub = (w * 32) >> ws.cap_shift;  // cap % 32 == 0: one sub-list per word
+    const int tot = __reduce_add_sync(0xffffffffu, unsigned(nspk));
+    int32_t base = 0;
+    if (lane == 0) {
+      atomicAdd(ws.spk + sub, tot);
+      base = atomicAdd(ws.count + sub, __popc(fb));
+    }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (any) ws.list[int64_t(sub) * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = i;
   }
 }
 
@@ -1583,7 +1610,7 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t neuron_items = ceil_div(d.batch, S) * ((n + 31) >> 5) * 32;
+    const int64_t neuron_warps = (n + 31) >> 5;  // a warp per 32-neuron word, all samples
     const unsigned planes = unsigned(d.bin_hi - d.bin_lo + 1);
     // a plane lists at most n rows: no more blocks than n rows need (small
     // networks would otherwise launch mostly idle blocks every step)
@@ -1599,12 +1626,12 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
                        : (S == 1 ? k_eng_neuron<KIND, HARD, USE_REF, 1, false>
                           : S == 2 ? k_eng_neuron<KIND, HARD, USE_REF, 2, false> : k_eng_neuron<KIND, HARD, USE_REF, 4, false>);
     // grid-stride neuron launch: as many blocks as are resident at once (the
-    // kernel's occupancy), fewer when the step has fewer items
+    // kernel's occupancy), fewer when the network has fewer words
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, neuron, kEngThreads, 0) != cudaSuccess || per_sm < 1)
       per_sm = 4;
     const dim3 grid(unsigned(std::max<int64_t>(
-        1, std::min<int64_t>(int64_t(sms) * per_sm, ceil_div(neuron_items, kEngThreads)))));
+        1, std::min<int64_t>(int64_t(sms) * per_sm, ceil_div(neuron_warps * 32, kEngThreads)))));
     auto pick = [&](auto g) {
       constexpr int G = decltype(g)::value;
       // MS >= ms: mask_stride gives 1, 2, 4, or 5..8 words (MS = 8)
