@@ -33,6 +33,9 @@ class SparseBackendConfig:
     gather_max_nnz_per_step: "auto" without timing data prefers gather when
         nnz is at most this, or when the active fraction is above
         `gather_min_active_fraction`.
+    tile: let the autotuner also try the persistent tile engine (networks
+        without synaptic delays or receptor channels, batches up to 256).
+        Off by default: its push delivery is slow in high-activity bursts.
     """
 
     direction: str = "auto"
@@ -41,6 +44,7 @@ class SparseBackendConfig:
     gather_max_nnz_per_step: int = 1 << 21
     gather_min_active_fraction: float = 0.25
     pull_min_batch: int = 4
+    tile: bool = False
 
     def validate(self) -> None:
         if self.direction not in DIRECTIONS:

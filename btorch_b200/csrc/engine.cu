@@ -254,173 +254,107 @@ __device__ __forceinline__ void publish_spikes(const bt_engine_desc& d, const St
   if (first) ws.list[sub * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = int32_t(i);
 }
 
-// The state of S samples of one neuron, loaded ahead of their update.
-template <int S>
-struct NeuronItem {
-  float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
-  int len[S];
-};
-
-// Issue the loads of samples b0 .. b0+S-1 of neuron i (off0 = b0 * n + i).
-// A sample past its length (k > len) reads no state unless state traces are
-// requested: its state is frozen and its accumulator is not read again.
-template <int KIND, bool USE_REF, int S>
-__device__ __forceinline__ void load_item(NeuronItem<S>& q, bool valid, int b0, int nb, int off0, int n, int k,
-                                          const float* ring, const float* psc, const float* vs, const float* refs,
-                                          const float* gks, const float* xk, const int32_t* slen, bool st_traces,
-                                          uint64_t pol_stream, uint64_t pol_keep) {
-#pragma unroll
-  for (int u = 0; u < S; ++u) q.len[u] = (valid && u < nb && slen) ? slen[b0 + u] : INT_MAX;
-#pragma unroll
-  for (int u = 0; u < S; ++u) {
-    const bool in = valid && u < nb;
-    const bool live = in && k < q.len[u], edge = in && k <= q.len[u], frozen = in && st_traces;
-    const int o = off0 + u * n;
-    q.pend[u] = edge ? ld_f32(ring + o, pol_keep) : 0.0f;
-    q.pv[u] = (edge || frozen) ? psc[o] : 0.0f;
-    q.xv[u] = (live && xk) ? ld_nc_f32(xk + o, pol_stream) : 0.0f;
-    q.vv[u] = (live || frozen) ? vs[o] : 0.0f;
-    q.rv[u] = ((live || frozen) && USE_REF) ? refs[o] : 0.0f;
-    q.gv[u] = ((live || frozen) && KIND == BT_NEURON_ALIF) ? gks[o] : 0.0f;
-  }
-}
-
-// A warp owns a 32-neuron word (lane = neuron) for every sample of the batch:
-// it walks the samples in groups of S (grid-stride over words), each group's
-// loads issued before the previous group's update and stores
-// (software-pipelined; groups touch disjoint state), and builds each neuron's
-// sample mask in registers.  Since no other warp handles these neurons, the
-// step's spike set is published with plain stores of the mask rows and one
-// warp-aggregated list append per word -- no per-neuron atomics, no waiting on
-// their results.  The per-thread set-up (parameters, divisors, pointers,
-// cache policies) is done once.  `ws` is the step's spike set, its pointers
-// computed on the host; indices are 32-bit (batch * n < 2^31 in scatter mode,
-// checked on the host) except into the per-step input and trace arrays.
+// Grid (ceil(n / 256), ceil(batch / S)): a thread owns neuron i for S
+// consecutive samples; a warp covers one 32-neuron bitmap word of each of
+// them.  All S samples' state is loaded before any is updated (memory-level
+// parallelism), and the neuron's parameters are read once for the S samples.
+// `ws` is the step's spike set, its pointers computed on the host; indices
+// are 32-bit (batch * n < 2^31 in scatter mode, checked on the host) except
+// into the per-step input and trace arrays.
 template <int KIND, bool HARD, bool USE_REF, int S, bool FAST>
 __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, int k, StepIdx si, ScatterScratch ws) {
   const int n = int(d.n), B = int(d.batch);
   const int words = (n + 31) >> 5;
-  const int groups = (B + S - 1) / S;
-  const int warps_total = int(gridDim.x) * (kEngThreads / 32);
-  float* __restrict__ ring = d.ring;
-  float* __restrict__ psc = d.psc;
-  float* __restrict__ vs = d.v;
-  float* __restrict__ refs = d.refractory;
-  float* __restrict__ gks = d.g_k;
-  const float* __restrict__ xk = d.x ? d.x + int64_t(k) * B * n : nullptr;
-  const int32_t* __restrict__ slen = d.sample_len;
-  uint32_t* __restrict__ hist = d.hist + int64_t(si.h_t) * B * words;
-  uint32_t* __restrict__ raster = d.raster ? d.raster + int64_t(k) * B * words : nullptr;
+  const int i = int(blockIdx.x) * kEngThreads + int(threadIdx.x);
+  const int b0 = int(blockIdx.y) * S;
+  if ((i & ~31) >= n) return;  // whole warps past the last word
+  const bool valid = i < n;
+  const int nb = B - b0 < S ? B - b0 : S;  // samples of this block (uniform)
+  const int off0 = b0 * n + (valid ? i : 0);
+  float* __restrict__ ring_p = d.ring + off0;  // acc: W z of the previous step
+  float* __restrict__ psc_p = d.psc + off0;
+  float* __restrict__ v_p = d.v + off0;
+  float* __restrict__ ref_p = USE_REF ? d.refractory + off0 : nullptr;
+  float* __restrict__ gk_p = KIND == BT_NEURON_ALIF ? d.g_k + off0 : nullptr;
+  const float* __restrict__ x_p = d.x ? d.x + int64_t(k) * B * n + off0 : nullptr;
   const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
+  // Every load before the first store: a load behind a store through a
+  // pointer that may alias it waits for the store.  A sample past its length
+  // (k > len) reads and writes no state unless state traces are requested:
+  // its state is frozen and its accumulator is not read again in this call.
   const bool traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace || d.spikes;
   const bool st_traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace;
-  const unsigned lane = lane_id();
-  const NeuronParams prm_u = load_params<KIND, USE_REF>(d.neuron, 0);
-  const float pc_u = d.psc_uniform ? d.psc_coef_s : 0.0f;
-  const Div dpt_u = make_div(d.psc_uniform ? d.psc_tau_s : 1.0f, d.psc_uniform && d.psc_fast_div, d.psc_rcp);
-  for (int w = int(blockIdx.x) * (kEngThreads / 32) + int(threadIdx.x >> 5); w < words; w += warps_total) {
-    const int i = w * 32 + int(lane);
-    const bool valid = i < n;
-    const int ip = valid ? i : 0;
-    NeuronParams prm = prm_u;
-    float pc = pc_u;
-    Div dpt = dpt_u;
-    if (!d.neuron.uniform) prm = load_params<KIND, USE_REF>(d.neuron, ip);
-    if (!d.psc_uniform) {
-      pc = ld(d.psc_coef, ip);
-      dpt = make_div(ld(d.psc_tau, ip), false, 0.0f);
-    }
-    // the neuron's sample mask (batch <= 256), a row of 32-sample words per
-    // lane in shared memory (each lane owns its own)
-    __shared__ uint32_t s_m[kEngThreads / 32][8][32];
-    uint32_t(*m)[32] = s_m[threadIdx.x >> 5];
+  float pend[S], pv[S], xv[S], vv[S], rv[S], gv[S];
+  int lenv[S];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) m[q][lane] = 0u;
-    int nspk = 0;
-    NeuronItem<S> cur;
-    load_item<KIND, USE_REF, S>(cur, valid, 0, B < S ? B : S, ip, n, k, ring, psc, vs, refs, gks, xk, slen,
-                                st_traces, pol_stream, pol_keep);
-    for (int g = 0; g < groups; ++g) {
-      const int b0 = g * S;
-      const int nb = B - b0 < S ? B - b0 : S;  // uniform across the warp
-      NeuronItem<S> nxt;
-      if (g + 1 < groups) {
-        const int b1 = b0 + S;
-        load_item<KIND, USE_REF, S>(nxt, valid, b1, B - b1 < S ? B - b1 : S, b1 * n + ip, n, k, ring, psc, vs, refs,
-                                    gks, xk, slen, st_traces, pol_stream, pol_keep);
-      }
-      const int off0 = b0 * n + ip;
+  for (int u = 0; u < S; ++u) lenv[u] = (valid && u < nb && d.sample_len) ? d.sample_len[b0 + u] : INT_MAX;
 #pragma unroll
-      for (int u = 0; u < S; ++u) {
-        if (u >= nb) break;  // uniform across the warp
-        const int o = off0 + u * n;
-        float s = 0.0f;
-        if (valid) {
-          const int len = cur.len[u];
-          if (k <= len) st_f32(ring + o, 0.0f, pol_keep);
-          float v = cur.vv[u], ref = cur.rv[u], gk = cur.gv[u];
-          float P;
-          if (k < len) {
-            P = add(cur.pv[u], cur.pend[u]);
-            const float I = xk ? add(P, cur.xv[u]) : P;
-            s = neuron_update<KIND, HARD, USE_REF, true, FAST>(prm, I, v, ref, gk).spike;
-            vs[o] = v;
-            if (USE_REF) refs[o] = ref;
-            if (KIND == BT_NEURON_ALIF) gks[o] = gk;
-            psc[o] = psc_decay_k<FAST>(pc, dpt, P);
-          } else {
-            // Finished sample: its state freezes at its last step.  On the
-            // first step past the end the pending sum completes psc of that
-            // last step; later arrivals are dropped.
-            P = cur.pv[u];
-            if (k == len) {
-              P = add(P, cur.pend[u]);
-              psc[o] = P;
-            }
-          }
-          if (traces) {
-            const int64_t tix = (int64_t(k) * B + b0 + u) * n + i;
-            if (d.psc_trace && k > 0) d.psc_trace[tix - int64_t(B) * n] = P;
-            if (d.v_trace) d.v_trace[tix] = v;
-            if (USE_REF && d.ref_trace) d.ref_trace[tix] = ref;
-            if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[tix] = gk;
-            if (d.spikes) d.spikes[tix] = s;
-          }
-        }
-        const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
-        if (lane == 0) {
-          const int wi = (b0 + u) * words + w;
-          hist[wi] = word;
-          if (raster) raster[wi] = word;
-        }
-        if (s != 0.0f) {
-          const int b = b0 + u;
-          m[b >> 5][lane] |= 1u << (b & 31);
-          ++nspk;
-        }
-      }
-      if (g + 1 < groups) cur = nxt;
-    }
-    // publish the word's spikes: the mask rows (plain stores: this warp is the
-    // only writer of these neurons' rows, cleared by their last reader), the
-    // spike total and one list append per word
-    const bool any = nspk != 0;
-    const uint32_t fb = __ballot_sync(0xffffffffu, any);
-    if (fb == 0) continue;  // warp-uniform
-    if (any) {
-      uint32_t* mrow = ws.mask + int64_t(i) * ws.ms;
-      for (int q = 0; q < ws.ms; ++q) mrow[q] = m[q][lane];
-    }
-    const int sub = (w * 32) >> ws.cap_shift;  // cap % 32 == 0: one sub-list per word
-    const int tot = __reduce_add_sync(0xffffffffu, unsigned(nspk));
-    int32_t base = 0;
-    if (lane == 0) {
-      atomicAdd(ws.spk + sub, tot);
-      base = atomicAdd(ws.count + sub, __popc(fb));
-    }
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (any) ws.list[int64_t(sub) * ws.cap + base + __popc(fb & ((1u << lane) - 1u))] = i;
+  for (int u = 0; u < S; ++u) {
+    const bool in = valid && u < nb;
+    const bool live = in && k < lenv[u], edge = in && k <= lenv[u], frozen = in && st_traces;
+    const int o = u * n;
+    pend[u] = edge ? ld_f32(ring_p + o, pol_keep) : 0.0f;
+    pv[u] = (edge || frozen) ? psc_p[o] : 0.0f;
+    xv[u] = (live && x_p) ? ld_nc_f32(x_p + o, pol_stream) : 0.0f;
+    vv[u] = (live || frozen) ? v_p[o] : 0.0f;
+    rv[u] = ((live || frozen) && USE_REF) ? ref_p[o] : 0.0f;
+    gv[u] = ((live || frozen) && KIND == BT_NEURON_ALIF) ? gk_p[o] : 0.0f;
   }
+  const int ip = valid ? i : 0;
+  const NeuronParams prm = load_params<KIND, USE_REF>(d.neuron, ip);
+  const float pc = d.psc_uniform ? d.psc_coef_s : ld(d.psc_coef, ip);
+  const float pt = d.psc_uniform ? d.psc_tau_s : ld(d.psc_tau, ip);
+  const Div dpt = make_div(pt, d.psc_uniform && d.psc_fast_div, d.psc_rcp);
+  const unsigned lane = lane_id();
+  uint32_t* hist_p = d.hist + (int64_t(si.h_t) * B + b0) * words + (i >> 5);
+  uint32_t* raster_p = d.raster ? d.raster + (int64_t(k) * B + b0) * words + (i >> 5) : nullptr;
+  uint32_t spiked = 0;  // bit u: spiked in sample b0 + u
+#pragma unroll
+  for (int u = 0; u < S; ++u) {
+    if (u >= nb) break;  // uniform across the block
+    const int o = u * n;
+    float s = 0.0f;
+    if (valid) {
+      const int len = lenv[u];
+      if (k <= len) st_f32(ring_p + o, 0.0f, pol_keep);
+      float v = vv[u], ref = rv[u], gk = gv[u];
+      float P;
+      if (k < len) {
+        P = add(pv[u], pend[u]);
+        const float I = x_p ? add(P, xv[u]) : P;
+        const NeuronOut out = neuron_update<KIND, HARD, USE_REF, true, FAST>(prm, I, v, ref, gk);
+        s = out.spike;
+        v_p[o] = v;
+        if (USE_REF) ref_p[o] = ref;
+        if (KIND == BT_NEURON_ALIF) gk_p[o] = gk;
+        psc_p[o] = psc_decay_k<FAST>(pc, dpt, P);
+      } else {
+        // Finished sample: its state freezes at its last step.  On the first
+        // step past the end the pending sum completes psc of that last step;
+        // later arrivals are dropped.
+        P = pv[u];
+        if (k == len) {
+          P = add(P, pend[u]);
+          psc_p[o] = P;
+        }
+      }
+      if (traces) {
+        const int64_t tix = (int64_t(k) * B + b0 + u) * n + i;
+        if (d.psc_trace && k > 0) d.psc_trace[tix - int64_t(B) * n] = P;
+        if (d.v_trace) d.v_trace[tix] = v;
+        if (USE_REF && d.ref_trace) d.ref_trace[tix] = ref;
+        if (KIND == BT_NEURON_ALIF && d.gk_trace) d.gk_trace[tix] = gk;
+        if (d.spikes) d.spikes[tix] = s;
+      }
+    }
+    const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
+    if (lane == 0) {
+      hist_p[u * words] = word;
+      if (raster_p) raster_p[u * words] = word;
+    }
+    if (s != 0.0f) spiked |= 1u << u;
+  }
+  publish_spikes_ws(ws, i, b0, spiked);
 }
 
 // SCATTER neuron step with receptor channels (n_rec = C > 1): for each
@@ -1607,10 +1541,10 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
   }
   if (d.mode == BT_MODE_SCATTER) {
     const int S = d.neuron_spt > 0 ? d.neuron_spt : 4;
+    const dim3 grid(unsigned(ceil_div(n, kEngThreads)), unsigned(ceil_div(d.batch, S)));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t neuron_warps = (n + 31) >> 5;  // a warp per 32-neuron word, all samples
     const unsigned planes = unsigned(d.bin_hi - d.bin_lo + 1);
     // a plane lists at most n rows: no more blocks than n rows need (small
     // networks would otherwise launch mostly idle blocks every step)
@@ -1625,13 +1559,6 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
                           : S == 2 ? k_eng_neuron<KIND, HARD, USE_REF, 2, true> : k_eng_neuron<KIND, HARD, USE_REF, 4, true>)
                        : (S == 1 ? k_eng_neuron<KIND, HARD, USE_REF, 1, false>
                           : S == 2 ? k_eng_neuron<KIND, HARD, USE_REF, 2, false> : k_eng_neuron<KIND, HARD, USE_REF, 4, false>);
-    // grid-stride neuron launch: as many blocks as are resident at once (the
-    // kernel's occupancy), fewer when the network has fewer words
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, neuron, kEngThreads, 0) != cudaSuccess || per_sm < 1)
-      per_sm = 4;
-    const dim3 grid(unsigned(std::max<int64_t>(
-        1, std::min<int64_t>(int64_t(sms) * per_sm, ceil_div(neuron_warps * 32, kEngThreads)))));
     auto pick = [&](auto g) {
       constexpr int G = decltype(g)::value;
       // MS >= ms: mask_stride gives 1, 2, 4, or 5..8 words (MS = 8)

@@ -58,9 +58,13 @@ def allowed_modes(conn, batch: int, receptors: int = 1, n_bins: int = 1) -> list
     if cfg.deterministic or cfg.direction == "gather":
         modes = [L.BT_MODE_GATHER, L.BT_MODE_PULL]
     elif cfg.direction == "scatter":
-        modes = [L.BT_MODE_SCATTER, L.BT_MODE_TILE]
+        modes = [L.BT_MODE_SCATTER]
     else:
-        modes = [L.BT_MODE_SCATTER, L.BT_MODE_TILE, L.BT_MODE_PULL, L.BT_MODE_GATHER]
+        modes = [L.BT_MODE_SCATTER, L.BT_MODE_PULL, L.BT_MODE_GATHER]
+    if cfg.tile and cfg.direction != "gather" and not cfg.deterministic:
+        # the persistent tile engine: opt-in -- its push delivery is slow in a
+        # start-up burst, which the tuner's trial window (after a warm-up) misses
+        modes.insert(1, L.BT_MODE_TILE)
     modes = [m for m in modes if receptors == 1 or m != L.BT_MODE_PULL]
     if receptors > 1 or n_bins > 1 or batch > 256:
         modes = [m for m in modes if m != L.BT_MODE_TILE]

@@ -323,3 +323,21 @@ def test_product_package_never_reaches_the_oracle():
     out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr[-2000:]
     assert out.stdout.strip().splitlines()[-1] == "False"
+
+
+def test_tile_mode_is_an_opt_in_candidate():
+    """The persistent tile engine is a tuner candidate only when the sparse
+    config asks for it, for networks without delays or receptor channels, in
+    a push direction and batches up to 256."""
+    from btorch_b200.models import autotune
+
+    conn = SparseConn(sp.random(64, 64, density=0.1, random_state=0, format="coo", dtype=np.float32),
+                      sparse_config={"direction": "scatter"})
+    assert L.BT_MODE_TILE not in autotune.allowed_modes(conn, 8)
+    conn.sparse_config.tile = True
+    assert L.BT_MODE_TILE in autotune.allowed_modes(conn, 8)
+    assert L.BT_MODE_TILE not in autotune.allowed_modes(conn, 8, n_bins=3)
+    assert L.BT_MODE_TILE not in autotune.allowed_modes(conn, 8, receptors=2)
+    assert L.BT_MODE_TILE not in autotune.allowed_modes(conn, 300)
+    conn.sparse_config.direction = "gather"
+    assert L.BT_MODE_TILE not in autotune.allowed_modes(conn, 8)
