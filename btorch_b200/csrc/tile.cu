@@ -427,28 +427,42 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile_engine(bt_engine_desc 
         }
         const int excl = incl - cntg[g];
         const int tot = __shfl_sync(0xffffffffu, incl, 31);
-        for (int f0 = 0; f0 < tot; f0 += 32) {
-          const int f = f0 + lane;
-          int r = 0;  // the last lane whose excl <= f
+        // EU passes of 32 edges per iteration: every edge load of the
+        // iteration is issued before its additions (memory-level parallelism)
+        constexpr int EU = 4;
+        for (int f0 = 0; f0 < tot; f0 += 32 * EU) {
+          uint2 rec2[EU];
+          uint32_t mm[EU][MS];
 #pragma unroll
-          for (int step = 16; step > 0; step >>= 1) {
-            const int x = __shfl_sync(0xffffffffu, excl, r + step);
-            if (x <= f) r += step;
+          for (int uu = 0; uu < EU; ++uu) {
+            const int f = f0 + uu * 32 + lane;
+            int r = 0;  // the last lane whose excl <= f
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+              const int x = __shfl_sync(0xffffffffu, excl, r + step);
+              if (x <= f) r += step;
+            }
+            const int eb = __shfl_sync(0xffffffffu, e0[g], r) + (f - __shfl_sync(0xffffffffu, excl, r));
+#pragma unroll
+            for (int q = 0; q < MS; ++q) mm[uu][q] = __shfl_sync(0xffffffffu, mk[g][q], r);
+            if (f < tot) {
+              rec2[uu] = ld_nc_u2(d.csr_edges + 2 * int64_t(eb), pol_stream);
+            } else {
+              rec2[uu] = make_uint2(0u, 0u);
+#pragma unroll
+              for (int q = 0; q < MS; ++q) mm[uu][q] = 0u;
+            }
           }
-          const int eb = __shfl_sync(0xffffffffu, e0[g], r) + (f - __shfl_sync(0xffffffffu, excl, r));
-          uint32_t m[MS];
 #pragma unroll
-          for (int q = 0; q < MS; ++q) m[q] = __shfl_sync(0xffffffffu, mk[g][q], r);
-          if (f < tot) {
-            const uint2 rec2 = ld_nc_u2(d.csr_edges + 2 * int64_t(eb), pol_stream);
-            const int lp = int((rec2.x & kIdMask) - uint32_t(p0));
-            const float wv = __uint_as_float(rec2.y);
+          for (int uu = 0; uu < EU; ++uu) {
+            const int lp = int((rec2[uu].x & kIdMask) - uint32_t(p0));
+            const float wv = __uint_as_float(rec2[uu].y);
 #pragma unroll
             for (int q = 0; q < MS; ++q) {
-              uint32_t mm = q < ms ? m[q] : 0u;
-              while (mm) {
-                const int bit = __ffs(mm) - 1;
-                mm &= mm - 1;
+              uint32_t bits = q < ms ? mm[uu][q] : 0u;
+              while (bits) {
+                const int bit = __ffs(bits) - 1;
+                bits &= bits - 1;
                 atomicAdd(s_acc + (q * 32 + bit) * Tp + lp, wv);
               }
             }
