@@ -239,7 +239,14 @@ def measure_training(cfg, args, dev):
                         unroll=cfg["unroll"]).to(dev)
     readout = torch.nn.Linear(n, cfg["n_out"]).to(dev)
     opt = torch.optim.Adam(list(brain.parameters()) + list(readout.parameters()), lr=cfg["lr"])
-    g = torch.Generator(device=dev).manual_seed(20_000 + args.seed)
+    import torch.distributed as dist
+
+    from btorch_b200.replicas import allreduce_gradients
+
+    world = dist.get_world_size() if dist.is_initialized() else 1
+    rank = dist.get_rank() if dist.is_initialized() else 0
+    params = list(brain.parameters()) + list(readout.parameters())
+    g = torch.Generator(device=dev).manual_seed(20_000 + args.seed + rank)  # each replica its own samples
     x = torch.poisson(torch.full((cfg["t_max"], B, cfg["c_in"]), cfg["in_rate"], device=dev), generator=g)
     target = torch.from_numpy(net["target"]).to(dev)
     outdeg = torch.bincount(torch.from_numpy(net["pre"]), minlength=n).to(dev, torch.float64)
@@ -255,6 +262,8 @@ def measure_training(cfg, args, dev):
             loss = ((readout(z) - target[sl]) ** 2).mean()
             opt.zero_grad(set_to_none=True)
             loss.backward()
+            # data parallel over replicas: one all-reduce of every gradient
+            allreduce_gradients(params)
             opt.step()
         detach_net(brain)
         if events is not None:
@@ -275,9 +284,13 @@ def measure_training(cfg, args, dev):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     ev = float(torch.stack(events).sum())
+    if world > 1:
+        ms, ev = job_totals(ms, ev, dev)
     return {"value": ev / (ms * 1e-3), "unit": "forward synaptic events/s of training time",
+            "replicas": world, "gradient_allreduce_bytes_per_step": 4 * sum(p.numel() for p in params)
+            if world > 1 else 0,
             "ms_per_window": ms / steps, "windows": steps, "window_steps": Wn,
-            "neuron_steps_per_s": n * B * Wn * steps / (ms * 1e-3),
+            "neuron_steps_per_s": n * B * Wn * steps * world / (ms * 1e-3),
             "loss_first_last": [float(losses[0]), float(losses[-1])], "direction": conn.direction(B),
             "path": brain.last_path, "bptt": getattr(brain, "last_bptt", None),
             "config": {"workload": f"training: LIF+ExpPSC N={n} p={cfg['p']} ({len(net['w'])} trainable weights) "
@@ -292,8 +305,15 @@ def measure_serving(cfg, args, dev):
     each size, plus a dense input layer of c_in channels with half-normal
     weights).  Each request drives a random number of channels at its own
     rate for its own number of steps; stimuli are synthesised on the device
-    before the run (they stand in for client uploads).  Returns p50/p99
-    latency (arrival to completion) and aggregate synaptic events/s."""
+    before the run (they stand in for client uploads).
+
+    Three load points: the configured arrival rate (200 req/s, above what the
+    server sustains: its latency is mostly queueing), then the server's
+    capacity measured there (requests completed per second) and the same
+    request mix offered at 50 % and 90 % of it.  Each reports p50/p99 latency
+    (arrival to completion) and wait (arrival to admission), the latter also
+    in ticks of the slowest network (one tick = `chunk` steps of all its
+    slots, timed alone with every slot busy)."""
     from btorch_b200.models import DenseConn
     from btorch_b200.serving import NetworkPool, SimRequest, SimulationServer
 
@@ -309,40 +329,74 @@ def measure_serving(cfg, args, dev):
         pools[f"n{n}"] = NetworkPool(f"n{n}", rnn, slots=cfg["slots"], chunk=cfg["chunk"], device=dev)
     names = list(pools)
     g = torch.Generator(device=dev).manual_seed(40_000 + args.seed)
-    t = 0.0
-    reqs = []
+    mix = []  # (gap in units of the mean inter-arrival time, network, stimulus)
     for i in range(cfg["n_requests"]):
-        t += rng.exponential(1.0 / cfg["rate_hz"])
+        gap = rng.exponential(1.0)
         T = int(rng.integers(cfg["steps"][0], cfg["steps"][1] + 1))
         c = int(rng.integers(cfg["channels"][0], cfg["channels"][1] + 1))
         hz = float(rng.uniform(*cfg["stim_hz"]))
         stim = torch.zeros((T, cfg["c_in"]), device=dev)
         stim[:, :c] = torch.poisson(torch.full((T, c), hz * 1e-3, device=dev), generator=g)
-        reqs.append(SimRequest(network=names[int(rng.integers(len(names)))], stimulus=stim, arrival=t, rid=i))
-    # warm-up: one tick per pool (graph capture) outside the measured run
+        mix.append((gap, names[int(rng.integers(len(names)))], stim))
+
+    def requests(rate):
+        t, out = 0.0, []
+        for i, (gap, name, stim) in enumerate(mix):
+            t += gap / rate
+            out.append(SimRequest(network=name, stimulus=stim, arrival=t, rid=i))
+        return out
+
+    # warm-up: one tick per pool (graph capture) outside the measured runs,
+    # then each pool's tick time alone with every slot busy
     warm = [SimRequest(network=nm, stimulus=torch.zeros((p.chunk, cfg["c_in"]), device=dev), rid=-1 - j)
             for j, (nm, p) in enumerate(pools.items())]
     SimulationServer(pools, hbm_budget_bytes=int(cfg["budget_gb"] * 2**30)).run(warm)
-    for p in pools.values():
-        p.drain_events()
-        p.events = 0
-        p.ticks = 0
-    server = SimulationServer(pools, hbm_budget_bytes=int(cfg["budget_gb"] * 2**30))
-    rep = server.run(reqs)
-    out = rep.summary()
-    lat = np.array([r.latency for r in rep.requests]) * 1e3
-    wait = np.array([r.t_admit - r.arrival for r in rep.requests]) * 1e3
-    steps = sum(r.steps for r in rep.requests)
-    out.update({"unit": "ms (latency), events/s", "mean_latency_ms": float(lat.mean()),
-                "p50_wait_ms": float(np.percentile(wait, 50)), "p99_wait_ms": float(np.percentile(wait, 99)),
-                "sample_steps_per_s": steps / rep.wall_s, "offered_rate_req_per_s": cfg["rate_hz"],
+    tick_ms = {}
+    for nm, p in pools.items():
+        full = [SimRequest(network=nm, stimulus=torch.zeros((p.chunk * 3, cfg["c_in"]), device=dev), rid=-100 - s)
+                for s in range(p.slots)]
+        t0 = time.perf_counter()
+        SimulationServer({nm: p}, hbm_budget_bytes=int(cfg["budget_gb"] * 2**30)).run(full)
+        tick_ms[nm] = (time.perf_counter() - t0) * 1e3 / 3
+    tick = max(tick_ms.values())
+
+    def serve(rate):
+        for p in pools.values():
+            p.drain_events()
+            p.events = 0
+            p.ticks = 0
+        server = SimulationServer(pools, hbm_budget_bytes=int(cfg["budget_gb"] * 2**30))
+        rep = server.run(requests(rate))
+        out = rep.summary()
+        lat = np.array([r.latency for r in rep.requests]) * 1e3
+        wait = np.array([r.t_admit - r.arrival for r in rep.requests]) * 1e3
+        steps = sum(r.steps for r in rep.requests)
+        out.update({"offered_rate_req_per_s": rate, "completed_req_per_s": len(rep.requests) / rep.wall_s,
+                    "mean_latency_ms": float(lat.mean()), "p50_wait_ms": float(np.percentile(wait, 50)),
+                    "p99_wait_ms": float(np.percentile(wait, 99)),
+                    "p99_wait_ticks": float(np.percentile(wait, 99)) / tick,
+                    "sample_steps_per_s": steps / rep.wall_s})
+        return out
+
+    out = serve(cfg["rate_hz"])
+    capacity = out["completed_req_per_s"]
+    out["load_points"] = {"saturated": {k: out[k] for k in ("offered_rate_req_per_s", "completed_req_per_s", "p50_ms",
+                                                             "p99_ms", "p50_wait_ms", "p99_wait_ms",
+                                                             "p99_wait_ticks")}}
+    for frac in (0.5, 0.9):
+        r = serve(frac * capacity)
+        out["load_points"][f"{int(frac * 100)}pct_of_capacity"] = {
+            k: r[k] for k in ("offered_rate_req_per_s", "completed_req_per_s", "p50_ms", "p99_ms", "p50_wait_ms",
+                              "p99_wait_ms", "p99_wait_ticks", "events_per_s")}
+    out.update({"unit": "ms (latency), events/s", "capacity_req_per_s": capacity, "tick_ms_alone": tick_ms,
                 "direction": args.direction,
                 "config": {"workload": f"serving: {cfg['n_requests']} requests, Poisson arrivals "
-                                       f"{cfg['rate_hz']} req/s over networks N={list(cfg['sizes'])} "
-                                       f"(connectome-shaped, delays 1..{cfg['n_bins']}), {cfg['slots']} slots "
-                                       f"each, ticks of {[p.chunk for p in pools.values()]} steps, stimulus "
-                                       f"{cfg['channels']} channels at {cfg['stim_hz']} Hz for {cfg['steps']} "
-                                       f"steps, HBM budget {cfg['budget_gb']} GiB"}})
+                                       f"{cfg['rate_hz']} req/s (and 50 %, 90 % of the measured capacity) over "
+                                       f"networks N={list(cfg['sizes'])} (connectome-shaped, delays "
+                                       f"1..{cfg['n_bins']}), {cfg['slots']} slots each, ticks of "
+                                       f"{[p.chunk for p in pools.values()]} steps, stimulus {cfg['channels']} "
+                                       f"channels at {cfg['stim_hz']} Hz for {cfg['steps']} steps, HBM budget "
+                                       f"{cfg['budget_gb']} GiB"}})
     return out
 
 

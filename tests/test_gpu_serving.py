@@ -52,3 +52,28 @@ def test_served_results_equal_alone(direction):
         np.testing.assert_array_equal(r.raster.cpu().numpy(), want, err_msg=f"request {r.rid}")
     s = rep.summary()
     assert s["p50_ms"] <= s["p99_ms"] and s["events_per_s"] > 0
+
+
+@pytest.mark.parametrize("limit", ["budget", "slots"])
+def test_admission_holds_a_request_until_budget_or_slot_frees(limit):
+    """Two requests arrive together.  Either the HBM budget fits only one of
+    them (two slots free) or the network has one slot: the second waits in
+    the queue until the first has retired, then runs, and each raster equals
+    the request run alone."""
+    d = cases.load("lif_dyadic_input")
+    slots = 2 if limit == "budget" else 1
+    rnn, _ = cases.build_model(dict(d, batch=np.int64(slots)), DEV, "scatter")
+    rnn.update_state_names = ()
+    pool = NetworkPool("inp", rnn, slots=slots, chunk=16, device=DEV, cudagraph=True)
+    stims = [torch.tensor(d["x"][:100, 0]), torch.tensor(d["x"][10:90, 1])]
+    reqs = [SimRequest(network="inp", stimulus=s.clone(), arrival=0.0, rid=i) for i, s in enumerate(stims)]
+    need = max(pool.request_bytes(r) for r in reqs)
+    budget = need if limit == "budget" else 10 * need
+    rep = SimulationServer({"inp": pool}, hbm_budget_bytes=budget).run(reqs)
+    done = {r.rid: r for r in rep.requests}
+    assert sorted(done) == [0, 1]
+    first, second = sorted(done.values(), key=lambda r: r.t_admit)
+    assert second.t_admit >= first.t_done  # held back until the first one retired
+    for r in rep.requests:
+        np.testing.assert_array_equal(r.raster.cpu().numpy(), alone(d, "scatter", stims[r.rid]),
+                                      err_msg=f"request {r.rid}")
