@@ -41,7 +41,6 @@
 // the receptor sum of its C channels (receptor_sum, the reference's
 // psc.reshape(..., n, C).sum(-1) rounding).  Scatter and gather modes.
 #include <algorithm>
-#include <mutex>
 #include <climits>
 #include <cstring>
 #include <type_traits>
@@ -125,12 +124,9 @@ __host__ __device__ __forceinline__ int mask_stride(int64_t batch) {
 // Slot indices of one step, computed on the host per launch so that no kernel
 // evaluates a 64-bit modulo per element.
 struct StepIdx {
-  int q_t;       // t mod (R + 1): spike-set slot of step t (scatter)
-  int h_t;       // t mod H:       history slot written at step t
-  int h_prev;    // (t - 1) mod H: history slot of step t - 1
-  int acc;       // scatter: accumulator slot the neuron launch of step t reads and clears
-  int acc_next;  // scatter: accumulator slot the scatter of step t adds into
-  int bin_last;  // scatter: the delay bin whose reader clears a spike set
+  int q_t;     // t mod (R + 1): spike-set slot of step t (scatter)
+  int h_t;     // t mod H:       history slot written at step t
+  int h_prev;  // (t - 1) mod H: history slot of step t - 1
 };
 
 inline StepIdx step_idx(int64_t t, int R, int H) {
@@ -138,20 +134,6 @@ inline StepIdx step_idx(int64_t t, int R, int H) {
   s.q_t = int(t % (R + 1));
   s.h_t = int(t % H);
   s.h_prev = int((t - 1) % H);
-  s.acc = s.acc_next = 0;
-  s.bin_last = R - 1;
-  return s;
-}
-
-// Accumulator slots: one, or two alternating by step parity when the scatter
-// of a step runs beside the next step's neuron launch (overlapped delays).
-inline StepIdx scatter_step_idx(const bt_engine_desc& d, int64_t t) {
-  StepIdx s = step_idx(t, d.n_bins, d.hist_len);
-  if (d.ring_slots == 2) {
-    s.acc = int(t & 1);
-    s.acc_next = int((t + 1) & 1);
-  }
-  s.bin_last = d.bin_hi;
   return s;
 }
 
@@ -289,7 +271,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron(bt_engine_desc d, in
   const bool valid = i < n;
   const int nb = B - b0 < S ? B - b0 : S;  // samples of this block (uniform)
   const int off0 = b0 * n + (valid ? i : 0);
-  float* __restrict__ ring_p = d.ring + int64_t(si.acc) * B * n + off0;  // acc: W z of the previous step
+  float* __restrict__ ring_p = d.ring + off0;  // acc: W z of the previous step
   float* __restrict__ psc_p = d.psc + off0;
   float* __restrict__ v_p = d.v + off0;
   float* __restrict__ ref_p = USE_REF ? d.refractory + off0 : nullptr;
@@ -398,7 +380,7 @@ __global__ void __launch_bounds__(kEngThreads) k_eng_neuron_rec(bt_engine_desc d
   const bool st_traces = d.v_trace || d.psc_trace || d.ref_trace || d.gk_trace;
   if (i < n && (k <= len || st_traces)) {  // else: past its length, nothing to read or write
     const int64_t idx = b * n + i, c0 = b * nc + i * C;
-    float* __restrict__ ring = d.ring + int64_t(si.acc) * B * nc + c0;
+    float* __restrict__ ring = d.ring + c0;
     float* __restrict__ psc = d.psc + c0;
     // loads
     float pend[M], stv[M], pc[M], pt[M];
@@ -568,7 +550,7 @@ __device__ __forceinline__ void block_stats(const bt_engine_desc& d, int64_t k, 
 // set's masks and flags are then cleared by the last block to finish
 // (block-completion counter in ctrl[0]; no block waits for another).
 template <int MS>
-__device__ void scatter_dense(const bt_engine_desc& d, int64_t k, const ScatterScratch& ws, float* accb, long long& ev,
+__device__ void scatter_dense(const bt_engine_desc& d, int64_t k, const ScatterScratch& ws, long long& ev,
                               long long& ed) {
   constexpr int W = kEngThreads / 32;
   __shared__ float s_acc[W][32][32];
@@ -626,7 +608,7 @@ __device__ void scatter_dense(const bt_engine_desc& d, int64_t k, const ScatterS
 #pragma unroll
         for (int v = 0; v < W; ++v) sum = add(sum, s_acc[v][l][ln]);
         const int64_t b = int64_t(w) * 32 + l, p = sl * 32 + ln;
-        if (b < B && p < nc && sum != 0.0f) accb[b * n32 + p] = sum;
+        if (b < B && p < nc && sum != 0.0f) d.ring[b * n32 + p] = sum;
       }
       __syncthreads();
     }
@@ -680,17 +662,16 @@ __global__ void __launch_bounds__(kEngThreads, MS <= 4 ? 4 : 3) k_eng_scatter(bt
   // dense when most neurons spike and they do so in several samples each
   if (d.dense_rows > 0 && count >= d.dense_rows && s_spk >= kDenseSpikesPerRow * count) {  // grid-uniform
     long long ev = 0, ed = 0;
-    scatter_dense<MS>(d, k, ws, d.ring + int64_t(si.acc_next) * d.batch * (d.n * n_rec(d)), ev, ed);
+    scatter_dense<MS>(d, k, ws, ev, ed);
     if (d.stats) block_stats(d, k, ev, ed);
     return;
   }
-  const bool last_use = bin == si.bin_last;  // this set is not read again: clear it
+  const bool last_use = bin == d.bin_hi;  // this set is not read again: clear it
   const unsigned lane = lane_id();
   const int grp = int(lane) / G, lig = int(lane) % G;
   constexpr int kPerWarp = 32 / G;
   const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   const int n32 = int(n * n_rec(d));  // acc row stride; batch * n * C < 2^31 (checked on the host)
-  float* __restrict__ accb = d.ring + int64_t(si.acc_next) * d.batch * n32;
   const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
   long long ev = 0, ed = 0;
   for (int64_t base = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kPerWarp; base < count;
@@ -760,7 +741,7 @@ __global__ void __launch_bounds__(kEngThreads, MS <= 4 ? 4 : 3) k_eng_scatter(bt
           while (m) {
             const int l = __ffs(m) - 1;
             m &= m - 1;
-            float* row = accb + (w * 32 + l) * n32;
+            float* row = d.ring + (w * 32 + l) * n32;
             if (v0) red_add_f32(row + p0, __uint_as_float(wq[u].x), pol_keep);
             if (v1) red_add_f32(row + p1, __uint_as_float(wq[u].y), pol_keep);
             if (v2) red_add_f32(row + p2, __uint_as_float(wq[u].z), pol_keep);
@@ -801,15 +782,14 @@ __global__ void __launch_bounds__(kEngThreads, MS <= 4 ? 4 : 3) k_eng_scatter_fl
   // dense when most neurons spike and they do so in several samples each
   if (d.dense_rows > 0 && count >= d.dense_rows && s_spk >= kDenseSpikesPerRow * count) {  // grid-uniform
     long long ev = 0, ed = 0;
-    scatter_dense<MS>(d, k, ws, d.ring + int64_t(si.acc_next) * d.batch * (d.n * n_rec(d)), ev, ed);
+    scatter_dense<MS>(d, k, ws, ev, ed);
     if (d.stats) block_stats(d, k, ev, ed);
     return;
   }
-  const bool last_use = bin == si.bin_last;
+  const bool last_use = bin == d.bin_hi;
   const int lane = int(lane_id());
   const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   const int n32 = int(d.n * n_rec(d));  // acc row stride; batch * n * C < 2^31 (checked on the host)
-  float* __restrict__ accb = d.ring + int64_t(si.acc_next) * d.batch * n32;
   const uint64_t pol_stream = l2_evict_first(), pol_keep = l2_evict_last();
   long long ev = 0, ed = 0;
   for (int64_t base = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * 32; base < count;
@@ -892,7 +872,7 @@ __global__ void __launch_bounds__(kEngThreads, MS <= 4 ? 4 : 3) k_eng_scatter_fl
           while (m) {
             const int l = __ffs(m) - 1;
             m &= m - 1;
-            red_add_f32(accb + (w * 32 + l) * n32 + pp[u], wv[u], pol_keep);
+            red_add_f32(d.ring + (w * 32 + l) * n32 + pp[u], wv[u], pol_keep);
           }
         }
       }
@@ -901,13 +881,13 @@ __global__ void __launch_bounds__(kEngThreads, MS <= 4 ? 4 : 3) k_eng_scatter_fl
   if (d.stats) block_stats(d, k, ev, ed);
 }
 
-// psc_{t_end-1} = stored + acc (accumulator slot `slot`); clears acc.
-__global__ void k_eng_scatter_final(bt_engine_desc d, int slot) {
+// psc_{t_end-1} = stored + acc; clears acc.
+__global__ void k_eng_scatter_final(bt_engine_desc d) {
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t nc = d.n * n_rec(d), B = d.batch;  // one thread per PSC column
   if (idx >= B * nc) return;
   // all loads before the first store (see k_eng_neuron_rec)
-  float* __restrict__ ring = d.ring + int64_t(slot) * B * nc;
+  float* __restrict__ ring = d.ring;
   float* __restrict__ psc = d.psc;
   const float pending = ring[idx];
   const float stored = psc[idx];
@@ -1497,9 +1477,6 @@ int engine_check(const bt_engine_desc* d) {
   BT_CHECK_ARG(d->n_rec >= 0 && d->n_rec <= kMaxRec, "n_rec=%d outside [0, %d]", d->n_rec, kMaxRec);
   BT_CHECK_ARG(d->n * n_rec(*d) < BT_MAX_NEURONS, "n * n_rec must be < 2^25");
   BT_CHECK_ARG(n_rec(*d) == 1 || d->mode != BT_MODE_PULL, "pull mode has no receptor channels");
-  BT_CHECK_ARG(d->ring_slots >= 0 && d->ring_slots <= 2, "ring_slots=%d (0, 1 or 2)", d->ring_slots);
-  BT_CHECK_ARG(d->ring_slots != 2 || (d->mode == BT_MODE_SCATTER && d->bin_hi >= 1),
-               "two accumulator slots overlap the delayed scatter: scatter mode with delay bins >= 1");
   if (d->mode == BT_MODE_SCATTER) {
     BT_CHECK_ARG(d->csr_ptr && d->csr_edges && d->ring && d->work, "scatter needs CSR, ring and work");
     BT_CHECK_ARG((reinterpret_cast<uintptr_t>(d->csr_edges) & 15) == 0, "csr_edges must be 16-byte aligned");
@@ -1553,38 +1530,12 @@ bool fast_divisors(const bt_engine_desc& d, int kind) {
   return ok;
 }
 
-// The second stream and two events of the overlapped scatter, one set per
-// device, created on first use and kept until exit.
-struct Aux {
-  cudaStream_t s;
-  cudaEvent_t a, b;
-};
-std::mutex g_aux_mu;
-Aux g_aux[64];
-bool g_aux_ok[64];
-
-int aux_streams(Aux** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return bt_set_error(BT_ERR_CUDA, "cudaGetDevice");
-  std::lock_guard<std::mutex> lock(g_aux_mu);
-  if (!g_aux_ok[dev]) {
-    Aux& x = g_aux[dev];
-    if (cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&x.a, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&x.b, cudaEventDisableTiming) != cudaSuccess)
-      return bt_set_error(BT_ERR_CUDA, "creating the overlap stream failed");
-    g_aux_ok[dev] = true;
-  }
-  *out = &g_aux[dev];
-  return BT_OK;
-}
-
 template <int KIND, bool HARD, bool USE_REF>
 int run_typed(const bt_engine_desc& d, cudaStream_t s) {
   const int64_t n = d.n;
   if (d.mode == BT_MODE_TILE) {
     if (int st = run_tile(d, fast_divisors(d, KIND), s)) return st;
-    k_eng_scatter_final<<<int(ceil_div(d.batch * n, 256)), 256, 0, s>>>(d, 0);
+    k_eng_scatter_final<<<int(ceil_div(d.batch * n, 256)), 256, 0, s>>>(d);
     BT_CHECK_LAUNCH("k_eng_scatter_final");
     return BT_OK;
   }
@@ -1594,16 +1545,13 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned planes = unsigned(d.bin_hi - d.bin_lo + 1);
     // a plane lists at most n rows: no more blocks than n rows need (small
     // networks would otherwise launch mostly idle blocks every step)
     const int64_t rows_per_block = d.scatter_lanes == 1 ? kEngThreads : d.scatter_lanes == 8 ? kEngThreads / 8
                                                                                             : kEngThreads / 32;
-    auto scatter_grid = [&](int lo, int hi) {
-      const unsigned planes = unsigned(hi - lo + 1);
-      const int64_t xblocks = std::min(ceil_div(int64_t(sms) * 8, planes), ceil_div(n, rows_per_block));
-      return dim3(unsigned(std::max<int64_t>(xblocks, 1)), planes);
-    };
-    const dim3 sgrid = scatter_grid(d.bin_lo, d.bin_hi);
+    const int64_t xblocks = std::min(ceil_div(int64_t(sms) * 8, planes), ceil_div(n, rows_per_block));
+    const dim3 sgrid(unsigned(std::max<int64_t>(xblocks, 1)), planes);
     const int ms = mask_stride(d.batch);
     // every divisor a power of two or a verified reciprocal: no IEEE division compiled in
     const bool fast = fast_divisors(d, KIND);
@@ -1627,55 +1575,16 @@ int run_typed(const bt_engine_desc& d, cudaStream_t s) {
     const bool aligned = ((reinterpret_cast<uintptr_t>(d.psc) | reinterpret_cast<uintptr_t>(d.ring)) & 15) == 0;
     auto rec = C == 4 && aligned ? k_eng_neuron_rec<KIND, HARD, USE_REF, 4>
              : C == 2 && aligned ? k_eng_neuron_rec<KIND, HARD, USE_REF, 2> : k_eng_neuron_rec<KIND, HARD, USE_REF, 0>;
-    if (d.ring_slots != 2) {
-      for (int64_t k = 0; k < d.n_steps; ++k) {
-        const StepIdx si = scatter_step_idx(d, d.t0 + k);
-        if (C > 1) rec<<<rgrid, kEngThreads, 0, s>>>(d, k, si);
-        else neuron<<<grid, kEngThreads, 0, s>>>(d, int(k), si, scatter_scratch(d, si.q_t));
-        scatter<<<sgrid, kEngThreads, 0, s>>>(d, k, si);
-      }
-      BT_CHECK_LAUNCH("k_eng_neuron/k_eng_scatter");
-      if (d.n_steps > 0) {
-        k_eng_scatter_final<<<int(ceil_div(d.batch * n * C, 256)), 256, 0, s>>>(d, 0);
-        BT_CHECK_LAUNCH("k_eng_scatter_final");
-      }
-    } else {
-      // Overlapped delays (two accumulator slots alternating by step parity):
-      // the delay bins >= 1 of step t read spike sets of steps <= t - 1 only,
-      // so their scatter runs on a second stream beside the neuron launch of
-      // step t (which reads and clears the other slot); bin 0 needs step t's
-      // spikes and follows the neuron launch on the caller's stream.
-      //   caller stream:  wait S_hi(t-1) | record A | N(t) | S_0(t)
-      //   second stream:  wait A | S_hi(t) | record B
-      // N(t) waits for S_hi(t-1) and S_0(t-1) (slot t mod 2 complete); S_hi(t)
-      // waits for N(t-1) (spike set of t - 1 written, slot (t+1) mod 2
-      // cleared).  Under stream capture the events become graph edges.
-      Aux* aux = nullptr;
-      if (int st = aux_streams(&aux)) return st;
-      bt_engine_desc d_hi = d, d_0 = d;
-      d_hi.bin_lo = std::max(d.bin_lo, 1);
-      const bool has0 = d.bin_lo == 0;
-      d_0.bin_hi = 0;
-      const dim3 g_hi = scatter_grid(d_hi.bin_lo, d_hi.bin_hi), g_0 = scatter_grid(0, 0);
-      for (int64_t k = 0; k < d.n_steps; ++k) {
-        const StepIdx si = scatter_step_idx(d, d.t0 + k);
-        if (k > 0 && cudaStreamWaitEvent(s, aux->b, 0) != cudaSuccess)
-          return bt_set_error(BT_ERR_CUDA, "cudaStreamWaitEvent failed");
-        if (cudaEventRecord(aux->a, s) != cudaSuccess || cudaStreamWaitEvent(aux->s, aux->a, 0) != cudaSuccess)
-          return bt_set_error(BT_ERR_CUDA, "event record / wait failed");
-        scatter<<<g_hi, kEngThreads, 0, aux->s>>>(d_hi, k, si);
-        if (cudaEventRecord(aux->b, aux->s) != cudaSuccess) return bt_set_error(BT_ERR_CUDA, "event record failed");
-        if (C > 1) rec<<<rgrid, kEngThreads, 0, s>>>(d, k, si);
-        else neuron<<<grid, kEngThreads, 0, s>>>(d, int(k), si, scatter_scratch(d, si.q_t));
-        if (has0) scatter<<<g_0, kEngThreads, 0, s>>>(d_0, k, si);
-      }
-      BT_CHECK_LAUNCH("k_eng_neuron/k_eng_scatter (overlapped)");
-      if (d.n_steps > 0) {
-        if (cudaStreamWaitEvent(s, aux->b, 0) != cudaSuccess) return bt_set_error(BT_ERR_CUDA, "wait failed");
-        const int slot = int((d.t0 + d.n_steps) & 1);  // the slot the last step's scatter added into
-        k_eng_scatter_final<<<int(ceil_div(d.batch * n * C, 256)), 256, 0, s>>>(d, slot);
-        BT_CHECK_LAUNCH("k_eng_scatter_final");
-      }
+    for (int64_t k = 0; k < d.n_steps; ++k) {
+      const StepIdx si = step_idx(d.t0 + k, d.n_bins, d.hist_len);
+      if (C > 1) rec<<<rgrid, kEngThreads, 0, s>>>(d, k, si);
+      else neuron<<<grid, kEngThreads, 0, s>>>(d, int(k), si, scatter_scratch(d, si.q_t));
+      scatter<<<sgrid, kEngThreads, 0, s>>>(d, k, si);
+    }
+    BT_CHECK_LAUNCH("k_eng_neuron/k_eng_scatter");
+    if (d.n_steps > 0) {
+      k_eng_scatter_final<<<int(ceil_div(d.batch * n * C, 256)), 256, 0, s>>>(d);
+      BT_CHECK_LAUNCH("k_eng_scatter_final");
     }
   } else if (d.mode == BT_MODE_PULL) {
     // Words of the sample mask per warp: the descriptor may ask for 2 or 4
@@ -1754,8 +1663,7 @@ extern "C" int bt_engine_prime(const bt_engine_desc* d, void* stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const size_t words = size_t(scatter_work_words(d->n, d->batch, d->n_bins));
   if (cudaMemsetAsync(d->work, 0, sizeof(int32_t) * words, s) != cudaSuccess ||
-      cudaMemsetAsync(d->ring, 0, sizeof(float) * size_t(d->batch * d->n * n_rec(*d)) * (d->ring_slots == 2 ? 2 : 1),
-                      s) != cudaSuccess)
+      cudaMemsetAsync(d->ring, 0, sizeof(float) * size_t(d->batch * d->n * n_rec(*d)), s) != cudaSuccess)
     return bt_set_error(BT_ERR_CUDA, "memset failed");
   if (d->bin_hi > 0) {
     const int64_t npad = ((d->n + 31) >> 5) * 32;

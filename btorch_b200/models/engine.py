@@ -389,14 +389,10 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             keep.append(sl_w_d)
             desc.sl_ptr, desc.sl_src, desc.sl_w = sl.sl_ptr.data_ptr(), sl.sl_src.data_ptr(), sl_w_d.data_ptr()
             desc.dense_rows = dense
-        # delay bins >= 1: two accumulator slots, the delayed bins' scatter
-        # overlapped with the next neuron launch on a second stream
-        slots = 2 if lay_s.bin_hi >= 1 else 1
-        ring = alloc("ring", (slots, B, nc), torch.float32)  # W z of the step (bt_engine_prime clears it)
+        ring = alloc("ring", (B, nc), torch.float32)  # W z of the step (bt_engine_prime clears it)
         work = alloc("work", (L.lib().bt_engine_work_words(n, B, R),), torch.int32)
         keep += [ring, work]
         desc.ring, desc.work = ring.data_ptr(), work.data_ptr()
-        desc.ring_slots = slots
     tile_ws = None
     if mode == L.BT_MODE_TILE:
         lay_s = conn.scatter_layout(R, plan.uniform_delay, dev)
@@ -558,8 +554,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         set_desc(k0, kc, xp, slc, outs)
         e0 = _ev() if profile is not None else None
         L.check(L.lib().bt_engine_run(C.byref(desc), stream), "bt_engine_run")
-        per_step = (3 if desc.ring_slots == 2 and desc.bin_lo == 0 else 2) if mode == L.BT_MODE_SCATTER else 1
-        nl += 2 if mode == L.BT_MODE_TILE else per_step * kc + 1
+        nl += 2 if mode == L.BT_MODE_TILE else (2 * kc if mode == L.BT_MODE_SCATTER else kc) + 1
         if profile is not None:
             profile.append(("step", e0, _ev()))
         return nl

@@ -51,7 +51,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 9
+#define BT_ABI_VERSION 8
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -389,13 +389,6 @@ typedef struct bt_engine_desc {
   const int32_t* tile_off;
   int32_t* tile_work;
   int32_t spin_limit;
-  /* scatter mode with delay bins >= 1: 2 = overlap (`ring` holds two
-     [batch][n * n_rec] accumulator slots alternating by step parity; the
-     scatter of the bins >= 1 of step t runs on a second stream beside the
-     neuron launch of step t; bin 0 follows it on `stream`); 0 or 1 = one
-     slot, one stream.  The overlap's second stream and events are created
-     by the library on first use per device. */
-  int32_t ring_slots;
 } bt_engine_desc;
 
 /* Tile mode scratch words and shared memory bytes per CTA for a shape
