@@ -110,7 +110,7 @@ def parse():
 
 
 def parse_choice(text):
-    """'scatter,spt=2,lanes=1' / 'gather' / 'pull,words=2' / 'tile,tp=896' -> autotune.EngineChoice."""
+    """'scatter,spt=2,lanes=1' / 'gather' / 'pull,words=2' / 'tile,tp=896' / 'cluster,ctas=8' -> autotune.EngineChoice."""
     if not text:
         return None
     from btorch_b200 import _lib as L
@@ -119,10 +119,10 @@ def parse_choice(text):
     mode, *kv = text.split(",")
     f = dict(item.split("=") for item in kv)
     modes = {"scatter": L.BT_MODE_SCATTER, "gather": L.BT_MODE_GATHER, "pull": L.BT_MODE_PULL,
-             "tile": L.BT_MODE_TILE}
+             "tile": L.BT_MODE_TILE, "cluster": L.BT_MODE_CLUSTER}
     return EngineChoice(modes[mode], neuron_spt=int(f.get("spt", 0)), scatter_lanes=int(f.get("lanes", 0)),
                         pull_words=int(f.get("words", 0)), dense_rows=int(f.get("dense", -1)),
-                        tile_posts=int(f.get("tp", 0)))
+                        tile_posts=int(f.get("tp", f.get("ctas", 0))))
 
 
 # ------------------------------------------------------------- workload --

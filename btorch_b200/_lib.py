@@ -17,7 +17,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libbtorch_b200.so"
 
 BT_OK, BT_ERR_INVALID, BT_ERR_CUDA, BT_ERR_TIMEOUT, BT_ERR_UNSUPPORTED, BT_ERR_LAYOUT = range(6)
 BT_NEURON_LIF, BT_NEURON_ALIF = 0, 1
-BT_MODE_SCATTER, BT_MODE_GATHER, BT_MODE_PULL, BT_MODE_TILE = 0, 1, 2, 3
+BT_MODE_SCATTER, BT_MODE_GATHER, BT_MODE_PULL, BT_MODE_TILE, BT_MODE_CLUSTER = 0, 1, 2, 3, 4
 BT_BIN_SHIFT = 25
 BT_MAX_BINS = 128
 
@@ -26,7 +26,7 @@ _i64 = C.c_int64
 _i32 = C.c_int32
 
 
-ABI_VERSION = 8  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
+ABI_VERSION = 9  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
 
 
 class BtParam(C.Structure):
@@ -61,6 +61,7 @@ class BtEngineDesc(C.Structure):
         ("psc_uniform", _i32), ("psc_coef_s", C.c_float), ("psc_tau_s", C.c_float), ("psc_fast_div", _i32),
         ("psc_rcp", C.c_float), ("n_rec", _i32), ("csr_edges", _vp),
         ("tile_posts", _i32), ("n_tiles", _i32), ("tile_off", _vp), ("tile_work", _vp), ("spin_limit", _i32),
+        ("tile_rows", _i64),
     ]
 
 
@@ -94,6 +95,7 @@ _PROTOS = {
     "bt_masks_to_float": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
     "bt_tile_work_words": (C.c_int64, [_i64, _i32, _i32]),
     "bt_tile_smem_bytes": (C.c_int64, [_i64, _i32, _i32]),
+    "bt_cluster_smem_bytes": (C.c_int64, [_i64, _i64, _i32, _i64]),
     "bt_tile_offsets": (C.c_int, [_i64, _vp, _vp, _i32, _i32, _vp, _vp]),
     "bt_input_grad_weight": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _i32, _vp, _vp]),
 }

@@ -18,7 +18,7 @@ PKG = CSRC.parent
 ROOT = PKG.parent
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libbtorch_b200.so"
-SOURCES = ["layout.cpp", "spmv.cu", "neuron.cu", "engine.cu", "tile.cu", "raster.cu"]
+SOURCES = ["layout.cpp", "spmv.cu", "neuron.cu", "engine.cu", "tile.cu", "cluster.cu", "raster.cu"]
 HEADERS = ["common.cuh", "neuron.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

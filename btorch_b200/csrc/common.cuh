@@ -4,6 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+#include <vector>
+
 #include "../../include/btorch_b200.h"
 
 // Set the thread-local error text and return `status` (defined in layout.cpp).
@@ -94,6 +97,44 @@ __device__ __forceinline__ void red_add_f32(float* ptr, float v, uint64_t pol) {
   // no "memory" clobber: nothing in the issuing kernel reads the target, so
   // independent loads may be scheduled across the reduction
   asm volatile("red.global.add.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(ptr), "f"(v), "l"(pol));
+}
+
+// Launch set-ups already checked (kernel, device, dynamic shared memory,
+// blocks): the attribute calls and occupancy queries of a persistent launch
+// run once per set-up, not on every call -- they cost the host far more
+// than a short launch takes on the device.
+struct LaunchSetup {
+  const void* kern;
+  int dev;
+  size_t smem;
+  int blocks;
+};
+inline std::mutex& launch_setup_mutex() {
+  static std::mutex m;
+  return m;
+}
+inline std::vector<LaunchSetup>& launch_setups() {
+  static std::vector<LaunchSetup> v;
+  return v;
+}
+inline bool launch_setup_known(const void* kern, int dev, size_t smem, int blocks) {
+  std::lock_guard<std::mutex> g(launch_setup_mutex());
+  for (const LaunchSetup& e : launch_setups())
+    if (e.kern == kern && e.dev == dev && e.smem == smem && e.blocks == blocks) return true;
+  return false;
+}
+// The dynamic shared memory to allow a kernel: at least `smem` and never less
+// than a set-up already checked on this device asked for (the attribute is
+// the kernel's, shared by all its set-ups).
+inline size_t launch_smem_allow(const void* kern, int dev, size_t smem) {
+  std::lock_guard<std::mutex> g(launch_setup_mutex());
+  for (const LaunchSetup& e : launch_setups())
+    if (e.kern == kern && e.dev == dev && e.smem > smem) smem = e.smem;
+  return smem;
+}
+inline void launch_setup_add(const void* kern, int dev, size_t smem, int blocks) {
+  std::lock_guard<std::mutex> g(launch_setup_mutex());
+  launch_setups().push_back(LaunchSetup{kern, dev, smem, blocks});
 }
 
 }  // namespace bt

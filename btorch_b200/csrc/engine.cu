@@ -1452,7 +1452,8 @@ __global__ void k_float_to_bits(int64_t rows, int64_t n, const float* __restrict
 using namespace bt;
 
 namespace bt {
-int run_tile(const bt_engine_desc& d, bool fast, cudaStream_t s);  // tile.cu
+int run_tile(const bt_engine_desc& d, bool fast, cudaStream_t s);     // tile.cu
+int run_cluster(const bt_engine_desc& d, bool fast, cudaStream_t s);  // cluster.cu
 }
 
 namespace {
@@ -1467,7 +1468,7 @@ int engine_check(const bt_engine_desc* d) {
   BT_CHECK_ARG(d->n_steps >= 0 && d->t0 >= 0, "negative step index");
   BT_CHECK_ARG(d->n_steps < (int64_t(1) << 31), "n_steps must be below 2^31");
   BT_CHECK_ARG(d->mode == BT_MODE_SCATTER || d->mode == BT_MODE_GATHER || d->mode == BT_MODE_PULL ||
-                   d->mode == BT_MODE_TILE,
+                   d->mode == BT_MODE_TILE || d->mode == BT_MODE_CLUSTER,
                "mode=%d", d->mode);
   BT_CHECK_ARG(d->v && d->psc && d->hist, "state pointer missing (v / psc / hist)");
   BT_CHECK_ARG(!d->neuron.use_refractory || d->refractory, "refractory state missing");
@@ -1503,6 +1504,18 @@ int engine_check(const bt_engine_desc* d) {
                      int64_t(d->n_tiles - 1) * d->tile_posts < d->n,
                  "n_tiles=%d x tile_posts=%d does not tile n=%lld", d->n_tiles, d->tile_posts, (long long)d->n);
     BT_CHECK_ARG(d->batch <= 256 && d->batch * d->n < (int64_t(1) << 31), "tile mode: batch <= 256, batch * n < 2^31");
+  } else if (d->mode == BT_MODE_CLUSTER) {
+    BT_CHECK_ARG(d->sl_ptr && d->sl_src && d->sl_w, "cluster mode needs the sliced in-edge view");
+    BT_CHECK_ARG(d->n_bins == 1, "cluster mode has no synaptic delays");
+    BT_CHECK_ARG(d->tile_rows >= 0 && d->tile_rows < (int64_t(1) << 26), "tile_rows=%lld", (long long)d->tile_rows);
+    BT_CHECK_ARG(n_rec(*d) == 1, "cluster mode has no receptor channels");
+    BT_CHECK_ARG(d->tile_posts > 0 && (d->tile_posts & 31) == 0, "tile_posts=%d must be a positive multiple of 32",
+                 d->tile_posts);
+    BT_CHECK_ARG(d->n_tiles >= 1 && d->n_tiles <= 16 && int64_t(d->n_tiles) * d->tile_posts >= d->n &&
+                     int64_t(d->n_tiles - 1) * d->tile_posts < d->n,
+                 "n_tiles=%d (1..16) x tile_posts=%d does not tile n=%lld", d->n_tiles, d->tile_posts,
+                 (long long)d->n);
+    BT_CHECK_ARG(d->batch <= 256 && d->batch * d->n < (int64_t(1) << 31), "cluster mode: batch <= 256");
   } else if (d->mode == BT_MODE_GATHER) {
     BT_CHECK_ARG(d->csc_ptr && d->csc_src && d->csc_w, "gather needs CSC");
   } else {
@@ -1533,6 +1546,7 @@ bool fast_divisors(const bt_engine_desc& d, int kind) {
 template <int KIND, bool HARD, bool USE_REF>
 int run_typed(const bt_engine_desc& d, cudaStream_t s) {
   const int64_t n = d.n;
+  if (d.mode == BT_MODE_CLUSTER) return run_cluster(d, fast_divisors(d, KIND), s);  // no final launch
   if (d.mode == BT_MODE_TILE) {
     if (int st = run_tile(d, fast_divisors(d, KIND), s)) return st;
     k_eng_scatter_final<<<int(ceil_div(d.batch * n, 256)), 256, 0, s>>>(d);

@@ -512,16 +512,21 @@ int tile_launch(const bt_engine_desc& d, bool fast, cudaStream_t s) {
   void (*kern)(bt_engine_desc) = fast ? tile_kernel<KIND, HARD, USE_REF, true>(ms)
                                       : tile_kernel<KIND, HARD, USE_REF, false>(ms);
   const size_t smem = tile_smem_bytes(d.batch, d.tile_posts, d.n_tiles);
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
-    return bt_set_error(BT_ERR_UNSUPPORTED, "tile engine: %zu bytes of shared memory refused", smem);
-  int dev = 0, sms = 0, per_sm = 0;
+  int dev = 0;
   cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileThreads, smem) != cudaSuccess)
-    return bt_set_error(BT_ERR_CUDA, "tile engine: occupancy query failed");
-  if (int64_t(per_sm) * sms < d.n_tiles)
-    return bt_set_error(BT_ERR_UNSUPPORTED, "tile engine: %d tiles but only %d co-resident blocks", d.n_tiles,
-                        per_sm * sms);
+  if (!launch_setup_known(reinterpret_cast<const void*>(kern), dev, smem, d.n_tiles)) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(launch_smem_allow(reinterpret_cast<const void*>(kern), dev, smem))) != cudaSuccess)
+      return bt_set_error(BT_ERR_UNSUPPORTED, "tile engine: %zu bytes of shared memory refused", smem);
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileThreads, smem) != cudaSuccess)
+      return bt_set_error(BT_ERR_CUDA, "tile engine: occupancy query failed");
+    if (int64_t(per_sm) * sms < d.n_tiles)
+      return bt_set_error(BT_ERR_UNSUPPORTED, "tile engine: %d tiles but only %d co-resident blocks", d.n_tiles,
+                          per_sm * sms);
+    launch_setup_add(reinterpret_cast<const void*>(kern), dev, smem, d.n_tiles);
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(d.n_tiles));
   cfg.blockDim = dim3(kTileThreads);

@@ -41,11 +41,11 @@ class EngineChoice:
     pull_words: int = 0        # pull: 32-sample mask words per warp (0 = one)
     dense_rows: int = -1       # scatter, one delay bin: spiking neurons from which a step is pulled
                                # densely (-1 = n / engine.DENSE_FRACTION, 0 = never)
-    tile_posts: int = 0        # tile: posts per CTA (0 = one tile per SM)
+    tile_posts: int = 0        # tile: posts per CTA (0 = one tile per SM); cluster: CTAs of the cluster (0 = most)
 
     def describe(self) -> dict:
         name = {L.BT_MODE_SCATTER: "scatter", L.BT_MODE_GATHER: "gather", L.BT_MODE_PULL: "pull",
-                L.BT_MODE_TILE: "tile"}[self.mode]
+                L.BT_MODE_TILE: "tile", L.BT_MODE_CLUSTER: "cluster"}[self.mode]
         return {"mode": name, "neuron_spt": self.neuron_spt, "scatter_lanes": self.scatter_lanes,
                 "pull_words": self.pull_words, "dense_rows": self.dense_rows, "tile_posts": self.tile_posts}
 
@@ -67,7 +67,7 @@ def allowed_modes(conn, batch: int, receptors: int = 1, n_bins: int = 1) -> list
         modes.insert(1, L.BT_MODE_TILE)
     modes = [m for m in modes if receptors == 1 or m != L.BT_MODE_PULL]
     if receptors > 1 or n_bins > 1 or batch > 256:
-        modes = [m for m in modes if m != L.BT_MODE_TILE]
+        modes = [m for m in modes if m not in (L.BT_MODE_TILE, L.BT_MODE_CLUSTER)]
     return modes
 
 
@@ -89,6 +89,15 @@ def candidates(conn, batch: int, receptors: int = 1, n_bins: int = 1, n: int = 0
     mw = L.lib().bt_mask_stride(batch)
     modes = allowed_modes(conn, batch, receptors, n_bins)
     for mode in modes:
+        if mode == L.BT_MODE_CLUSTER:
+            from .engine import cluster_shape, slices_of
+
+            if n and dev is not None:
+                lay = conn.engine_layout(1, 0, dev)
+                slices_of(lay, dev)
+                if cluster_shape(n, batch, lay.slices_ptr_host) is not None:
+                    out.append(EngineChoice(mode))
+            continue
         if mode == L.BT_MODE_TILE:
             from .engine import tile_shape
 

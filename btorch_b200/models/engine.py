@@ -167,6 +167,54 @@ def tile_shape(n: int, batch: int, dev, tile_posts: int = 0):
     return tp, P
 
 
+def cluster_shape(n: int, batch: int, sl_ptr, ctas: int = 0):
+    """(tile_posts, n_ctas, tile_rows) of the single-cluster engine, or None
+    when the tiles' state and in-edges do not fit one cluster's shared
+    memory.  sl_ptr: the sliced in-edge view's slice -> first row offsets
+    (host array).  By default the most CTAs (up to 16) whose tiles hold at
+    least 128 posts, else the most that fit."""
+    import numpy as np
+
+    sl_ptr = np.asarray(sl_ptr, dtype=np.int64)
+    if batch > 256:
+        return None
+
+    def shape(cl):
+        tp = 32 * -(-(-(-n // cl)) // 32)
+        P = -(-n // tp)
+        if P > 16:
+            return None
+        w = tp // 32
+        # rows of each tile's slices, each slice rounded up to a multiple of 4
+        slice_rows = -(-np.diff(sl_ptr) // 4) * 4
+        acc = np.concatenate([[0], np.cumsum(slice_rows)])
+        starts = np.minimum(np.arange(P + 1) * w, len(acc) - 1)
+        rows = int(np.diff(acc[starts]).max(initial=0))
+        if L.lib().bt_cluster_smem_bytes(n, batch, tp, rows) > MAX_TILE_SMEM - 1024:  # + static barriers
+            return None
+        return tp, P, rows
+
+    counts = [int(ctas)] if ctas else [16, 8, 4, 2, 1]
+    for big_tiles in ((True, False) if not ctas else (False,)):
+        for cl in counts:
+            got = shape(cl)
+            if got is not None and (not big_tiles or got[0] >= 128 or cl == 1):
+                return got
+    return None
+
+
+def slices_of(lay, dev):
+    """The sliced in-edge view of a layout (built once, kept on the layout),
+    with a host copy of its slice offsets."""
+    sl = getattr(lay, "slices", None)
+    if sl is None:
+        sl = build_slices(lay, dev)
+        lay.slices = sl
+    if getattr(lay, "slices_ptr_host", None) is None:
+        lay.slices_ptr_host = sl.sl_ptr.cpu().numpy()
+    return sl
+
+
 def tile_offsets(lay, edges: torch.Tensor, tp: int, P: int, dev) -> torch.Tensor:
     """The CSR rows split at the tile boundaries ([rows][P + 1] int32), cached
     on the layout per tile shape (they depend on the posts only)."""
@@ -411,6 +459,20 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         desc.tile_posts, desc.n_tiles = tp, P
         desc.tile_off, desc.tile_work = toff.data_ptr(), tile_ws.data_ptr()
         desc.spin_limit = int(getattr(rnn, "engine_spin_limit", 0))
+    if mode == L.BT_MODE_CLUSTER:
+        if R > 1:
+            raise NotImplementedError("cluster mode has no synaptic delays")
+        sl = slices_of(lay, dev)
+        shape = cluster_shape(n, B, lay.slices_ptr_host, choice.tile_posts)
+        if shape is None:
+            raise NotImplementedError("cluster mode: the network does not fit one cluster's shared memory")
+        sl_w = static("sl_w", pack_slice_weights(sl, w))
+        tile_ws = alloc("tile_work", (32,), torch.int32, zero=True)  # word 2: status (a wait that gave up)
+        keep += [sl_w, tile_ws]
+        desc.sl_ptr, desc.sl_src, desc.sl_w = sl.sl_ptr.data_ptr(), sl.sl_src.data_ptr(), sl_w.data_ptr()
+        desc.tile_posts, desc.n_tiles, desc.tile_rows = shape
+        desc.tile_work = tile_ws.data_ptr()
+        desc.spin_limit = int(getattr(rnn, "engine_spin_limit", 0))
     if mode == L.BT_MODE_PULL:
         sl = getattr(lay, "slices", None)
         if sl is None:
@@ -554,7 +616,8 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         set_desc(k0, kc, xp, slc, outs)
         e0 = _ev() if profile is not None else None
         L.check(L.lib().bt_engine_run(C.byref(desc), stream), "bt_engine_run")
-        nl += 2 if mode == L.BT_MODE_TILE else (2 * kc if mode == L.BT_MODE_SCATTER else kc) + 1
+        nl += 1 if mode == L.BT_MODE_CLUSTER else 2 if mode == L.BT_MODE_TILE else \
+            (2 * kc if mode == L.BT_MODE_SCATTER else kc) + 1
         if profile is not None:
             profile.append(("step", e0, _ev()))
         return nl
@@ -625,8 +688,8 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         status = int(tile_ws[2].item())  # the launches' status word (a barrier wait that gave up)
         if status:
             tile_ws[:32].zero_()
-            raise RuntimeError("fused engine, tile mode: a grid barrier wait gave up (BT_ERR_TIMEOUT); "
-                               "the call's results are invalid")
+            what = "tile mode: a grid barrier" if mode == L.BT_MODE_TILE else "cluster mode: a spike-word"
+            raise RuntimeError(f"fused engine, {what} wait gave up (BT_ERR_TIMEOUT); the call's results are invalid")
 
     if use_graph:
         v_mod.copy_(v)
@@ -676,7 +739,8 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             states[key] = traces[kind].view(T, *batch_shape, *_nshape(plan, key))
     rnn.last_engine_stats = stat_t
     rnn.last_engine_direction = {L.BT_MODE_SCATTER: "scatter", L.BT_MODE_GATHER: "gather",
-                                 L.BT_MODE_PULL: "pull", L.BT_MODE_TILE: "scatter"}[mode]
+                                 L.BT_MODE_PULL: "pull", L.BT_MODE_TILE: "scatter",
+                                 L.BT_MODE_CLUSTER: "gather"}[mode]
     rnn.last_engine_launches = launches
     rnn.last_engine_choice = choice
     if z is not None:

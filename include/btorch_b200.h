@@ -51,7 +51,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 8
+#define BT_ABI_VERSION 9
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -285,6 +285,12 @@ BT_API int bt_psc_step(int64_t batch, int64_t n, bt_param coef, bt_param tau_syn
 #define BT_MODE_TILE 3     /* persistent: one launch for all n_steps, one CTA per tile
                               of posts with its synaptic input in shared memory, a
                               bounded grid barrier per step; single delay bin 0 */
+#define BT_MODE_CLUSTER 4  /* persistent, small networks: one launch for all n_steps,
+                              one thread-block cluster of n_tiles <= 16 CTAs holds
+                              state and in-edges in shared memory, ordered in-edge
+                              sums (bit-exact), spike words exchanged through
+                              distributed shared memory, a hardware cluster barrier
+                              per step; single delay bin 0, no receptor channels */
 
 typedef struct bt_engine_desc {
   /* sizes */
@@ -389,7 +395,18 @@ typedef struct bt_engine_desc {
   const int32_t* tile_off;
   int32_t* tile_work;
   int32_t spin_limit;
+  /* cluster mode (BT_MODE_CLUSTER, no counterpart in the reference): rank t
+     of the cluster owns posts [t * tile_posts, (t + 1) * tile_posts), n_tiles
+     <= 16 CTAs cover n; the in-edges come from the sliced view sl_ptr /
+     sl_src / sl_w (one launch per call, no final launch, no ring).
+     tile_rows: the most SELL-32 rows of any tile's slices, which sizes the
+     shared memory (a tile with more rows has its excess ignored) */
+  int64_t tile_rows;
 } bt_engine_desc;
+
+/* Cluster mode shared memory per CTA (0 for a bad shape): n neurons, a
+   tile of tile_posts posts (a multiple of 32) holding tile_rows slice rows. */
+BT_API int64_t bt_cluster_smem_bytes(int64_t n, int64_t batch, int32_t tile_posts, int64_t tile_rows);
 
 /* Tile mode scratch words and shared memory bytes per CTA for a shape
    (0 for a bad shape). */

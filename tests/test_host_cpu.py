@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
     for s in syms:
         assert hasattr(lib, s), s
     assert set(syms) == set(L.exported_symbols())
-    assert lib.bt_abi_version() == L.ABI_VERSION == 8
+    assert lib.bt_abi_version() == L.ABI_VERSION == 9
 
 
 def test_layout_matches_numpy_reference():
