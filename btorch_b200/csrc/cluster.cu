@@ -38,15 +38,18 @@ namespace cg = cooperative_groups;
 
 namespace bt {
 
-constexpr int kClThreads = 512;
+constexpr int kClThreads = 256;
+// in-edge rows of a slice are padded to a multiple of kClRows; the sum walks
+// them kClRows at a time with every load of the block issued first
+constexpr int kClRows = 16;
 constexpr int kClMaxCtas = 16;
 
 // Shared-memory carve-up of one CTA (bytes, every part 16-byte aligned):
 // state [4][B][Tp] f32 | edge weights [rows][32] f32 | presynaptic ids
 // [rows][32] (u16 when src16, else u32) | bitmaps [2][B][Wd] u32 | slice
 // group offsets [NW + 1] i32 | sample lengths [B] i32 | out-degrees [Tp] i32.
-// rows: the tile's slice rows, each slice rounded up to a multiple of 4 and
-// stored as groups of 4 rows per lane ([group][lane][4]), so that one
+// rows: the tile's slice rows, each slice rounded up to a multiple of kClRows
+// and stored as groups of 4 rows per lane ([group][lane][4]), so that one
 // 8- or 16-byte load brings 4 in-edges of a post.
 struct ClusterSmem {
   size_t state, w, src, bits, gptr, len, deg, total;
@@ -198,7 +201,7 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
     int acc = 0;
     for (int w = 0; w < NWv; ++w) {
       s_gptr[w] = min(acc, g_max);
-      acc += int((d.sl_ptr[w0 + w + 1] - d.sl_ptr[w0 + w] + 3) >> 2);
+      acc += int((d.sl_ptr[w0 + w + 1] - d.sl_ptr[w0 + w] + kClRows - 1) / kClRows) * (kClRows / 4);
     }
     s_gptr[NWv] = min(acc, g_max);
   }
@@ -290,17 +293,29 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
         const float4* wg = reinterpret_cast<const float4*>(s_w);
         float g = 0.0f;
         const int ge = s_gptr[w + 1];
-#pragma unroll 2
-        for (int gi = s_gptr[w]; gi < ge; ++gi) {
-          uint32_t sr[4], bw[4];
-          SrcGroup<SRC16>::split(srcg[gi * 32 + lane], sr);
-          const float4 wv = wg[gi * 32 + lane];
+        // blocks of kClRows rows (kClRows / 4 groups): the ids, the bitmap
+        // words and the weights of a block are loaded before its additions
+        constexpr int NG = kClRows / 4;
+        for (int gc = s_gptr[w]; gc < ge; gc += NG) {
+          uint32_t sr[kClRows], rot[kClRows];
+          float wv[kClRows];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) bw[u] = bits[sr[u] >> 5];
-          if (int(__funnelshift_l(bw[0], bw[0], sr[0])) < 0) g = add(g, wv.x);
-          if (int(__funnelshift_l(bw[1], bw[1], sr[1])) < 0) g = add(g, wv.y);
-          if (int(__funnelshift_l(bw[2], bw[2], sr[2])) < 0) g = add(g, wv.z);
-          if (int(__funnelshift_l(bw[3], bw[3], sr[3])) < 0) g = add(g, wv.w);
+          for (int j = 0; j < NG; ++j) {
+            SrcGroup<SRC16>::split(srcg[(gc + j) * 32 + lane], sr + 4 * j);
+            const float4 w4 = wg[(gc + j) * 32 + lane];
+            wv[4 * j] = w4.x;
+            wv[4 * j + 1] = w4.y;
+            wv[4 * j + 2] = w4.z;
+            wv[4 * j + 3] = w4.w;
+          }
+#pragma unroll
+          for (int u = 0; u < kClRows; ++u) {
+            const uint32_t bw = bits[sr[u] >> 5];
+            rot[u] = __funnelshift_l(bw, bw, sr[u]);
+          }
+#pragma unroll
+          for (int u = 0; u < kClRows; ++u)
+            if (int(rot[u]) < 0) g = add(g, wv[u]);
         }
         float pc = pc_u;
         Div dpt = dpt_u;
@@ -362,15 +377,17 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
       }
     }
     __syncwarp();
+    // the history ring holds the last H steps: only those are written
+    const bool hist = k + H >= d.n_steps;
     for (int it = warp; it < items; it += W) {
       const int b = it / NWv, w = it - b * NWv;
       if (lane == 0) {
         const uint32_t word = s_bits[(cur * B + b) * Wd + w0 + w];  // this warp's own store
-        d.hist[(int64_t(h_t) * B + b) * words + w0 + w] = word;
+        if (hist) d.hist[(int64_t(h_t) * B + b) * words + w0 + w] = word;
         if (d.raster) d.raster[(k * B + b) * words + w0 + w] = word;
       }
     }
-    if (d.stats) {
+    if (d.stats && (warp < items || B > 1)) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         st_un += __shfl_xor_sync(0xffffffffu, st_un, o);

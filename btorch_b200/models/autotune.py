@@ -53,7 +53,8 @@ class EngineChoice:
 def allowed_modes(conn, batch: int, receptors: int = 1, n_bins: int = 1) -> list[int]:
     """Delivery modes the sparse config admits (the sliced pull has no
     receptor channels: with receptors > 1 it is left out; the tile mode
-    delivers push-wise like scatter, without delays or receptor channels)."""
+    delivers push-wise like scatter, the cluster mode pulls like gather, both
+    without delays or receptor channels)."""
     cfg = conn.sparse_config
     if cfg.deterministic or cfg.direction == "gather":
         modes = [L.BT_MODE_GATHER, L.BT_MODE_PULL]
@@ -65,6 +66,11 @@ def allowed_modes(conn, batch: int, receptors: int = 1, n_bins: int = 1) -> list
         # the persistent tile engine: opt-in -- its push delivery is slow in a
         # start-up burst, which the tuner's trial window (after a warm-up) misses
         modes.insert(1, L.BT_MODE_TILE)
+    if cfg.direction != "scatter":
+        # the single-cluster engine: an ordered in-edge gather (bit-exact, so
+        # also under `deterministic`) for networks that fit one cluster's
+        # shared memory, see candidates()
+        modes.insert(1, L.BT_MODE_CLUSTER)
     modes = [m for m in modes if receptors == 1 or m != L.BT_MODE_PULL]
     if receptors > 1 or n_bins > 1 or batch > 256:
         modes = [m for m in modes if m not in (L.BT_MODE_TILE, L.BT_MODE_CLUSTER)]
@@ -147,6 +153,8 @@ def choose(plan, rnn, x: torch.Tensor, sample_len, run) -> EngineChoice:
     if not plan.conn.sparse_config.autotune or T < TUNE_MIN_STEPS:
         return heuristic(plan.conn, B, plan.n_rec)
     cands = candidates(plan.conn, B, plan.n_rec, plan.n_bins, plan.neuron.size, plan.neuron.v.device)
+    if plan.uniform_delay:  # a DelayedPSC delay: the persistent modes have none
+        cands = [c for c in cands if c.mode not in (L.BT_MODE_TILE, L.BT_MODE_CLUSTER)]
     if len(cands) == 1:
         cache[key] = (cands[0], {})
         return cands[0]

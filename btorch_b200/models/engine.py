@@ -185,8 +185,8 @@ def cluster_shape(n: int, batch: int, sl_ptr, ctas: int = 0):
         if P > 16:
             return None
         w = tp // 32
-        # rows of each tile's slices, each slice rounded up to a multiple of 4
-        slice_rows = -(-np.diff(sl_ptr) // 4) * 4
+        # rows of each tile's slices, each slice rounded up to a multiple of 16
+        slice_rows = -(-np.diff(sl_ptr) // 16) * 16
         acc = np.concatenate([[0], np.cumsum(slice_rows)])
         starts = np.minimum(np.arange(P + 1) * w, len(acc) - 1)
         rows = int(np.diff(acc[starts]).max(initial=0))
@@ -261,6 +261,10 @@ class _GraphEntry:
         self.sig = None
         self.captures = 0
         self.replays = 0
+        # shorter last chunks of a call (T not a multiple of the chunk):
+        # steps -> [graph, signature, launches, times seen]; captured the
+        # second time a length comes (a one-off call stays eager)
+        self.rest: dict[int, list] = {}
 
     def alloc(self, name, shape, dtype, dev, zero=False):
         t = self.buf.get(name)
@@ -268,6 +272,7 @@ class _GraphEntry:
             t = torch.empty(shape, device=dev, dtype=dtype)
             self.buf[name] = t
             self.graph = None
+            self.rest = {}
         if zero:
             t.zero_()
         return t
@@ -315,7 +320,8 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     replayed for every full chunk (the counterpart of the reference's
     CudaGraphRunner, btorch/models/cudagraph.py:101-242, with the state copied
     in once per call rather than once per chunk); a shorter last chunk runs
-    eagerly on the same buffers.
+    eagerly on the same buffers the first time its length comes and is
+    captured (and replayed from then on) the second time.
 
     profile: if a list, (kind, start_event, end_event) CUDA-event pairs are
     appended for every input-projection ("project") and recurrent-step
@@ -325,6 +331,7 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     choice: delivery mode and tiles (default: the autotuner's cached or fresh
     choice for this problem shape, see autotune.py)."""
     _check_input(plan, x)
+    check_pending_status(rnn)  # an earlier deferred status that has arrived
     launches = 0
 
     def _ev():
@@ -669,6 +676,27 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
                 entry.replays += 1
                 nl = entry.nodes
             launches += nl
+        elif profile is None:
+            # the call's shorter last chunk (it starts at a multiple of K: the
+            # slot phase of k0 = 0, like the full chunks)
+            set_desc(0, kc, xp, slc, out_c)
+            sig = _graph_signature(desc, xin, xp, slc, out_c, w_t if inp is not None else None,
+                                   bias if inp is not None else None)
+            rest = entry.rest.setdefault(kc, [None, None, 0, 0])
+            rest[3] += 1
+            if rest[0] is not None and rest[1] == sig:
+                rest[0].replay()
+                launches += rest[2]
+            else:
+                launches += launch(k0, kc, xin, xp, slc, out_c, s)
+                if rest[3] >= 2:
+                    torch.cuda.synchronize(dev)
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g):
+                        if "stats" in out_c:
+                            out_c["stats"].zero_()
+                        rest[2] = launch(0, kc, xin, xp, slc, out_c, L.stream_of(dev))
+                    rest[0], rest[1] = g, sig
         else:
             launches += launch(k0, kc, xin, xp, slc, out_c, s)
         if host_io:
@@ -685,11 +713,20 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     if host_io:
         io.finish()
     if tile_ws is not None:
-        status = int(tile_ws[2].item())  # the launches' status word (a barrier wait that gave up)
-        if status:
-            tile_ws[:32].zero_()
-            what = "tile mode: a grid barrier" if mode == L.BT_MODE_TILE else "cluster mode: a spike-word"
-            raise RuntimeError(f"fused engine, {what} wait gave up (BT_ERR_TIMEOUT); the call's results are invalid")
+        # the launches' status word (a wait that gave up)
+        what = "tile mode: a grid barrier" if mode == L.BT_MODE_TILE else "cluster mode: a spike-word"
+        if getattr(rnn, "engine_status_check", "sync") == "deferred":
+            host = torch.empty(1, dtype=torch.int32, pin_memory=True)
+            host.copy_(tile_ws[2:3], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.current_stream(dev))
+            rnn._engine_pending_status = (host, ev, what)
+        else:
+            status = int(tile_ws[2].item())
+            if status:
+                tile_ws[:32].zero_()
+                raise RuntimeError(f"fused engine, {what} wait gave up (BT_ERR_TIMEOUT); "
+                                   "the call's results are invalid")
 
     if use_graph:
         v_mod.copy_(v)
@@ -820,6 +857,23 @@ class _HostStreams:
 
     def finish(self):
         self.cs.synchronize()  # host outputs complete; staging buffers idle
+
+
+def check_pending_status(rnn, wait: bool = False) -> None:
+    """Raise for a deferred status word of an earlier call that reports a
+    wait that gave up.  Without `wait`, a status still in flight stays
+    pending."""
+    pend = getattr(rnn, "_engine_pending_status", None)
+    if pend is None:
+        return
+    host, ev, what = pend
+    if not wait and not ev.query():
+        return
+    ev.synchronize()
+    rnn._engine_pending_status = None
+    if int(host[0]):
+        raise RuntimeError(f"fused engine, {what} wait gave up (BT_ERR_TIMEOUT) in an earlier call; "
+                           "its results are invalid")
 
 
 def _graph_signature(desc, *tensors):

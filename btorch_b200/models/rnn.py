@@ -44,6 +44,12 @@ class RecurrentNNAbstract(base.MemoryModule):
         self.cudagraph_warmup = cudagraph_warmup
         self._cudagraph_runner = CudaGraphRunner(warmup=cudagraph_warmup)
         self.fused = fused
+        # the persistent engine modes' status word (a bounded wait that gave
+        # up): "sync" reads it at the end of every call (one host
+        # synchronisation; the call raises), "deferred" copies it to the host
+        # asynchronously and raises at a later call or at engine_status()
+        self.engine_status_check = "sync"
+        self._engine_pending_status = None
         self.last_engine_stats = None
         self.last_engine_direction = None
         self.last_path = None
@@ -209,6 +215,11 @@ class RecurrentNN(RecurrentNNAbstract):
         z = self.neuron(self.synapse.psc + x)
         self.synapse(z if x_syn is None else z + x_syn)
         return z, filter_hidden_states(self, self.update_state_names, allow_buffer=self.allow_buffer)
+
+    def engine_status(self):
+        """Wait for the status of the last persistent-engine call checked in
+        "deferred" mode and raise RuntimeError if a wait in it gave up."""
+        _engine.check_pending_status(self, wait=True)
 
     def fused_plan(self):
         """The engine plan for this model, or (None, reason)."""

@@ -91,9 +91,9 @@ def test_cluster_any_weights_bitwise_vs_oracle_and_gather(n, batch):
 def test_cluster_shape_and_too_large_network():
     from btorch_b200.models.engine import cluster_shape
 
-    sl_ptr = np.arange(0, 129) * 60  # 128 slices of 60 rows: n = 4096
-    assert cluster_shape(4096, 1, sl_ptr) == (256, 16, 480)
-    assert cluster_shape(4096, 1, sl_ptr, ctas=8) == (512, 8, 960)
+    sl_ptr = np.arange(0, 129) * 64  # 128 slices of 64 rows: n = 4096
+    assert cluster_shape(4096, 1, sl_ptr) == (256, 16, 512)
+    assert cluster_shape(4096, 1, sl_ptr, ctas=8) == (512, 8, 1024)
     assert cluster_shape(4096, 1, np.arange(0, 129) * 61) == (256, 16, 512)  # slices rounded up to 64 rows
     assert cluster_shape(4096, 1, sl_ptr * 2, ctas=8) is None  # 1920 rows: 368 KB of edges
     assert cluster_shape(4096, 1, np.arange(0, 129) * 1000) is None  # 8000 rows a tile
@@ -171,3 +171,23 @@ def test_cluster_wait_timeout_is_reported_and_the_context_stays_usable():
     spec = _spec(conn, n, 0)
     o = O.run(spec, O.init_state(spec, B), x, events=True)
     np.testing.assert_array_equal(z.cpu().numpy().astype(np.uint8), o["spikes"])
+
+
+def test_cluster_deferred_status_reports_at_engine_status():
+    """engine_status_check = "deferred": the call that gave up returns
+    without a host synchronisation; engine_status() raises for it."""
+    rng = np.random.default_rng(8)
+    n, T, B = 4096, 100, 1
+    conn = _dyadic(rng, n, 0.02)
+    x = torch.tensor((np.round(rng.poisson(0.05, (T, B, n)) * 0.5 * 64) / 64).astype(np.float32), device="cuda")
+    rnn = _model(conn, n, 0, B, names=())
+    rnn.engine_status_check = "deferred"
+    rnn.engine_spin_limit = 1
+    with torch.no_grad(), environ.context(dt=1.0):
+        rnn(x, engine_choice=cluster())
+    with pytest.raises(RuntimeError, match="gave up"):
+        rnn.engine_status()
+    rnn.engine_spin_limit = 0
+    with torch.no_grad(), environ.context(dt=1.0):
+        rnn(x, engine_choice=cluster())
+    rnn.engine_status()  # nothing pending that failed

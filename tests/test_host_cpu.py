@@ -341,3 +341,25 @@ def test_tile_mode_is_an_opt_in_candidate():
     assert L.BT_MODE_TILE not in autotune.allowed_modes(conn, 300)
     conn.sparse_config.direction = "gather"
     assert L.BT_MODE_TILE not in autotune.allowed_modes(conn, 8)
+
+
+def test_cluster_mode_is_a_candidate_unless_scatter_is_asked_for():
+    """The single-cluster engine (an ordered gather) is offered with
+    direction auto or gather, deterministic included, but not with an
+    explicit scatter, receptor channels, delays or more than 256 samples."""
+    import scipy.sparse as sp
+
+    from btorch_b200.models import SparseConn, autotune
+
+    conn = SparseConn(sp.coo_array(np.eye(64, dtype=np.float32)), sparse_config={"direction": "auto"})
+    assert L.BT_MODE_CLUSTER in autotune.allowed_modes(conn, 8)
+    assert L.BT_MODE_CLUSTER not in autotune.allowed_modes(conn, 8, receptors=2)
+    assert L.BT_MODE_CLUSTER not in autotune.allowed_modes(conn, 8, n_bins=3)
+    assert L.BT_MODE_CLUSTER not in autotune.allowed_modes(conn, 300)
+    conn.sparse_config.direction = "gather"
+    assert L.BT_MODE_CLUSTER in autotune.allowed_modes(conn, 8)
+    conn.sparse_config.deterministic = True
+    assert L.BT_MODE_CLUSTER in autotune.allowed_modes(conn, 8)
+    conn.sparse_config.deterministic = False
+    conn.sparse_config.direction = "scatter"
+    assert L.BT_MODE_CLUSTER not in autotune.allowed_modes(conn, 8)
