@@ -8,7 +8,7 @@
 //   - its tile's state (v, psc, refractory, g_k) for every sample;
 //   - its tile's in-edges, the SELL-32 slices of the CSC (lane = post, the
 //     k-th in-edge of each post in row k, ascending canonical order), the
-//     presynaptic id narrowed to 16 bits when n < 2^16;
+//     presynaptic id stored as id ^ 31 (16 bits when n + 32 <= 2^16);
 //   - two copies of the whole network's spike bitmap ([2][batch][words + 1],
 //     the last word of each sample zero: the slices' padding points there).
 // Per step k, each warp takes (32-post word of the tile, sample):
@@ -17,13 +17,14 @@
 //             fp32 chain of the gather engine: the reference's rounding for
 //             ANY weights, not only dyadic ones;
 //   neuron    I = P + x, LIF/ALIF update, the spike word by ballot;
-//   publish   the word into bitmap copy k mod 2 of every CTA of the cluster
-//             (distributed shared memory stores, one lane per CTA).
-// then one hardware cluster barrier.  Double-buffered bitmaps make one
-// barrier per step enough: step k reads copy (k - 1) mod 2 and writes copy
-// k mod 2, which was last read during step k - 1 -- by every CTA before the
-// barrier that ends step k - 1, which every CTA passes before its first
-// store of step k.
+//   publish   the word into bitmap copy k mod 2 of every other CTA of the
+//             cluster (st.async, one lane per CTA, its bytes counted on the
+//             receiver's mbarrier for that copy) and of its own (plain store).
+// Then thread 0 waits (bounded) for the copy's barrier phase and the CTA
+// synchronises: every word of step k is in this CTA's copy.  Double-buffered
+// copies need no cluster-wide barrier: a CTA arms a copy's barrier for step
+// s + 1 right after its wait for step s - 1 and before it publishes step s,
+// which every sender of step s + 1 has to have received first.
 // After the last step the launch applies the synapse update of that step
 // (the gather engine's final launch) and writes the state back: one launch
 // per call, nothing per step in global memory but the input read and the
