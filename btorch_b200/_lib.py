@@ -26,7 +26,7 @@ _i64 = C.c_int64
 _i32 = C.c_int32
 
 
-ABI_VERSION = 9  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
+ABI_VERSION = 10  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
 
 
 class BtParam(C.Structure):
@@ -61,7 +61,7 @@ class BtEngineDesc(C.Structure):
         ("psc_uniform", _i32), ("psc_coef_s", C.c_float), ("psc_tau_s", C.c_float), ("psc_fast_div", _i32),
         ("psc_rcp", C.c_float), ("n_rec", _i32), ("csr_edges", _vp),
         ("tile_posts", _i32), ("n_tiles", _i32), ("tile_off", _vp), ("tile_work", _vp), ("spin_limit", _i32),
-        ("tile_rows", _i64),
+        ("tile_rows", _i64), ("cl_w", _vp), ("cl_src", _vp), ("cl_gptr", _vp),
     ]
 
 

@@ -115,6 +115,15 @@ __device__ __forceinline__ uint32_t cluster_addr(const void* local, uint32_t ran
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_addr(local)), "r"(rank));
   return r;
 }
+// bulk copy (no multicast) of `bytes` (a multiple of 16, both addresses
+// 16-byte aligned) from global into this CTA's shared memory, completing on
+// the CTA's mbarrier `bar`
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* gmem_src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(smem_dst)),
+               "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
 __device__ __forceinline__ void st_async_word(uint32_t raddr, uint32_t v, uint32_t rbar) {
   asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.u32 [%0], %1, [%2];" ::"r"(raddr), "r"(v),
                "r"(rbar)
@@ -195,33 +204,22 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
   for (int q = threadIdx.x; q < B; q += kClThreads)
     s_len[q] = d.sample_len ? int(min(int64_t(d.sample_len[q]), int64_t(INT32_MAX))) : INT32_MAX;
   for (int l = threadIdx.x; l < Tp; l += kClThreads) s_deg[l] = (d.outdeg && l < tile_n) ? d.outdeg[p0 + l] : 0;
-  // slice group offsets (clamped to the groups the shared memory holds, which
-  // the caller sizes to the largest tile: accesses stay in bounds whatever it
-  // passes)
+  // the tile's in-edges: its packed block of each array, one bulk copy each,
+  // completing on s_mbar[2]; its slice group offsets (clamped to the groups
+  // the shared memory holds: the accesses stay in bounds whatever is passed)
+  const int gstride = Tp / 32 + 1;
+  for (int q = threadIdx.x; q <= NWv; q += kClThreads) s_gptr[q] = min(d.cl_gptr[rank * gstride + q], g_max);
+  __shared__ __align__(8) uint64_t s_mbar[3];  // [0], [1]: the bitmap copies; [2]: the in-edge copies
   if (threadIdx.x == 0) {
-    int acc = 0;
-    for (int w = 0; w < NWv; ++w) {
-      s_gptr[w] = min(acc, g_max);
-      acc += int((d.sl_ptr[w0 + w + 1] - d.sl_ptr[w0 + w] + kClRows - 1) / kClRows) * (kClRows / 4);
-    }
-    s_gptr[NWv] = min(acc, g_max);
-  }
-  __syncthreads();
-  // in-edges, group-major (rows 4 g .. 4 g + 3 of a lane contiguous); rows
-  // past a slice's end hold the padding id n, weight 0
-  const uint32_t pad = uint32_t(n) ^ 31u;
-  for (int w = 0; w < NWv; ++w) {
-    const int64_t row0 = d.sl_ptr[w0 + w], rows = d.sl_ptr[w0 + w + 1] - row0;
-    const int g0 = s_gptr[w], ng = s_gptr[w + 1] - g0;
-    for (int e = threadIdx.x; e < ng * 128; e += kClThreads) {
-      const int grp = e >> 7, u = (e >> 5) & 3, ln = e & 31;
-      const int64_t row = int64_t(grp) * 4 + u;
-      const bool in = row < rows;
-      const uint32_t src = in ? (__ldg(d.sl_src + (row0 + row) * 32 + ln) & kIdMask) ^ 31u : pad;
-      const float wv = in ? __ldg(d.sl_w + (row0 + row) * 32 + ln) : 0.0f;
-      const int at = ((g0 + grp) * 32 + ln) * 4 + u;
-      s_src[at] = Src(src);
-      s_w[at] = wv;
+    mbar_init(&s_mbar[2], 1);
+    mbar_init_fence();
+    const int ng = NWv ? min(d.cl_gptr[rank * gstride + NWv], g_max) : 0;
+    const uint32_t bw = uint32_t(ng) * 128u * 4u, bs = uint32_t(ng) * 128u * uint32_t(sizeof(Src));
+    mbar_arm(&s_mbar[2], bw + bs);
+    if (ng) {
+      const int64_t blk = int64_t(rank) * g_max * 128;  // the tile's first element
+      bulk_load(s_w, d.cl_w + blk, bw, &s_mbar[2]);
+      bulk_load(s_src, static_cast<const Src*>(d.cl_src) + blk, bs, &s_mbar[2]);
     }
   }
   const NeuronParams prm_u = load_params<KIND, USE_REF>(d.neuron, 0);
@@ -231,7 +229,6 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
   // (words - NWv) words per sample.  Armed for steps 0 and 1 here; after the
   // wait for step s - 1, for step s + 1 -- before this CTA publishes step s,
   // which every sender of step s + 1 has to have received first.
-  __shared__ __align__(8) uint64_t s_mbar[2];
   // a wait gave up somewhere in the cluster: every CTA stops waiting and
   // publishing, runs out its loop and meets the others at the final barrier
   __shared__ int s_dead;
@@ -247,6 +244,20 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
   }
   const unsigned spin = d.spin_limit > 0 ? unsigned(d.spin_limit) : kClDefaultSpinLimit;
   cluster.sync();  // every CTA resident, its bitmaps zeroed and barriers armed before the first remote store
+  // the in-edges have landed (bounded wait by one thread; then every thread's
+  // own acquire of the completed phase)
+  if (threadIdx.x == 0) {
+    unsigned polls = 0;
+    while (!mbar_done(&s_mbar[2], 0)) {
+      if (++polls > spin) {
+        if (d.tile_work) atomicCAS(d.tile_work + 2, 0, BT_ERR_TIMEOUT);
+        for (int r = 0; r < CL; ++r) *reinterpret_cast<volatile int*>(cluster.map_shared_rank(&s_dead, r)) = 1;
+        break;
+      }
+    }
+  }
+  __syncthreads();
+  if (!*dead) (void)mbar_done(&s_mbar[2], 0);
 
   const int items = NWv * B;  // (word, sample) pairs of this tile; item it = (b, w) = divmod(it, NWv)
   int h_t = int(d.t0 % H);

@@ -1505,9 +1505,12 @@ int engine_check(const bt_engine_desc* d) {
                  "n_tiles=%d x tile_posts=%d does not tile n=%lld", d->n_tiles, d->tile_posts, (long long)d->n);
     BT_CHECK_ARG(d->batch <= 256 && d->batch * d->n < (int64_t(1) << 31), "tile mode: batch <= 256, batch * n < 2^31");
   } else if (d->mode == BT_MODE_CLUSTER) {
-    BT_CHECK_ARG(d->sl_ptr && d->sl_src && d->sl_w, "cluster mode needs the sliced in-edge view");
+    BT_CHECK_ARG(d->cl_w && d->cl_src && d->cl_gptr, "cluster mode needs the packed in-edges cl_w / cl_src / cl_gptr");
+    BT_CHECK_ARG(((reinterpret_cast<uintptr_t>(d->cl_w) | reinterpret_cast<uintptr_t>(d->cl_src)) & 15) == 0,
+                 "cl_w and cl_src must be 16-byte aligned (bulk copies)");
     BT_CHECK_ARG(d->n_bins == 1, "cluster mode has no synaptic delays");
-    BT_CHECK_ARG(d->tile_rows >= 0 && d->tile_rows < (int64_t(1) << 26), "tile_rows=%lld", (long long)d->tile_rows);
+    BT_CHECK_ARG(d->tile_rows >= 0 && d->tile_rows % 16 == 0 && d->tile_rows < (int64_t(1) << 24),
+                 "tile_rows=%lld must be a multiple of 16", (long long)d->tile_rows);
     BT_CHECK_ARG(n_rec(*d) == 1, "cluster mode has no receptor channels");
     BT_CHECK_ARG(d->tile_posts > 0 && (d->tile_posts & 31) == 0, "tile_posts=%d must be a positive multiple of 32",
                  d->tile_posts);

@@ -36,6 +36,7 @@ from .synapse import DelayedPSC, ExponentialPSC, HeterSynapsePSC, receptor_sum
 DEFAULT_CHUNK = 512
 DENSE_FRACTION = 4  # scatter steps with at least n / DENSE_FRACTION spiking neurons are pulled densely
 DEFAULT_GRAPH_CHUNK = 128  # steps per captured chunk (rounded to a multiple of the slot period)
+CLUSTER_CHUNK = 1024  # the most steps per chunk (and launch) of the single-cluster engine
 MAX_RECEPTORS = 16  # receptor channels per neuron the kernels take (bt_engine_desc.n_rec)
 
 
@@ -201,6 +202,58 @@ def cluster_shape(n: int, batch: int, sl_ptr, ctas: int = 0):
             if got is not None and (not big_tiles or got[0] >= 128 or cl == 1):
                 return got
     return None
+
+
+def cluster_pack_index(lay, n: int, tp: int, P: int, rows: int, dev):
+    """Where the cluster engine's packed in-edge arrays take their elements
+    from: for tile t, group g, lane l, u, the flat index into the sliced view
+    of row 4 g + u of the tile's slice holding (g, l), or -1 on padding
+    ([P][rows / 4][32][4], int64 on `dev`); and the tiles' slice group
+    offsets ([P][tp / 32 + 1] int32 on `dev`).  Built once per layout and
+    shape (kept on the layout)."""
+    import numpy as np
+
+    cache = getattr(lay, "cluster_pack", None)
+    if cache is None:
+        cache = lay.cluster_pack = {}
+    key = (tp, P, rows, str(dev))
+    if key in cache:
+        return cache[key]
+    sl_ptr = np.asarray(lay.slices_ptr_host, dtype=np.int64)
+    n_sl = len(sl_ptr) - 1
+    G, NW = rows // 4, tp // 32
+    idx = np.full((P, G, 32, 4), -1, np.int64)
+    gptr = np.zeros((P, NW + 1), np.int32)
+    g_, l_, u_ = np.meshgrid(np.arange(G), np.arange(32), np.arange(4), indexing="ij")
+    for t in range(P):
+        tile_n = min(tp, n - t * tp)
+        acc = 0
+        for w in range((tile_n + 31) // 32):
+            s_ = t * NW + w
+            r0, nr = int(sl_ptr[s_]), int(sl_ptr[s_ + 1] - sl_ptr[s_])
+            ng = -(-nr // 16) * 4
+            gptr[t, w] = acc
+            row = g_[:ng] * 4 + u_[:ng]
+            idx[t, acc:acc + ng] = np.where(row < nr, (r0 + row) * 32 + l_[:ng], -1)
+            acc += ng
+        gptr[t, (tile_n + 31) // 32:] = acc
+    assert n_sl >= (n + 31) // 32
+    out = (torch.from_numpy(idx.reshape(-1)).to(dev), torch.from_numpy(gptr.reshape(-1)).to(dev))
+    cache[key] = out
+    return out
+
+
+def cluster_pack(sl, sl_w: torch.Tensor, index: torch.Tensor, n: int):
+    """The packed weights (fp32) and ids (id XOR 31, padding n XOR 31; int16
+    bits when n + 32 <= 65536, else int32) of the cluster engine."""
+    valid = index >= 0
+    at = index.clamp(min=0)
+    w = torch.where(valid, sl_w.reshape(-1).index_select(0, at), torch.zeros((), device=sl_w.device))
+    ids = (sl.sl_src.reshape(-1).index_select(0, at) & ((1 << L.BT_BIN_SHIFT) - 1)) ^ 31
+    ids = torch.where(valid, ids, torch.full((), n ^ 31, dtype=ids.dtype, device=ids.device))
+    if n + 32 <= 65536:
+        ids = torch.where(ids >= 32768, ids - 65536, ids).to(torch.int16)
+    return w.contiguous(), ids.contiguous()
 
 
 def slices_of(lay, dev):
@@ -374,6 +427,10 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
     mode = choice.mode
 
     use_graph = bool(getattr(rnn, "cudagraph", False))
+    if mode == L.BT_MODE_CLUSTER and chunk is None:
+        # one launch per chunk, each loading the tiles' in-edges into shared
+        # memory: longer chunks, while the chunk's input buffers stay small
+        chunk = max(DEFAULT_GRAPH_CHUNK, min(CLUSTER_CHUNK, (64 << 20) // max(1, 4 * B * max(n, c_in))))
     if use_graph:
         H = graph_hist_len(R)
         K = graph_chunk(R, chunk)
@@ -473,10 +530,13 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         shape = cluster_shape(n, B, lay.slices_ptr_host, choice.tile_posts)
         if shape is None:
             raise NotImplementedError("cluster mode: the network does not fit one cluster's shared memory")
-        sl_w = static("sl_w", pack_slice_weights(sl, w))
+        tp_c, P_c, rows_c = shape
+        index, gptr = cluster_pack_index(lay, n, tp_c, P_c, rows_c, dev)
+        cl_w, cl_src = cluster_pack(sl, pack_slice_weights(sl, w), index, n)
+        cl_w, cl_src = static("cl_w", cl_w), static("cl_src", cl_src)
         tile_ws = alloc("tile_work", (32,), torch.int32, zero=True)  # word 2: status (a wait that gave up)
-        keep += [sl_w, tile_ws]
-        desc.sl_ptr, desc.sl_src, desc.sl_w = sl.sl_ptr.data_ptr(), sl.sl_src.data_ptr(), sl_w.data_ptr()
+        keep += [cl_w, cl_src, gptr, tile_ws]
+        desc.cl_w, desc.cl_src, desc.cl_gptr = cl_w.data_ptr(), cl_src.data_ptr(), gptr.data_ptr()
         desc.tile_posts, desc.n_tiles, desc.tile_rows = shape
         desc.tile_work = tile_ws.data_ptr()
         desc.spin_limit = int(getattr(rnn, "engine_spin_limit", 0))

@@ -51,7 +51,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 9
+#define BT_ABI_VERSION 10
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -397,15 +397,28 @@ typedef struct bt_engine_desc {
   int32_t spin_limit;
   /* cluster mode (BT_MODE_CLUSTER, no counterpart in the reference): rank t
      of the cluster owns posts [t * tile_posts, (t + 1) * tile_posts), n_tiles
-     <= 16 CTAs cover n; the in-edges come from the sliced view sl_ptr /
-     sl_src / sl_w (one launch per call, no final launch, no ring).
-     tile_rows: the most SELL-32 rows of any tile's slices, which sizes the
-     shared memory (a tile with more rows has its excess ignored) */
+     <= 16 CTAs cover n (one launch per call, no final launch, no ring).  The
+     tiles' in-edges are packed as the kernel keeps them in shared memory and
+     copied there with one bulk copy per array:
+       tile_rows  rows per tile (the SELL-32 rows of its slices, each slice
+                  rounded up to a multiple of 16), a multiple of 16;
+       cl_w       [n_tiles][tile_rows / 4][32][4] fp32: group g, lane l, u =
+                  the weight of row 4 g + u of lane l's post, 0 on padding;
+       cl_src     the same shape, the presynaptic id XOR 31 (padding: n XOR
+                  31), uint16 when n + 32 <= 65536, else uint32;
+       cl_gptr    [n_tiles][tile_posts / 32 + 1] int32: the first group of each
+                  of the tile's 32-post slices, then the tile's group count;
+     all three 16-byte aligned.  tile_work: 32 int32 words, word 2 the status
+     (nonzero after a wait gave up), zero before the call. */
   int64_t tile_rows;
+  const float* cl_w;
+  const void* cl_src;
+  const int32_t* cl_gptr;
 } bt_engine_desc;
 
 /* Cluster mode shared memory per CTA (0 for a bad shape): n neurons, a
-   tile of tile_posts posts (a multiple of 32) holding tile_rows slice rows. */
+   tile of tile_posts posts (a multiple of 32) holding tile_rows slice rows
+   (a multiple of 16). */
 BT_API int64_t bt_cluster_smem_bytes(int64_t n, int64_t batch, int32_t tile_posts, int64_t tile_rows);
 
 /* Tile mode scratch words and shared memory bytes per CTA for a shape

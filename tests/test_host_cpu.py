@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
     for s in syms:
         assert hasattr(lib, s), s
     assert set(syms) == set(L.exported_symbols())
-    assert lib.bt_abi_version() == L.ABI_VERSION == 9
+    assert lib.bt_abi_version() == L.ABI_VERSION == 10
 
 
 def test_layout_matches_numpy_reference():
@@ -363,3 +363,45 @@ def test_cluster_mode_is_a_candidate_unless_scatter_is_asked_for():
     conn.sparse_config.deterministic = False
     conn.sparse_config.direction = "scatter"
     assert L.BT_MODE_CLUSTER not in autotune.allowed_modes(conn, 8)
+
+
+@pytest.mark.parametrize("n,tp", [(300, 32), (1000, 128), (4096, 256)])
+def test_cluster_packing_holds_every_in_edge_in_order(n, tp):
+    """The cluster engine's packed in-edges, read back the way the kernel
+    walks them (tile, slice, lane: groups of 4 rows in order), list every
+    post's in-edges in ascending canonical order, with id XOR 31 and the
+    weight, and only padding (id n, weight 0) after them."""
+    from btorch_b200.models import SparseConn
+    from btorch_b200.models._ops import pack_slice_weights
+    from btorch_b200.models.engine import cluster_pack, cluster_pack_index, cluster_shape, slices_of
+
+    rng = np.random.default_rng(n)
+    dense = (rng.random((n, n)) < min(0.03, 80.0 / n)) * rng.normal(0, 1, (n, n))
+    conn = SparseConn(sp.coo_array(dense.astype(np.float32)))
+    lay = conn.engine_layout(1, 0, "cpu")
+    sl = slices_of(lay, "cpu")
+    shape = cluster_shape(n, 1, lay.slices_ptr_host, ctas=-(-n // tp))
+    assert shape is not None and shape[0] == tp
+    tp, P, rows = shape
+    index, gptr = cluster_pack_index(lay, n, tp, P, rows, "cpu")
+    w = conn._edge_weight().detach().float().contiguous()
+    cl_w, cl_src = cluster_pack(sl, pack_slice_weights(sl, w), index, n)
+    G = rows // 4
+    cw = cl_w.numpy().reshape(P, G, 32, 4)
+    cs = cl_src.numpy().astype(np.int64).reshape(P, G, 32, 4) & 0xFFFF if n + 32 <= 65536 else None
+    gp = gptr.numpy().reshape(P, tp // 32 + 1)
+    csc = dense.T  # [post, pre]
+    for t in range(P):
+        for s_ in range((min(tp, n - t * tp) + 31) // 32):
+            for ln in range(32):
+                post = t * tp + s_ * 32 + ln
+                got_ids = (cs[t, gp[t, s_]:gp[t, s_ + 1], ln, :].reshape(-1) ^ 31)
+                got_w = cw[t, gp[t, s_]:gp[t, s_ + 1], ln, :].reshape(-1)
+                if post >= n:
+                    assert (got_ids == n).all()
+                    continue
+                pres = np.nonzero(csc[post])[0]
+                k = len(pres)
+                np.testing.assert_array_equal(got_ids[:k], pres)
+                np.testing.assert_array_equal(got_w[:k], csc[post, pres].astype(np.float32))
+                assert (got_ids[k:] == n).all() and (got_w[k:] == 0).all()
