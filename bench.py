@@ -658,10 +658,11 @@ def raster_bits(raster, n):
     return np.unpackbits(np.ascontiguousarray(r).view(np.uint8), axis=-1, bitorder="little")[..., :n]
 
 
-def engine_window(cfg, net, x, lens, dev, direction, steps, trace_v=False, cudagraph=True):
-    """A fresh model of the workload run for `steps` steps on x[:steps].
-    Returns (spikes uint8 [steps, B, n], final state dict of numpy arrays,
-    v trace or None, the model's delivery direction)."""
+def engine_window(cfg, net, x, lens, dev, direction, steps, trace_v=False, cudagraph=True, choice=None):
+    """A fresh model of the workload run for `steps` steps on x[:steps]
+    (`choice`: a parse_choice string pinning the delivery mode, else the
+    tuner's).  Returns (spikes uint8 [steps, B, n], final state dict of numpy
+    arrays, v trace or None, the model's delivery direction and mode)."""
     from btorch_b200.models import environ
     from btorch_b200.models import engine as E
 
@@ -671,14 +672,15 @@ def engine_window(cfg, net, x, lens, dev, direction, steps, trace_v=False, cudag
         rnn.update_state_names = ("neuron.v",)
     sl = None if lens is None else lens.clamp(max=steps)
     with torch.inference_mode(), environ.context(dt=1.0):
-        raster, st = rnn(x[:steps].contiguous(), sample_len=sl, spikes_out="bitmask")
+        raster, st = rnn(x[:steps].contiguous(), sample_len=sl, spikes_out="bitmask",
+                         engine_choice=parse_choice(choice))
     plan, _ = E.match(rnn)
     final = {"v": rnn.neuron.v, "psc": plan.psc_mod.psc, "ref": rnn.neuron.refractory}
     if cfg["model"] == "alif_dense_input":
         final["gk"] = rnn.neuron.g_k
     final = {k: t.reshape(t.shape[0], -1).cpu().numpy() for k, t in final.items()}
     vtr = st["neuron.v"].cpu().numpy() if trace_v else None
-    direction = rnn.last_engine_direction
+    direction = f"{rnn.last_engine_direction} ({rnn.last_engine_choice.describe()['mode']})"
     del rnn
     return raster_bits(raster, cfg["n"]), final, vtr, direction
 
@@ -717,11 +719,11 @@ def _sample_divergence(a, b):
     return np.where(bad.any(0), bad.argmax(0), T)
 
 
-def parity_bitwise(name, cfg, net, x, lens, dev, steps, direction):
+def parity_bitwise(name, cfg, net, x, lens, dev, steps, direction, choice=None):
     """Rasters of every step and the final state bit for bit (dyadic
     weights, or an ordered delivery mode)."""
     t0 = time.perf_counter()
-    z, fin, _, used = engine_window(cfg, net, x, lens, dev, direction, steps)
+    z, fin, _, used = engine_window(cfg, net, x, lens, dev, direction, steps, choice=choice)
     oz, ofin, _ = oracle_window(cfg, net, x.cpu().numpy() if torch.is_tensor(x) else x, steps,
                                 None if lens is None else lens.cpu().numpy())
     k = first_divergence(z, oz)
@@ -1109,14 +1111,18 @@ def main():
                                    "sample": f"all {ecfg['t_max']} steps ({t:.2f} s)", "ms_per_step": 1e3 * t / ecfg["t_max"]}
             if checks:
                 # the port forms W z over every synapse in the reference's order;
-                # the timed run sums non-dyadic weights in arrival order
+                # the timed run is the tuner's mode (the single-cluster engine on
+                # this workload sums in that order too; the scatter would not)
                 parity[f"{extra}_timed_vs_port_raster_equal_steps"] = first_divergence(
                     raster_bits(raster, ecfg["n"]), z_port)
         del raster
         del m
         torch.cuda.empty_cache()
         if checks and ecfg["model"] == "lif_plain":
-            parity[f"{extra}_gather"] = parity_bitwise(extra, ecfg, ne, xe, le, dev, ecfg["t_max"], "gather")
+            parity[f"{extra}_gather"] = parity_bitwise(extra, ecfg, ne, xe, le, dev, ecfg["t_max"], "gather",
+                                                       choice="gather")
+            parity[f"{extra}_cluster"] = parity_bitwise(extra, ecfg, ne, xe, le, dev, ecfg["t_max"], "gather",
+                                                        choice="cluster")
             parity[f"{extra}_scatter"] = parity_tolerance(extra, ecfg, ne, xe, le, dev, ecfg["t_max"], "scatter")
         if checks and ecfg["model"] == "lif_hetero_delay":
             parity[f"{extra}_200"] = parity_bitwise(extra, ecfg, ne, xe, le, dev, min(200, ecfg["t_max"]),

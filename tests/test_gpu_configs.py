@@ -5,7 +5,8 @@ per-synapse chain; pinned in tests/test_oracle_golden.py).
 
   plain       LIF N 4096, p 0.02, lognormal E/I weights, 1000 Poisson
               channels through a dense input layer, batch 1, T 1000: the
-              ordered gather bit for bit over all 1000 steps; the scatter
+              ordered gather and the single-cluster engine bit for bit over
+              all 1000 steps; the scatter
               (arrival-order sums of non-dyadic weights) within rel 1e-5
               until the first spike divergence.
   connectome  LIF N 140000, 48.8M synapses (dyadic counts x 2^-6), delays
@@ -36,9 +37,13 @@ def _workload(name, steps):
     return cfg, net, x, lens
 
 
-def test_plain_gather_bitwise_all_steps():
+@pytest.mark.parametrize("mode", ["gather", "cluster"])
+def test_plain_ordered_modes_bitwise_all_steps(mode):
+    """The warp-per-post gather and the single-cluster engine (the tuner's
+    choice for this workload), each over all 1000 steps."""
     cfg, net, x, lens = _workload("plain", 1000)
-    r = bench.parity_bitwise("plain", cfg, net, x, lens, DEV, 1000, "gather")
+    r = bench.parity_bitwise("plain", cfg, net, x, lens, DEV, 1000, "gather", choice=mode)
+    assert r["direction"] == f"gather ({mode})", r
     assert r["spikes"] > 0
     assert r["check"] == "bitwise", r
 
@@ -53,7 +58,7 @@ def test_plain_scatter_within_tolerance_until_divergence():
 def test_connectome_scatter_bitwise_first_200_steps():
     cfg, net, x, lens = _workload("connectome", 200)
     r = bench.parity_bitwise("connectome", cfg, net, x, lens, DEV, 200, "scatter")
-    assert r["direction"] == "scatter"
+    assert r["direction"].startswith("scatter")
     assert r["spikes"] > 1000
     assert r["check"] == "bitwise", r
 
