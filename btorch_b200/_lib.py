@@ -26,7 +26,7 @@ _i64 = C.c_int64
 _i32 = C.c_int32
 
 
-ABI_VERSION = 10  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
+ABI_VERSION = 11  # BT_ABI_VERSION of include/btorch_b200.h the structures below mirror
 
 
 class BtParam(C.Structure):
@@ -95,7 +95,7 @@ _PROTOS = {
     "bt_masks_to_float": (C.c_int, [_i64, _i64, _vp, _vp, _vp]),
     "bt_tile_work_words": (C.c_int64, [_i64, _i32, _i32]),
     "bt_tile_smem_bytes": (C.c_int64, [_i64, _i32, _i32]),
-    "bt_cluster_smem_bytes": (C.c_int64, [_i64, _i64, _i32, _i64]),
+    "bt_cluster_smem_bytes": (C.c_int64, [_i64, _i64, _i32, _i64, _i32]),
     "bt_tile_offsets": (C.c_int, [_i64, _vp, _vp, _i32, _i32, _vp, _vp]),
     "bt_input_grad_weight": (C.c_int, [_i64, _i64, _i64, _vp, _vp, _vp, _i32, _vp, _vp]),
 }

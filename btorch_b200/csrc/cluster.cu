@@ -1,5 +1,5 @@
-// Single-cluster persistent engine (BT_MODE_CLUSTER) for small networks
-// without synaptic delays: every step of a call in ONE launch of one
+// Single-cluster persistent engine (BT_MODE_CLUSTER) for small networks,
+// with or without synaptic delay bins: every step of a call in ONE launch of one
 // thread-block cluster of up to 16 CTAs, the step of btorch/models/rnn.py:
 // 517-528 repeated over time (rnn.py:200-332).
 //
@@ -9,22 +9,29 @@
 //   - its tile's in-edges, the SELL-32 slices of the CSC (lane = post, the
 //     k-th in-edge of each post in row k, ascending canonical order), the
 //     presynaptic id stored as id ^ 31 (16 bits when n + 32 <= 2^16);
-//   - two copies of the whole network's spike bitmap ([2][batch][words + 1],
-//     the last word of each sample zero: the slices' padding points there).
+//   - copies of the whole network's spike bitmap ([copies][batch][words + 1],
+//     the last word of each sample zero: the slices' padding points there),
+//     step k in copy k mod copies: 2 copies, or R + 1 with R delay bins
+//     (bin b of step k reads the spikes of step k - 1 - b).
 // Per step k, each warp takes (32-post word of the tile, sample):
-//   synapse   P = decay(P) + sum over the post's in-edges in ascending order
-//             of w * z_{k-1}[pre] (the bitmap of step k - 1, local), the
+//   synapse   P = decay(P) + sum over the post's in-edges (pre, bin) in
+//             ascending order of w * z_{k-1-bin}[pre] (local bitmaps), the
 //             fp32 chain of the gather engine: the reference's rounding for
 //             ANY weights, not only dyadic ones;
 //   neuron    I = P + x, LIF/ALIF update, the spike word by ballot;
-//   publish   the word into bitmap copy k mod 2 of every other CTA of the
+//   publish   the word into bitmap copy k mod copies of every other CTA of the
 //             cluster (st.async, one lane per CTA, its bytes counted on the
 //             receiver's mbarrier for that copy) and of its own (plain store).
-// Then thread 0 waits (bounded) for the copy's barrier phase and the CTA
-// synchronises: every word of step k is in this CTA's copy.  Double-buffered
-// copies need no cluster-wide barrier: a CTA arms a copy's barrier for step
-// s + 1 right after its wait for step s - 1 and before it publishes step s,
-// which every sender of step s + 1 has to have received first.
+// Then thread 0 waits (bounded) for the barrier phase of the step (two
+// mbarriers, by step parity) and the CTA synchronises: every word of step k
+// is in this CTA's copy.  No cluster-wide barrier: a CTA arms a barrier for
+// step s + 1 right after its wait for step s - 1 and before it publishes step
+// s, which every sender of step s + 1 has to have received first; and a copy
+// is overwritten (step k into the copy of step k - copies) only by a sender
+// that has received every CTA's step k - 1, published after that CTA's last
+// read of the copy (its step k - 1 reads steps k - 2 .. k - 1 - R).  With
+// delay bins the copies of the call's first steps' history come from the
+// history ring (d.hist) at the start.
 // After the last step the launch applies the synapse update of that step
 // (the gather engine's final launch) and writes the state back: one launch
 // per call, nothing per step in global memory but the input read and the
@@ -47,7 +54,7 @@ constexpr int kClMaxCtas = 16;
 
 // Shared-memory carve-up of one CTA (bytes, every part 16-byte aligned):
 // state [4][B][Tp] f32 | edge weights [rows][32] f32 | presynaptic ids
-// [rows][32] (u16 when src16, else u32) | bitmaps [2][B][Wd] u32 | slice
+// [rows][32] (u16 when src16, else u32) | bitmaps [copies][B][Wd] u32 | slice
 // group offsets [NW + 1] i32 | sample lengths [B] i32 | out-degrees [Tp] i32.
 // rows: the tile's slice rows, each slice rounded up to a multiple of kClRows
 // and stored as groups of 4 rows per lane ([group][lane][4]), so that one
@@ -60,15 +67,24 @@ __host__ __device__ __forceinline__ size_t cl_align16(size_t x) { return (x + 15
 
 __host__ __device__ __forceinline__ bool cluster_src16(int64_t n) { return n + 32 <= 65536; }
 
+// Presynaptic id encodings (template IDS): 0 = pre ^ 31 in 16 bits (no
+// delay bins, n + 32 <= 2^16), 1 = the same in 32 bits, 2 = (pre ^ 31) in
+// bits 0..19 and the delay bin in bits 20..24 (n + 32 <= 2^20, R <= 32).
+constexpr int kClBinShift = 20;
+__host__ __device__ __forceinline__ int cluster_ids(int64_t n, int n_bins) {
+  return n_bins > 1 ? 2 : cluster_src16(n) ? 0 : 1;
+}
+__host__ __device__ __forceinline__ int cluster_copies(int n_bins) { return n_bins > 1 ? n_bins + 1 : 2; }
+
 __host__ __device__ __forceinline__ ClusterSmem cluster_smem(int64_t n, int64_t batch, int tp, int64_t rows,
-                                                            bool src16) {
+                                                            bool src16, int copies) {
   ClusterSmem s;
   const int64_t wd = ((n + 31) >> 5) + 1;
   s.state = 0;
   s.w = cl_align16(sizeof(float) * 4 * size_t(batch) * tp);
   s.src = s.w + cl_align16(sizeof(float) * size_t(rows) * 32);
   s.bits = s.src + cl_align16((src16 ? 2 : 4) * size_t(rows) * 32);
-  s.gptr = s.bits + cl_align16(sizeof(uint32_t) * 2 * size_t(batch) * size_t(wd));
+  s.gptr = s.bits + cl_align16(sizeof(uint32_t) * size_t(copies) * size_t(batch) * size_t(wd));
   s.len = s.gptr + cl_align16(sizeof(int32_t) * size_t(tp / 32 + 1));
   s.deg = s.len + cl_align16(sizeof(int32_t) * size_t(batch));
   s.total = s.deg + cl_align16(sizeof(int32_t) * size_t(tp));
@@ -156,8 +172,9 @@ struct SrcGroup<false> {
   }
 };
 
-template <int KIND, bool HARD, bool USE_REF, bool FAST, bool SRC16>
+template <int KIND, bool HARD, bool USE_REF, bool FAST, int IDS>
 __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc d) {
+  constexpr bool SRC16 = IDS == 0, DELAY = IDS == 2;
   extern __shared__ __align__(16) unsigned char cl_smem[];
   using Src = typename std::conditional<SRC16, uint16_t, uint32_t>::type;
   using G4 = typename SrcGroup<SRC16>::T;
@@ -173,7 +190,9 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
   const int tile_n = int(p0 + Tp <= n ? Tp : (p0 < n ? n - p0 : 0));  // posts of this tile
   const int NWv = (tile_n + 31) >> 5;                                  // its words
   const int w0 = int(p0 >> 5);                                         // its first word
-  const ClusterSmem L = cluster_smem(n, B, Tp, d.tile_rows, SRC16);
+  const int R = DELAY ? d.n_bins : 1;
+  const int Hc = DELAY ? R + 1 : 2;  // bitmap copies
+  const ClusterSmem L = cluster_smem(n, B, Tp, d.tile_rows, SRC16, Hc);
   const int g_max = int(d.tile_rows >> 2);  // groups of 4 rows the shared memory holds
   float* s_v = reinterpret_cast<float*>(cl_smem + L.state);
   float* s_psc = s_v + B * Tp;
@@ -200,7 +219,18 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
     s_ref[q] = (in && USE_REF) ? d.refractory[g] : 0.0f;
     s_gk[q] = (in && KIND == BT_NEURON_ALIF) ? d.g_k[g] : 0.0f;
   }
-  for (int q = threadIdx.x; q < 2 * B * Wd; q += kClThreads) s_bits[q] = 0u;
+  // bitmaps: zero, but for the copies of the steps before the call that
+  // delay bins read (steps -1 .. -(R - 1) in copies Hc - 1 .. Hc - R + 1),
+  // which come from the history ring
+  for (int q = threadIdx.x; q < Hc * B * Wd; q += kClThreads) {
+    const int c = q / (B * Wd), rem = q - c * (B * Wd);
+    const int b = rem / Wd, wi = rem - b * Wd;
+    const int j = Hc - c;  // the copy of step -j
+    uint32_t word = 0u;
+    if (DELAY && j >= 1 && j <= R - 1 && wi < words)
+      word = uint32_t(d.hist[(((d.t0 - j) % H) * B + b) * words + wi]);
+    s_bits[q] = word;
+  }
   for (int q = threadIdx.x; q < B; q += kClThreads)
     s_len[q] = d.sample_len ? int(min(int64_t(d.sample_len[q]), int64_t(INT32_MAX))) : INT32_MAX;
   for (int l = threadIdx.x; l < Tp; l += kClThreads) s_deg[l] = (d.outdeg && l < tile_n) ? d.outdeg[p0 + l] : 0;
@@ -268,9 +298,10 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
     return (d.x && kk < d.n_steps && l < tile_n && kk < s_len[b]) ? __ldcs(d.x + (kk * B + b) * n + p0 + l) : 0.0f;
   };
   if (warp < items) x_ahead = drive(0, warp);
+  int kc = 0, kp = Hc - 1;  // the copies of steps k and k - 1
   for (int64_t k = 0; k <= d.n_steps; ++k) {
     const bool last = k == d.n_steps;  // only the synapse update of step n_steps - 1
-    const int cur = int(k & 1), prv = cur ^ 1;
+    const int cur = int(k & 1), prv = cur ^ 1;  // mbarriers by step parity
     if (k > 0) {
       // z_{k-1}: every CTA's words of step k - 1 in copy prv
       if (threadIdx.x == 0 && !*dead) {
@@ -299,8 +330,8 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
       const float xv = it == warp ? x_ahead : drive(k, it);
       float P = s_psc[q];
       if (k > 0 && k - 1 < len) {
-        // ordered in-edge sum over z_{k-1} (zero terms skipped: exact)
-        const uint32_t* bits = s_bits + (prv * B + b) * Wd;
+        // ordered in-edge sum over z_{k-1-bin} (zero terms skipped: exact)
+        const uint32_t* bits = s_bits + (kp * B + b) * Wd;
         const G4* srcg = reinterpret_cast<const G4*>(s_src);
         const float4* wg = reinterpret_cast<const float4*>(s_w);
         float g = 0.0f;
@@ -322,7 +353,14 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
           }
 #pragma unroll
           for (int u = 0; u < kClRows; ++u) {
-            const uint32_t bw = bits[sr[u] >> 5];
+            uint32_t bw;
+            if constexpr (DELAY) {
+              int c = kp - int(sr[u] >> kClBinShift);  // the copy of step k - 1 - bin
+              c += c < 0 ? Hc : 0;
+              bw = s_bits[(c * B + b) * Wd + ((sr[u] & ((1u << kClBinShift) - 1u)) >> 5)];
+            } else {
+              bw = bits[sr[u] >> 5];
+            }
             rot[u] = __funnelshift_l(bw, bw, sr[u]);
           }
 #pragma unroll
@@ -364,7 +402,7 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
       }
       const uint32_t word = __ballot_sync(0xffffffffu, s != 0.0f);
       // publish: lane c stores the word into CTA c's copy (c = rank: its own)
-      const int off = (cur * B + b) * Wd + w0 + w;
+      const int off = (kc * B + b) * Wd + w0 + w;
       if (lane == rank) s_bits[off] = word;
       else if (lane < CL && !*dead) st_async_word(cluster_addr(s_bits + off, lane), word, cluster_addr(&s_mbar[cur], lane));
       if (s != 0.0f) {
@@ -381,7 +419,7 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
       st_un = st_ed = 0;
       for (int l = threadIdx.x; l < tile_n; l += kClThreads) {
         uint32_t any = 0u;
-        for (int b = 0; b < B; ++b) any |= s_bits[(cur * B + b) * Wd + w0 + (l >> 5)];
+        for (int b = 0; b < B; ++b) any |= s_bits[(kc * B + b) * Wd + w0 + (l >> 5)];
         if ((any >> (l & 31)) & 1u) {
           st_un += 1;
           st_ed += s_deg[l];
@@ -394,7 +432,7 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
     for (int it = warp; it < items; it += W) {
       const int b = it / NWv, w = it - b * NWv;
       if (lane == 0) {
-        const uint32_t word = s_bits[(cur * B + b) * Wd + w0 + w];  // this warp's own store
+        const uint32_t word = s_bits[(kc * B + b) * Wd + w0 + w];  // this warp's own store
         if (hist) d.hist[(int64_t(h_t) * B + b) * words + w0 + w] = word;
         if (d.raster) d.raster[(k * B + b) * words + w0 + w] = word;
       }
@@ -415,6 +453,8 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
     }
     if (warp < items) x_ahead = drive(k + 1, warp);
     h_t = h_t + 1 == H ? 0 : h_t + 1;
+    kp = kc;
+    kc = kc + 1 == Hc ? 0 : kc + 1;
   }
   // every remote store into this CTA was waited for (the last iteration's
   // wait covers the last step); the barrier keeps every CTA resident until
@@ -431,11 +471,11 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
   }
 }
 
-template <int KIND, bool HARD, bool USE_REF, bool FAST, bool SRC16>
+template <int KIND, bool HARD, bool USE_REF, bool FAST, int IDS>
 int cluster_launch(const bt_engine_desc& d, cudaStream_t s) {
-  void (*kern)(bt_engine_desc) = k_cluster_engine<KIND, HARD, USE_REF, FAST, SRC16>;
+  void (*kern)(bt_engine_desc) = k_cluster_engine<KIND, HARD, USE_REF, FAST, IDS>;
   const int CL = d.n_tiles;
-  const size_t smem = cluster_smem(d.n, d.batch, d.tile_posts, d.tile_rows, SRC16).total;
+  const size_t smem = cluster_smem(d.n, d.batch, d.tile_posts, d.tile_rows, IDS == 0, cluster_copies(d.n_bins)).total;
   int dev = 0;
   cudaGetDevice(&dev);
   const bool known = launch_setup_known(reinterpret_cast<const void*>(kern), dev, smem, CL);
@@ -471,11 +511,14 @@ int cluster_launch(const bt_engine_desc& d, cudaStream_t s) {
 
 template <int KIND, bool HARD, bool USE_REF>
 int cluster_pick(const bt_engine_desc& d, bool fast, cudaStream_t s) {
-  const bool src16 = cluster_src16(d.n);  // ids 0..n (n: the padding) stored as id ^ 31 in 16 bits
-  if (fast) return src16 ? cluster_launch<KIND, HARD, USE_REF, true, true>(d, s)
-                         : cluster_launch<KIND, HARD, USE_REF, true, false>(d, s);
-  return src16 ? cluster_launch<KIND, HARD, USE_REF, false, true>(d, s)
-               : cluster_launch<KIND, HARD, USE_REF, false, false>(d, s);
+  switch (cluster_ids(d.n, d.n_bins)) {  // the encoding the packed ids were written in
+    case 0:
+      return fast ? cluster_launch<KIND, HARD, USE_REF, true, 0>(d, s) : cluster_launch<KIND, HARD, USE_REF, false, 0>(d, s);
+    case 1:
+      return fast ? cluster_launch<KIND, HARD, USE_REF, true, 1>(d, s) : cluster_launch<KIND, HARD, USE_REF, false, 1>(d, s);
+    default:
+      return fast ? cluster_launch<KIND, HARD, USE_REF, true, 2>(d, s) : cluster_launch<KIND, HARD, USE_REF, false, 2>(d, s);
+  }
 }
 
 int run_cluster(const bt_engine_desc& d, bool fast, cudaStream_t s) {
@@ -494,7 +537,12 @@ int run_cluster(const bt_engine_desc& d, bool fast, cudaStream_t s) {
 
 }  // namespace bt
 
-extern "C" int64_t bt_cluster_smem_bytes(int64_t n, int64_t batch, int32_t tile_posts, int64_t tile_rows) {
-  if (n <= 0 || batch <= 0 || tile_posts <= 0 || (tile_posts & 31) || tile_rows < 0 || (tile_rows & 3)) return 0;
-  return int64_t(bt::cluster_smem(n, batch, tile_posts, tile_rows, bt::cluster_src16(n)).total);
+extern "C" int64_t bt_cluster_smem_bytes(int64_t n, int64_t batch, int32_t tile_posts, int64_t tile_rows,
+                                         int32_t n_bins) {
+  if (n <= 0 || batch <= 0 || tile_posts <= 0 || (tile_posts & 31) || tile_rows < 0 || (tile_rows & 3) ||
+      n_bins < 1 || n_bins > 32 || (n_bins > 1 && n + 32 > (int64_t(1) << bt::kClBinShift)))
+    return 0;
+  return int64_t(bt::cluster_smem(n, batch, tile_posts, tile_rows, bt::cluster_ids(n, n_bins) == 0,
+                                  bt::cluster_copies(n_bins))
+                     .total);
 }

@@ -1508,7 +1508,8 @@ int engine_check(const bt_engine_desc* d) {
     BT_CHECK_ARG(d->cl_w && d->cl_src && d->cl_gptr, "cluster mode needs the packed in-edges cl_w / cl_src / cl_gptr");
     BT_CHECK_ARG(((reinterpret_cast<uintptr_t>(d->cl_w) | reinterpret_cast<uintptr_t>(d->cl_src)) & 15) == 0,
                  "cl_w and cl_src must be 16-byte aligned (bulk copies)");
-    BT_CHECK_ARG(d->n_bins == 1, "cluster mode has no synaptic delays");
+    BT_CHECK_ARG(d->n_bins >= 1 && d->n_bins <= 32 && (d->n_bins == 1 || d->n + 32 <= (int64_t(1) << 20)),
+                 "cluster mode: n_bins=%d (1..32; with delays n + 32 <= 2^20)", d->n_bins);
     BT_CHECK_ARG(d->tile_rows >= 0 && d->tile_rows % 16 == 0 && d->tile_rows < (int64_t(1) << 24),
                  "tile_rows=%lld must be a multiple of 16", (long long)d->tile_rows);
     BT_CHECK_ARG(n_rec(*d) == 1, "cluster mode has no receptor channels");

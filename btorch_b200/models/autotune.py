@@ -53,8 +53,9 @@ class EngineChoice:
 def allowed_modes(conn, batch: int, receptors: int = 1, n_bins: int = 1) -> list[int]:
     """Delivery modes the sparse config admits (the sliced pull has no
     receptor channels: with receptors > 1 it is left out; the tile mode
-    delivers push-wise like scatter, the cluster mode pulls like gather, both
-    without delays or receptor channels)."""
+    delivers push-wise like scatter, without delays or receptor channels; the
+    cluster mode pulls like gather, without receptor channels, up to 32 delay
+    bins)."""
     cfg = conn.sparse_config
     if cfg.deterministic or cfg.direction == "gather":
         modes = [L.BT_MODE_GATHER, L.BT_MODE_PULL]
@@ -73,7 +74,9 @@ def allowed_modes(conn, batch: int, receptors: int = 1, n_bins: int = 1) -> list
         modes.insert(1, L.BT_MODE_CLUSTER)
     modes = [m for m in modes if receptors == 1 or m != L.BT_MODE_PULL]
     if receptors > 1 or n_bins > 1 or batch > 256:
-        modes = [m for m in modes if m not in (L.BT_MODE_TILE, L.BT_MODE_CLUSTER)]
+        modes = [m for m in modes if m != L.BT_MODE_TILE]
+    if receptors > 1 or n_bins > 32 or batch > 256:
+        modes = [m for m in modes if m != L.BT_MODE_CLUSTER]
     return modes
 
 
@@ -101,7 +104,7 @@ def candidates(conn, batch: int, receptors: int = 1, n_bins: int = 1, n: int = 0
             if n and dev is not None:
                 lay = conn.engine_layout(1, 0, dev)
                 slices_of(lay, dev)
-                if cluster_shape(n, batch, lay.slices_ptr_host) is not None:
+                if cluster_shape(n, batch, lay.slices_ptr_host, n_bins=n_bins) is not None:
                     out.append(EngineChoice(mode))
             continue
         if mode == L.BT_MODE_TILE:
@@ -153,8 +156,8 @@ def choose(plan, rnn, x: torch.Tensor, sample_len, run) -> EngineChoice:
     if not plan.conn.sparse_config.autotune or T < TUNE_MIN_STEPS:
         return heuristic(plan.conn, B, plan.n_rec)
     cands = candidates(plan.conn, B, plan.n_rec, plan.n_bins, plan.neuron.size, plan.neuron.v.device)
-    if plan.uniform_delay:  # a DelayedPSC delay: the persistent modes have none
-        cands = [c for c in cands if c.mode not in (L.BT_MODE_TILE, L.BT_MODE_CLUSTER)]
+    if plan.uniform_delay:  # a DelayedPSC delay: the tile mode has none
+        cands = [c for c in cands if c.mode != L.BT_MODE_TILE]
     if len(cands) == 1:
         cache[key] = (cands[0], {})
         return cands[0]

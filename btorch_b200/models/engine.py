@@ -168,12 +168,14 @@ def tile_shape(n: int, batch: int, dev, tile_posts: int = 0):
     return tp, P
 
 
-def cluster_shape(n: int, batch: int, sl_ptr, ctas: int = 0):
+def cluster_shape(n: int, batch: int, sl_ptr, ctas: int = 0, n_bins: int = 1):
     """(tile_posts, n_ctas, tile_rows) of the single-cluster engine, or None
     when the tiles' state and in-edges do not fit one cluster's shared
     memory.  sl_ptr: the sliced in-edge view's slice -> first row offsets
-    (host array).  By default the most CTAs (up to 16) whose tiles hold at
-    least 128 posts, else the most that fit."""
+    (host array; a post's in-edges are the same rows whatever the delay
+    bins).  n_bins: delay bins (1..32), one bitmap copy each in shared memory.
+    By default the most CTAs (up to 16) whose tiles hold at least 128 posts,
+    else the most that fit."""
     import numpy as np
 
     sl_ptr = np.asarray(sl_ptr, dtype=np.int64)
@@ -191,7 +193,8 @@ def cluster_shape(n: int, batch: int, sl_ptr, ctas: int = 0):
         acc = np.concatenate([[0], np.cumsum(slice_rows)])
         starts = np.minimum(np.arange(P + 1) * w, len(acc) - 1)
         rows = int(np.diff(acc[starts]).max(initial=0))
-        if L.lib().bt_cluster_smem_bytes(n, batch, tp, rows) > MAX_TILE_SMEM - 1024:  # + static barriers
+        smem = L.lib().bt_cluster_smem_bytes(n, batch, tp, rows, n_bins)
+        if smem == 0 or smem > MAX_TILE_SMEM - 1024:  # (+ the static barriers)
             return None
         return tp, P, rows
 
@@ -243,14 +246,19 @@ def cluster_pack_index(lay, n: int, tp: int, P: int, rows: int, dev):
     return out
 
 
-def cluster_pack(sl, sl_w: torch.Tensor, index: torch.Tensor, n: int):
+def cluster_pack(sl, sl_w: torch.Tensor, index: torch.Tensor, n: int, n_bins: int = 1):
     """The packed weights (fp32) and ids (id XOR 31, padding n XOR 31; int16
-    bits when n + 32 <= 65536, else int32) of the cluster engine."""
+    bits when n + 32 <= 65536, else int32; with delay bins int32 with the
+    edge's bin in bits 20..24) of the cluster engine."""
     valid = index >= 0
     at = index.clamp(min=0)
     w = torch.where(valid, sl_w.reshape(-1).index_select(0, at), torch.zeros((), device=sl_w.device))
-    ids = (sl.sl_src.reshape(-1).index_select(0, at) & ((1 << L.BT_BIN_SHIFT) - 1)) ^ 31
+    src = sl.sl_src.reshape(-1).index_select(0, at)
+    ids = (src & ((1 << L.BT_BIN_SHIFT) - 1)) ^ 31
     ids = torch.where(valid, ids, torch.full((), n ^ 31, dtype=ids.dtype, device=ids.device))
+    if n_bins > 1:
+        bins = torch.where(valid, (src >> L.BT_BIN_SHIFT) & 31, torch.zeros((), dtype=src.dtype, device=src.device))
+        return w.contiguous(), (ids | (bins << 20)).contiguous()
     if n + 32 <= 65536:
         ids = torch.where(ids >= 32768, ids - 65536, ids).to(torch.int16)
     return w.contiguous(), ids.contiguous()
@@ -524,15 +532,13 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
         desc.tile_off, desc.tile_work = toff.data_ptr(), tile_ws.data_ptr()
         desc.spin_limit = int(getattr(rnn, "engine_spin_limit", 0))
     if mode == L.BT_MODE_CLUSTER:
-        if R > 1:
-            raise NotImplementedError("cluster mode has no synaptic delays")
         sl = slices_of(lay, dev)
-        shape = cluster_shape(n, B, lay.slices_ptr_host, choice.tile_posts)
+        shape = cluster_shape(n, B, lay.slices_ptr_host, choice.tile_posts, R)
         if shape is None:
             raise NotImplementedError("cluster mode: the network does not fit one cluster's shared memory")
         tp_c, P_c, rows_c = shape
         index, gptr = cluster_pack_index(lay, n, tp_c, P_c, rows_c, dev)
-        cl_w, cl_src = cluster_pack(sl, pack_slice_weights(sl, w), index, n)
+        cl_w, cl_src = cluster_pack(sl, pack_slice_weights(sl, w), index, n, R)
         cl_w, cl_src = static("cl_w", cl_w), static("cl_src", cl_src)
         tile_ws = alloc("tile_work", (32,), torch.int32, zero=True)  # word 2: status (a wait that gave up)
         keep += [cl_w, cl_src, gptr, tile_ws]

@@ -51,7 +51,7 @@ extern "C" {
 #define BT_API
 #endif
 
-#define BT_ABI_VERSION 10
+#define BT_ABI_VERSION 11
 #define BT_BIN_SHIFT 25              /* low 25 bits: neuron id, high 7: delay bin */
 #define BT_MAX_NEURONS (1 << 25)
 #define BT_MAX_BINS 128
@@ -289,8 +289,9 @@ BT_API int bt_psc_step(int64_t batch, int64_t n, bt_param coef, bt_param tau_syn
                               one thread-block cluster of n_tiles <= 16 CTAs holds
                               state and in-edges in shared memory, ordered in-edge
                               sums (bit-exact), spike words exchanged through
-                              distributed shared memory, a hardware cluster barrier
-                              per step; single delay bin 0, no receptor channels */
+                              distributed shared memory (asynchronous stores counted
+                              on mbarriers, bounded waits); delay bins up to 32, no
+                              receptor channels */
 
 typedef struct bt_engine_desc {
   /* sizes */
@@ -405,7 +406,9 @@ typedef struct bt_engine_desc {
        cl_w       [n_tiles][tile_rows / 4][32][4] fp32: group g, lane l, u =
                   the weight of row 4 g + u of lane l's post, 0 on padding;
        cl_src     the same shape, the presynaptic id XOR 31 (padding: n XOR
-                  31), uint16 when n + 32 <= 65536, else uint32;
+                  31), uint16 when n + 32 <= 65536, else uint32; with
+                  delay bins (n_bins > 1, n + 32 <= 2^20) uint32, the id
+                  XOR 31 in bits 0..19 and the edge's bin in bits 20..24;
        cl_gptr    [n_tiles][tile_posts / 32 + 1] int32: the first group of each
                   of the tile's 32-post slices, then the tile's group count;
      all three 16-byte aligned.  tile_work: 32 int32 words, word 2 the status
@@ -418,8 +421,9 @@ typedef struct bt_engine_desc {
 
 /* Cluster mode shared memory per CTA (0 for a bad shape): n neurons, a
    tile of tile_posts posts (a multiple of 32) holding tile_rows slice rows
-   (a multiple of 16). */
-BT_API int64_t bt_cluster_smem_bytes(int64_t n, int64_t batch, int32_t tile_posts, int64_t tile_rows);
+   (a multiple of 16), n_bins delay bins (1..32). */
+BT_API int64_t bt_cluster_smem_bytes(int64_t n, int64_t batch, int32_t tile_posts, int64_t tile_rows,
+                                     int32_t n_bins);
 
 /* Tile mode scratch words and shared memory bytes per CTA for a shape
    (0 for a bad shape). */

@@ -191,3 +191,88 @@ def test_cluster_deferred_status_reports_at_engine_status():
     with torch.no_grad(), environ.context(dt=1.0):
         rnn(x, engine_choice=cluster())
     rnn.engine_status()  # nothing pending that failed
+
+
+# ------------------------------------------------------------ delay bins --
+
+@pytest.mark.parametrize("name", ["delayed_psc", "hetero_delay", "lif_dyadic_soft", "lif_dyadic_input"])
+def test_cluster_bitwise_vs_reference_fixtures(name):
+    """The reference's own runs (golden fixtures; DelayedPSC's uniform delay,
+    HeterSynapsePSC's per-synapse delay bins, no delays): spike rasters, v
+    and psc traces and the final state bit for bit, in one launch."""
+    from tests import cases
+
+    d = cases.load(name)
+    rnn, psc_name = cases.build_model(d, "cuda", "gather")
+    with torch.no_grad(), environ.context(dt=float(d["dt"])):
+        z, st = rnn(torch.tensor(d["x"], device="cuda"), engine_choice=cluster())
+    assert rnn.last_engine_choice == cluster()
+    assert rnn.last_engine_launches == (3 if rnn.neuron_inp_module is not None else 1)  # (+ the projection's 2)
+    K = d["v"].shape[0]
+    np.testing.assert_array_equal(z.cpu().numpy().astype(np.uint8), cases.spikes(d))
+    np.testing.assert_array_equal(st["neuron.v"].cpu().numpy()[:K].reshape(d["v"].shape), d["v"])
+    np.testing.assert_array_equal(st[psc_name].cpu().numpy()[:K].reshape(d["psc"].shape), d["psc"])
+    np.testing.assert_array_equal(rnn.neuron.v.cpu().numpy().reshape(d["v_final"].shape), d["v_final"])
+
+
+@pytest.mark.parametrize("name", ["delayed_psc", "hetero_delay"])
+def test_cluster_delays_split_calls_and_uneven_lengths_equal_gather(name):
+    """Calls split at several points (the delay history carried across calls
+    through the modules), per-sample lengths, graph replay: the cluster engine
+    equals the gather engine bit for bit."""
+    from tests import cases
+
+    d = cases.load(name)
+    x = torch.tensor(d["x"], device="cuda")
+    B = x.shape[1]
+    lens = torch.tensor([x.shape[0] - 7 * b for b in range(B)], device="cuda")
+    outs = []
+    for choice in (GATHER, cluster()):
+        for graph in (False, True):
+            rnn, psc_name = cases.build_model(d, "cuda", "gather")
+            rnn.cudagraph = graph
+            zs = []
+            with torch.no_grad(), environ.context(dt=float(d["dt"])):
+                for a, b in ((0, 5), (5, 37), (37, x.shape[0])):
+                    z, _ = rnn(x[a:b], sample_len=(lens - a).clamp(min=0, max=b - a), engine_choice=choice)
+                    zs.append(z.cpu().numpy())
+            outs.append((np.concatenate(zs), rnn.neuron.v.cpu().numpy(), getattr(rnn.synapse, "psc", None)))
+    ref = outs[0]
+    assert ref[0].sum() > 50
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o[0], ref[0])
+        np.testing.assert_array_equal(o[1], ref[1])
+
+
+def test_cluster_many_delay_bins_any_weights_equal_gather():
+    """A random network with per-synapse delays of 1..12 steps (12 bins, 13
+    bitmap copies) and non-dyadic weights, batch 3: the cluster engine's
+    ordered sums equal the gather engine's bit for bit over 200 steps."""
+    import pandas as pd
+    import scipy.sparse as sp
+
+    from btorch_b200.models import LIF, HeterSynapsePSC, RecurrentNN, SparseConn
+    from btorch_b200.models.functional import init_net_state
+
+    rng = np.random.default_rng(12)
+    n, R, B, T = 1200, 12, 3, 200
+    nnz = 40 * n
+    pre = rng.integers(0, n, nnz)
+    post = rng.integers(0, n, nnz)
+    binv = rng.integers(0, R, nnz)
+    w = (rng.normal(0.0, 0.25, nnz) * np.where(pre < 0.8 * n, 1.0, -2.0)).astype(np.float32)
+    m = sp.coo_array((w, (pre * R + binv, post)), shape=(n * R, n)).tocsr().tocoo()
+    x = torch.tensor((rng.random((T, B, n)) < 0.02).astype(np.float32) * 1.5, device="cuda")
+    outs = []
+    for choice in (GATHER, cluster()):
+        rti = pd.DataFrame({"receptor_type": ["syn"], "receptor_index": [0]})
+        conn = SparseConn(m, sparse_config={"direction": "gather"})
+        syn = HeterSynapsePSC(n, 1, rti, conn, max_delay_steps=R, use_circular_buffer=True, tau_syn=5.0)
+        rnn = RecurrentNN(LIF(n, tau_ref=2.0, hard_reset=True), syn, update_state_names=("neuron.v",)).cuda()
+        init_net_state(rnn, batch_size=B, dtype=torch.float32, device="cuda")
+        with torch.no_grad(), environ.context(dt=1.0):
+            z, st = rnn(x, engine_choice=choice)
+        outs.append((z.cpu().numpy(), st["neuron.v"].cpu().numpy()))
+    assert outs[0][0].sum() > 500
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)

@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
     for s in syms:
         assert hasattr(lib, s), s
     assert set(syms) == set(L.exported_symbols())
-    assert lib.bt_abi_version() == L.ABI_VERSION == 10
+    assert lib.bt_abi_version() == L.ABI_VERSION == 11
 
 
 def test_layout_matches_numpy_reference():
@@ -345,8 +345,9 @@ def test_tile_mode_is_an_opt_in_candidate():
 
 def test_cluster_mode_is_a_candidate_unless_scatter_is_asked_for():
     """The single-cluster engine (an ordered gather) is offered with
-    direction auto or gather, deterministic included, but not with an
-    explicit scatter, receptor channels, delays or more than 256 samples."""
+    direction auto or gather, deterministic included, with up to 32 delay
+    bins, but not with an explicit scatter, receptor channels or more than
+    256 samples."""
     import scipy.sparse as sp
 
     from btorch_b200.models import SparseConn, autotune
@@ -354,7 +355,8 @@ def test_cluster_mode_is_a_candidate_unless_scatter_is_asked_for():
     conn = SparseConn(sp.coo_array(np.eye(64, dtype=np.float32)), sparse_config={"direction": "auto"})
     assert L.BT_MODE_CLUSTER in autotune.allowed_modes(conn, 8)
     assert L.BT_MODE_CLUSTER not in autotune.allowed_modes(conn, 8, receptors=2)
-    assert L.BT_MODE_CLUSTER not in autotune.allowed_modes(conn, 8, n_bins=3)
+    assert L.BT_MODE_CLUSTER in autotune.allowed_modes(conn, 8, n_bins=3)
+    assert L.BT_MODE_CLUSTER not in autotune.allowed_modes(conn, 8, n_bins=40)
     assert L.BT_MODE_CLUSTER not in autotune.allowed_modes(conn, 300)
     conn.sparse_config.direction = "gather"
     assert L.BT_MODE_CLUSTER in autotune.allowed_modes(conn, 8)
@@ -405,3 +407,32 @@ def test_cluster_packing_holds_every_in_edge_in_order(n, tp):
                 np.testing.assert_array_equal(got_ids[:k], pres)
                 np.testing.assert_array_equal(got_w[:k], csc[post, pres].astype(np.float32))
                 assert (got_ids[k:] == n).all() and (got_w[k:] == 0).all()
+
+
+def test_cluster_packing_carries_the_delay_bin():
+    """With delay bins (here DelayedPSC's uniform delay: every edge in bin 2)
+    the packed ids are 32-bit, the id XOR 31 in bits 0..19 and the bin in
+    bits 20..24; the padding has bin 0 and id n."""
+    from btorch_b200.models import SparseConn
+    from btorch_b200.models._ops import pack_slice_weights
+    from btorch_b200.models.engine import cluster_pack, cluster_pack_index, cluster_shape, slices_of
+
+    n = 700
+    rng = np.random.default_rng(2)
+    dense = (rng.random((n, n)) < 0.04) * rng.normal(0, 1, (n, n))
+    conn = SparseConn(sp.coo_array(dense.astype(np.float32)))
+    lay = conn.engine_layout(3, 2, "cpu")
+    sl = slices_of(lay, "cpu")
+    tp, P, rows = cluster_shape(n, 2, lay.slices_ptr_host, n_bins=3)
+    index, gptr = cluster_pack_index(lay, n, tp, P, rows, "cpu")
+    w = conn._edge_weight().detach().float().contiguous()
+    cl_w, cl_src = cluster_pack(sl, pack_slice_weights(sl, w), index, n, 3)
+    assert cl_src.dtype == torch.int32
+    ids = cl_src.numpy().astype(np.int64)
+    pre = (ids & 0xFFFFF) ^ 31
+    edge = pre != n  # the slices' own padding and the rows added per slice hold id n, bin 0
+    assert ((ids[edge] >> 20) == 2).all() and ((ids[~edge] >> 20) == 0).all()
+    pres = pre[edge]
+    assert pres.max() < n and np.bincount(pres, minlength=n).sum() == int((dense != 0).sum())
+    assert L.lib().bt_cluster_smem_bytes(n, 2, tp, rows, 3) > L.lib().bt_cluster_smem_bytes(n, 2, tp, rows, 1)
+    assert L.lib().bt_cluster_smem_bytes(n, 2, tp, rows, 33) == 0
