@@ -862,6 +862,17 @@ def _allreduce(v, dev, op):
     return float(t.item())
 
 
+def _step_kernel(rnn):
+    """What the roofline's step time covers, by the engine mode that ran."""
+    mode = rnn.last_engine_choice.describe()["mode"] if rnn.last_engine_choice is not None else "?"
+    if mode == "cluster":
+        return ("single-cluster engine, one launch per call (state and in-edges in the shared memory of 16 SMs: "
+                "HBM does not bind; profiles/cluster_engine_plain.md)")
+    if mode == "tile":
+        return "persistent tile engine, one launch per call"
+    return f"recurrent step ({mode}: neuron + synapse launches)"
+
+
 def measure(name, cfg, args, dev, world, rank, local):
     """Time args.steps whole batches of workload `name`.  Returns (line dict,
     or None on ranks > 0; model; input; lengths; network; step function; the
@@ -948,7 +959,7 @@ def measure(name, cfg, args, dev, world, rank, local):
             "neuron_steps_per_s": n * live_steps / (elapsed_ms * 1e-3) if world == 1 else None,
             "spike_rate_per_step": events_total / max(1, live_steps) / len(net["w"]),
             "events_per_live_sample_step": events_total / max(1, live_steps),
-            "roofline": {"bound": "hbm", "kernel": "recurrent step (neuron + synapse launches)",
+            "roofline": {"bound": "hbm", "kernel": _step_kernel(rnn),
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_src, "traffic": traffic,
                          "traffic_note": "DRAM bytes per batch, scaled from profiles/eng_step_*_traffic.json",
