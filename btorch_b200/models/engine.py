@@ -538,7 +538,16 @@ def run(plan: EnginePlan, rnn, x: torch.Tensor, sample_len: torch.Tensor | None 
             raise NotImplementedError("cluster mode: the network does not fit one cluster's shared memory")
         tp_c, P_c, rows_c = shape
         index, gptr = cluster_pack_index(lay, n, tp_c, P_c, rows_c, dev)
-        cl_w, cl_src = cluster_pack(sl, pack_slice_weights(sl, w), index, n, R)
+        # packed again only when the connection's parameters or buffers (its
+        # effective weight's inputs) changed: in place (version) or replaced
+        key = (tp_c, P_c, rows_c, R, str(dev),
+               tuple((t.data_ptr(), t._version) for t in [*conn.parameters(), *conn.buffers()]))
+        cached = getattr(conn, "_cluster_packed", None)
+        if cached is not None and cached[0] == key:
+            cl_w, cl_src = cached[1], cached[2]
+        else:
+            cl_w, cl_src = cluster_pack(sl, pack_slice_weights(sl, w), index, n, R)
+            conn._cluster_packed = (key, cl_w, cl_src)
         cl_w, cl_src = static("cl_w", cl_w), static("cl_src", cl_src)
         tile_ws = alloc("tile_work", (32,), torch.int32, zero=True)  # word 2: status (a wait that gave up)
         keep += [cl_w, cl_src, gptr, tile_ws]

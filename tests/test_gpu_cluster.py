@@ -276,3 +276,32 @@ def test_cluster_many_delay_bins_any_weights_equal_gather():
     assert outs[0][0].sum() > 500
     for a, b in zip(*outs):
         np.testing.assert_array_equal(a, b)
+
+
+def test_cluster_repacks_after_a_weight_change():
+    """The packed in-edges are reused across calls while the connection's
+    parameters are unchanged, and packed again after an in-place change of
+    the magnitudes: the run then equals a fresh model with the new weights."""
+    rng = np.random.default_rng(21)
+    n, T, B = 2000, 40, 2
+    conn = _dyadic(rng, n, 0.02)
+    x = torch.tensor((np.round(rng.poisson(0.08, (T, B, n)) * 0.5 * 64) / 64).astype(np.float32), device="cuda")
+    rnn = _model(conn, n, 0, B, names=())
+    with torch.no_grad(), environ.context(dt=1.0):
+        rnn(x, engine_choice=cluster())
+        packed = rnn.synapse.linear._cluster_packed
+        rnn(x, engine_choice=cluster())
+        assert rnn.synapse.linear._cluster_packed is packed  # reused
+        rnn.synapse.linear.magnitude.mul_(2.0)
+        from btorch_b200.models.functional import init_net_state
+
+        init_net_state(rnn, batch_size=B, dtype=torch.float32, device="cuda")
+        z, _ = rnn(x, engine_choice=cluster())
+    assert rnn.synapse.linear._cluster_packed is not packed
+    conn2 = conn.copy()
+    conn2.data = conn2.data * 2.0
+    fresh = _model(conn2, n, 0, B, names=())
+    with torch.no_grad(), environ.context(dt=1.0):
+        z2, _ = fresh(x, engine_choice=GATHER)
+    np.testing.assert_array_equal(z.cpu().numpy(), z2.cpu().numpy())
+    assert z.cpu().numpy().sum() > 50
