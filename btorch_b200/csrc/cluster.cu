@@ -438,17 +438,16 @@ __global__ void __launch_bounds__(kClThreads, 1) k_cluster_engine(bt_engine_desc
       }
     }
     if (d.stats && (warp < items || B > 1)) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        st_un += __shfl_xor_sync(0xffffffffu, st_un, o);
-        st_ev += __shfl_xor_sync(0xffffffffu, st_ev, o);
-        st_ed += __shfl_xor_sync(0xffffffffu, st_ed, o);
-      }
+      // warp sums in 32 bits: a step's counts are at most batch x synapses,
+      // which a network that fits one cluster keeps below 2^32
+      const unsigned un = __reduce_add_sync(0xffffffffu, unsigned(st_un));
+      const unsigned ev = __reduce_add_sync(0xffffffffu, unsigned(st_ev));
+      const unsigned ed = __reduce_add_sync(0xffffffffu, unsigned(st_ed));
       if (lane == 0) {
         unsigned long long* st = reinterpret_cast<unsigned long long*>(d.stats + k * 4);
-        if (st_un) atomicAdd(st + 0, (unsigned long long)st_un);
-        if (st_ev) atomicAdd(st + 1, (unsigned long long)st_ev);
-        if (st_ed) atomicAdd(st + 2, (unsigned long long)st_ed);
+        if (un) atomicAdd(st + 0, (unsigned long long)un);
+        if (ev) atomicAdd(st + 1, (unsigned long long)ev);
+        if (ed) atomicAdd(st + 2, (unsigned long long)ed);
       }
     }
     if (warp < items) x_ahead = drive(k + 1, warp);
